@@ -1,0 +1,181 @@
+/*
+ * kls.h - C ABI of libkls.so, the B200 (sm_100a) implementation of the
+ * Kalnajs log-spiral matrix-method eigenvalue path:
+ *
+ *   orbit integration -> W_l(alpha) table + N_m(alpha) -> M(omega) contraction
+ *   -> det(I - M(omega)) -> omega-plane scan / Newton root (Omega_p, gamma).
+ *
+ * Every entry point returns an int status (KLS_OK = 0).  The library owns all
+ * device memory; the caller owns host buffers.  Host arrays exported in
+ * "reference layout" use the reference's Julia column-major order.
+ *
+ * Threading: one context per device per host thread.  A context is not
+ * re-entrant; distinct contexts are independent.
+ *
+ * Reference interfaces replaced (paths inside epolyach/Kalnajs_log_spirals):
+ *   KalnajsConfig / load_config     src/KalnajsLogSpiral/Configuration.jl:139-261
+ *   create_toomre_zang_model        src/KalnajsLogSpiral/Models.jl:40-57
+ *   precompute_all + to_device      src/KalnajsLogSpiral/BasisFunctions.jl:73-165, 397-437
+ *   compute_determinant(_batched)   src/KalnajsLogSpiral/MatrixBuilder.jl:197-239
+ *   build_M_matrix                  src/KalnajsLogSpiral/MatrixBuilder.jl:242-244
+ *   grid_scan / find_minimum        src/KalnajsLogSpiral/GridScan.jl:25-88, 234-246
+ *   newton_search / NewtonResult    src/KalnajsLogSpiral/NewtonSolver.jl:19-172
+ */
+#ifndef KLS_H
+#define KLS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define KLS_OK               0
+#define KLS_ERR_CONFIG       1  /* invalid configuration / argument          */
+#define KLS_ERR_CUDA         2  /* a CUDA runtime call failed                 */
+#define KLS_ERR_OOM          3  /* device allocation failed                   */
+#define KLS_ERR_STATE        4  /* call order (e.g. det before precompute)    */
+#define KLS_ERR_NONFINITE    5  /* non-finite value in an input or result     */
+#define KLS_ERR_SINGULAR     6  /* singular 2x2 Newton Jacobian               */
+#define KLS_ERR_UNSUPPORTED  7  /* mode not available on this device          */
+
+/* ---- precision modes of the contraction -------------------------------- */
+#define KLS_MODE_FP64        0  /* plain FP64 (the oracle form)               */
+#define KLS_MODE_MIXED       1  /* split-BF16 tensor-core contraction, FP32
+                                   accumulation; FP64 weights/LU              */
+
+/* ---- configuration: the [physics] [model] [grid] TOML sections ---------- *
+ * Mirrors PhysicsConfig / ModelConfig / GridConfig
+ * (Configuration.jl:31-67).  q1 is real-valued here (the reference types it
+ * Int, Configuration.jl:42); integer values reproduce the reference.        */
+typedef struct kls_config {
+    int32_t m;          /* azimuthal number                                 */
+    double  G;          /* gravitational constant                           */
+    double  L0;         /* taper angular-momentum scale                     */
+    int32_t n_zang;     /* taper exponent                                   */
+    double  q1;         /* dispersion parameter, q = q1 - 1                 */
+    int32_t NR;         /* guiding-centre radii                             */
+    int32_t Ne;         /* circulation (v) points                           */
+    double  Rc_min, Rc_max, v_min;
+    int32_t N_alpha;    /* log-spiral alpha points on [-alpha_max, alpha_max]*/
+    double  alpha_max;
+    int32_t l_min, l_max;  /* radial harmonics                              */
+    int32_t nw;         /* orbit integration points                          */
+    int32_t nwa;        /* stored (subsampled) orbit points                  */
+} kls_config;
+
+/* Dimensions derived from a config (and device padding). */
+typedef struct kls_dims {
+    int32_t NPh;        /* NR * Ne                                          */
+    int32_t n_l;        /* l_max - l_min + 1                                */
+    int32_t N_alpha;
+    int32_t N_alpha_pad;/* row length of the device W table                 */
+    int64_t K;          /* NPh * n_l contraction length                     */
+    int64_t K_pad;      /* padded rows of the device W table                */
+    int32_t nwa;
+    int64_t device_bytes; /* device memory held by the context             */
+} kls_dims;
+
+/* Newton parameters: NewtonConfig (Configuration.jl:84-100). */
+typedef struct kls_newton_cfg {
+    int32_t max_iter;
+    double  tol;
+    double  delta;
+    int32_t use_line_search;
+    int32_t max_line_search;
+    int32_t mode;          /* KLS_MODE_* used for every det evaluation        */
+} kls_newton_cfg;
+
+/* NewtonResult (NewtonSolver.jl:19-27). */
+typedef struct kls_newton_result {
+    double  Omega_p;
+    double  gamma;
+    double  omega_re, omega_im;
+    double  det_re, det_im;
+    int32_t iterations;
+    int32_t converged;
+    int32_t det_evals;     /* determinant evaluations performed               */
+} kls_newton_result;
+
+/* Grid-scan parameters: ScanConfig (Configuration.jl:72-79). */
+typedef struct kls_scan_cfg {
+    int32_t n_Op, n_gamma;
+    double  Omega_p_min, Omega_p_max;
+    double  gamma_min, gamma_max;
+    int32_t mode;
+    int32_t batch;         /* omegas per device launch (<=0: library choice)  */
+} kls_scan_cfg;
+
+typedef struct kls_ctx kls_ctx;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+/* Replaces create_toomre_zang_model + the device selection of to_device. */
+int kls_create(const kls_config* cfg, int device, kls_ctx** out);
+int kls_destroy(kls_ctx* ctx);
+/* Message of the last failing call on this context (never NULL). */
+const char* kls_last_error(const kls_ctx* ctx);
+/* Message for failures of kls_create, where no context exists yet. */
+const char* kls_create_error(void);
+int kls_get_dims(const kls_ctx* ctx, kls_dims* out);
+/* Launch subsequent work on this cudaStream_t (NULL = the context's own). */
+int kls_set_stream(kls_ctx* ctx, void* cuda_stream);
+
+/* ---- omega-independent stage: precompute_all + to_device ---------------- *
+ * Grids, orbit integration, Jacobian + DF, W_l table, N_m(alpha), DJ, F0l,
+ * Omega_res; all on the device, table device-resident (BasisFunctions.jl:73). */
+int kls_precompute(kls_ctx* ctx);
+/* Build the split-BF16 copy of the W table used by KLS_MODE_MIXED.         */
+int kls_prepare_mixed(kls_ctx* ctx);
+
+/* ---- exports in reference layout (host, column-major) ------------------- *
+ * Omega_1/Omega_2/jacobian/F0/FE/FL/DJ: [NR, Ne]; w1/ra/pha: [nwa, NR, Ne]
+ * (OrbitIntegration.jl:43-54); any pointer may be NULL to skip it.         */
+int kls_export_orbits(kls_ctx* ctx, double* Omega_1, double* Omega_2,
+                      double* jacobian, double* F0, double* FE, double* FL,
+                      double* DJ, double* w1, double* ra, double* pha);
+/* Grids (OrbitIntegration.jl:26-38): each [NR, Ne] except S_RC [NR].      */
+int kls_export_grids(kls_ctx* ctx, double* Rc, double* e, double* E,
+                     double* L_m, double* S_RC, double* S_e);
+/* alpha, d_alpha, N_kernel: [N_alpha] (BasisFunctions.jl:106-121).         */
+int kls_export_alpha(kls_ctx* ctx, double* alpha, double* d_alpha, double* N_kernel);
+/* F0l, Omega_res: [NPh, n_l] (BasisFunctions.jl:139-153).                  */
+int kls_export_resonant(kls_ctx* ctx, double* F0l, double* Omega_res);
+/* W_l_mat [NPh, N_alpha, n_l] complex (interleaved re,im), restricted to the
+ * harmonics [il0, il0+nl) to bound host memory (BasisFunctions.jl:55-56).  */
+int kls_export_W(kls_ctx* ctx, int il0, int nl, double* W_ri);
+
+/* ---- hot path ----------------------------------------------------------- */
+/* compute_determinant for n omegas (interleaved re,im), one batched launch
+ * sequence; det_ri interleaved re,im; log_abs = log|det| (may be NULL).
+ * Host buffers in, host buffers out (MatrixBuilder.jl:197-239).            */
+int kls_det_batch(kls_ctx* ctx, const double* omega_ri, int n, int mode,
+                  double* det_ri, double* log_abs);
+/* Same with device buffers on the context's stream; no host synchronisation.*/
+int kls_det_batch_device(kls_ctx* ctx, const double* d_omega_ri, int n, int mode,
+                         double* d_det_ri, double* d_log_abs);
+/* M(omega) [N_alpha, N_alpha] complex column-major (MatrixBuilder.jl:242).  */
+int kls_build_M(kls_ctx* ctx, double omega_re, double omega_im, int mode, double* M_ri);
+
+/* grid_scan (GridScan.jl:25-88): det_grid [n_gamma, n_Op] column-major
+ * complex; argmin of |det| in column-major order (GridScan.jl:234-246).   */
+int kls_scan(kls_ctx* ctx, const kls_scan_cfg* sc, double* det_grid_ri,
+             double* log_abs_grid, double* Omega_p0, double* gamma0);
+
+/* newton_search (NewtonSolver.jl:36-172).  history: (max_iter) x 3 row-major
+ * (Omega_p, gamma, |det|) per iteration, may be NULL.                      */
+int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cfg* nc,
+               kls_newton_result* res, double* history);
+
+/* ---- instrumentation ----------------------------------------------------- */
+/* Per-stage device time (ms) of the last det batch when timing is enabled:
+ * [0] weights, [1] contraction, [2] reduce/epilogue, [3] LU.               */
+int kls_enable_timing(kls_ctx* ctx, int on);
+int kls_get_stage_ms(kls_ctx* ctx, float* ms4);
+/* Kernels launched by this context since creation (monotone counter).      */
+int64_t kls_launch_count(const kls_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KLS_H */

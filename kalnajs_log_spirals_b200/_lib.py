@@ -1,0 +1,130 @@
+"""ctypes binding of libkls.so (include/kls.h).
+
+The shared library is built in-tree (``kalnajs_log_spirals_b200/libkls.so``).
+There is no CPU fallback: if the library is missing or has no CUDA device to
+run on, the calls raise ``KlsError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkls.so")
+
+KLS_OK = 0
+KLS_ERR_CONFIG = 1
+KLS_ERR_CUDA = 2
+KLS_ERR_OOM = 3
+KLS_ERR_STATE = 4
+KLS_ERR_NONFINITE = 5
+KLS_ERR_SINGULAR = 6
+KLS_ERR_UNSUPPORTED = 7
+
+KLS_MODE_FP64 = 0
+KLS_MODE_MIXED = 1
+
+STATUS_NAMES = {0: "KLS_OK", 1: "KLS_ERR_CONFIG", 2: "KLS_ERR_CUDA", 3: "KLS_ERR_OOM",
+                4: "KLS_ERR_STATE", 5: "KLS_ERR_NONFINITE", 6: "KLS_ERR_SINGULAR",
+                7: "KLS_ERR_UNSUPPORTED"}
+
+
+class KlsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class kls_config(C.Structure):
+    _fields_ = [("m", C.c_int32), ("G", C.c_double), ("L0", C.c_double), ("n_zang", C.c_int32),
+                ("q1", C.c_double), ("NR", C.c_int32), ("Ne", C.c_int32),
+                ("Rc_min", C.c_double), ("Rc_max", C.c_double), ("v_min", C.c_double),
+                ("N_alpha", C.c_int32), ("alpha_max", C.c_double), ("l_min", C.c_int32),
+                ("l_max", C.c_int32), ("nw", C.c_int32), ("nwa", C.c_int32)]
+
+
+class kls_dims(C.Structure):
+    _fields_ = [("NPh", C.c_int32), ("n_l", C.c_int32), ("N_alpha", C.c_int32),
+                ("N_alpha_pad", C.c_int32), ("K", C.c_int64), ("K_pad", C.c_int64),
+                ("nwa", C.c_int32), ("device_bytes", C.c_int64)]
+
+
+class kls_newton_cfg(C.Structure):
+    _fields_ = [("max_iter", C.c_int32), ("tol", C.c_double), ("delta", C.c_double),
+                ("use_line_search", C.c_int32), ("max_line_search", C.c_int32),
+                ("mode", C.c_int32)]
+
+
+class kls_newton_result(C.Structure):
+    _fields_ = [("Omega_p", C.c_double), ("gamma", C.c_double), ("omega_re", C.c_double),
+                ("omega_im", C.c_double), ("det_re", C.c_double), ("det_im", C.c_double),
+                ("iterations", C.c_int32), ("converged", C.c_int32), ("det_evals", C.c_int32)]
+
+
+class kls_scan_cfg(C.Structure):
+    _fields_ = [("n_Op", C.c_int32), ("n_gamma", C.c_int32), ("Omega_p_min", C.c_double),
+                ("Omega_p_max", C.c_double), ("gamma_min", C.c_double),
+                ("gamma_max", C.c_double), ("mode", C.c_int32), ("batch", C.c_int32)]
+
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes); every symbol include/kls.h declares
+SIGNATURES = {
+    "kls_create": (C.c_int, [C.POINTER(kls_config), C.c_int, C.POINTER(_P)]),
+    "kls_destroy": (C.c_int, [_P]),
+    "kls_last_error": (C.c_char_p, [_P]),
+    "kls_create_error": (C.c_char_p, []),
+    "kls_get_dims": (C.c_int, [_P, C.POINTER(kls_dims)]),
+    "kls_set_stream": (C.c_int, [_P, _P]),
+    "kls_precompute": (C.c_int, [_P]),
+    "kls_prepare_mixed": (C.c_int, [_P]),
+    "kls_export_orbits": (C.c_int, [_P] + [_D] * 10),
+    "kls_export_grids": (C.c_int, [_P] + [_D] * 6),
+    "kls_export_alpha": (C.c_int, [_P] + [_D] * 3),
+    "kls_export_resonant": (C.c_int, [_P] + [_D] * 2),
+    "kls_export_W": (C.c_int, [_P, C.c_int, C.c_int, _D]),
+    "kls_det_batch": (C.c_int, [_P, _D, C.c_int, C.c_int, _D, _D]),
+    "kls_det_batch_device": (C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
+    "kls_build_M": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _D]),
+    "kls_scan": (C.c_int, [_P, C.POINTER(kls_scan_cfg), _D, _D, _D, _D]),
+    "kls_newton": (C.c_int, [_P, C.c_double, C.c_double, C.POINTER(kls_newton_cfg),
+                             C.POINTER(kls_newton_result), _D]),
+    "kls_enable_timing": (C.c_int, [_P, C.c_int]),
+    "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "kls_launch_count": (C.c_int64, [_P]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load libkls.so once; raises KlsError if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise KlsError(KLS_ERR_STATE, f"{path} is missing: build it with "
+                                      "`python -m kalnajs_log_spirals_b200.build`")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def dptr(a) -> _D:
+    """double* of a C-contiguous float64 numpy array (or NULL for None)."""
+    if a is None:
+        return C.cast(None, _D)
+    assert a.dtype.name in ("float64", "complex128") and a.flags.c_contiguous or a.flags.f_contiguous
+    return a.ctypes.data_as(_D)
+
+
+def check(ctx, code: int) -> None:
+    if code != KLS_OK:
+        lib = load()
+        msg = lib.kls_last_error(ctx).decode() if ctx else lib.kls_create_error().decode()
+        raise KlsError(code, msg)

@@ -1,0 +1,555 @@
+// C ABI of libkls.so (declared in include/kls.h).
+//
+// Host-side control of the path: configuration checks, device memory,
+// the omega-independent precompute (BasisFunctions.precompute_all +
+// to_device), batched determinants (MatrixBuilder.compute_determinant /
+// _batched), the omega-plane scan (GridScan.grid_scan / find_minimum) and the
+// Newton search (NewtonSolver.newton_search) with the reference's exact
+// step, line-search, clamp and stopping rules.
+#include "kls_internal.cuh"
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+static thread_local std::string g_create_err;
+
+int kls_fail(kls_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  else g_create_err = msg;
+  return code;
+}
+
+int kls_cuda_fail(kls_ctx* c, cudaError_t e, const char* what) {
+  std::string m = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+  int code = (e == cudaErrorMemoryAllocation) ? KLS_ERR_OOM : KLS_ERR_CUDA;
+  return kls_fail(c, code, m);
+}
+
+namespace {
+
+constexpr int WS_CHUNK = 16;   // omegas per device launch sequence
+
+int validate(const kls_config* k, std::string& msg) {
+  char buf[256];
+  auto bad = [&](const char* m) { msg = m; return KLS_ERR_CONFIG; };
+  if (!k) return bad("config is NULL");
+  if (k->NR < 1 || k->Ne < 1) return bad("NR and Ne must be >= 1");
+  if (k->N_alpha < 1) return bad("N_alpha must be >= 1");
+  if (k->l_max < k->l_min) return bad("l_max must be >= l_min");
+  if (!(k->Rc_min > 0.0) || !(k->Rc_max >= k->Rc_min)) return bad("need 0 < Rc_min <= Rc_max");
+  if (!(k->q1 > 0.0)) return bad("q1 must be > 0");
+  if (!(k->alpha_max >= 0.0)) return bad("alpha_max must be >= 0");
+  if (k->n_zang < 0) return bad("n_zang must be >= 0");
+  if (k->nw < 3 || k->nwa < 2 || k->nwa > k->nw) return bad("need nw >= 3 and 2 <= nwa <= nw");
+  int nwai = (k->nw - 1) / (k->nwa - 1);
+  int len = (k->nw - 1) / nwai + 1;   // length(1:nwai:nw)
+  if (len != k->nwa) {
+    snprintf(buf, sizeof buf,
+             "length(1:nwai:nw) = %d differs from nwa = %d (the reference fails with a "
+             "DimensionMismatch for this (nw, nwa))", len, k->nwa);
+    msg = buf;
+    return KLS_ERR_CONFIG;
+  }
+  double np = (double)k->NR * k->Ne;
+  if (np * (k->l_max - k->l_min + 1) > 4.0e9) return bad("NPh * n_l too large");
+  if (!std::isfinite(k->G) || !std::isfinite(k->L0) || !std::isfinite(k->v_min))
+    return bad("non-finite G, L0 or v_min");
+  return KLS_OK;
+}
+
+template <typename T>
+int dalloc(kls_ctx* c, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T) + 16);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    char buf[160];
+    snprintf(buf, sizeof buf, "cudaMalloc of %.3f GB failed: %s", count * sizeof(T) / 1e9,
+             cudaGetErrorString(e));
+    return kls_fail(c, KLS_ERR_OOM, buf);
+  }
+  c->device_bytes += (int64_t)(count * sizeof(T));
+  return KLS_OK;
+}
+
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+
+int ensure_ws(kls_ctx* c, int n) {
+  if (n <= c->ws_omega && c->d_part) return KLS_OK;
+  int cap = std::max(n, c->ws_omega);
+  dfree(c->d_omega); dfree(c->d_wt); dfree(c->d_part); dfree(c->d_A); dfree(c->d_det);
+  dfree(c->d_logabs);
+  c->d_omega = nullptr; c->d_wt = nullptr; c->d_part = nullptr; c->d_A = nullptr;
+  c->d_det = nullptr; c->d_logabs = nullptr;
+  c->ws_omega = 0;
+  int r;
+  if ((r = dalloc(c, &c->d_omega, (size_t)2 * cap))) return r;
+  if ((r = dalloc(c, &c->d_wt, (size_t)cap * c->K_pad))) return r;
+  if ((r = dalloc(c, &c->d_part, (size_t)cap * c->splits * c->Na_pad * c->Na_pad))) return r;
+  if ((r = dalloc(c, &c->d_A, (size_t)cap * c->Na * c->Na))) return r;
+  if ((r = dalloc(c, &c->d_det, (size_t)cap))) return r;
+  if ((r = dalloc(c, &c->d_logabs, (size_t)cap))) return r;
+  c->ws_omega = cap;
+  return KLS_OK;
+}
+
+// One launch sequence for n (<= ws) omegas already in c->d_omega.
+int run_batch(kls_ctx* c, int n, int mode, bool export_M) {
+  int r;
+  const int splits = c->splits;
+  if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[0], c->stream));
+  if ((r = kls_run_weights(c, n))) return r;
+  if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[1], c->stream));
+  if (mode == KLS_MODE_FP64) {
+    if ((r = kls_run_contract_f64(c, n, splits))) return r;
+  } else if (mode == KLS_MODE_MIXED) {
+    if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
+    if ((r = kls_mixed_contract(c, n, splits))) return r;
+  } else {
+    return kls_fail(c, KLS_ERR_CONFIG, "unknown precision mode");
+  }
+  if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[2], c->stream));
+  if ((r = kls_run_reduce(c, n, splits, export_M))) return r;
+  if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[3], c->stream));
+  if ((r = kls_run_lu(c, n))) return r;
+  if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[4], c->stream));
+  return KLS_OK;
+}
+
+int collect_timing(kls_ctx* c) {
+  if (!c->timing) return KLS_OK;
+  KLS_CK(c, cudaEventSynchronize(c->ev[4]));
+  for (int i = 0; i < 4; ++i) {
+    float ms = 0.f;
+    KLS_CK(c, cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]));
+    c->stage_ms[i] += ms;
+  }
+  return KLS_OK;
+}
+
+int check_ready(kls_ctx* c) {
+  if (!c) return KLS_ERR_CONFIG;
+  if (!c->precomputed) return kls_fail(c, KLS_ERR_STATE, "kls_precompute has not run");
+  KLS_CK(c, cudaSetDevice(c->device));
+  return KLS_OK;
+}
+
+// Host-buffer batch: omegas in, dets out, chunked by the workspace size.
+int det_batch_host(kls_ctx* c, const double* omega_ri, int n, int mode, double* det_ri,
+                   double* log_abs) {
+  int r;
+  if (c->timing) std::fill(c->stage_ms, c->stage_ms + 4, 0.f);
+  for (int b = 0; b < n; b += WS_CHUNK) {
+    int nb = std::min(WS_CHUNK, n - b);
+    for (int i = 0; i < 2 * nb; ++i)
+      if (!std::isfinite(omega_ri[2 * b + i]))
+        return kls_fail(c, KLS_ERR_NONFINITE, "non-finite omega");
+    if ((r = ensure_ws(c, nb))) return r;
+    KLS_CK(c, cudaMemcpyAsync(c->d_omega, omega_ri + 2 * b, 2 * nb * sizeof(double),
+                              cudaMemcpyHostToDevice, c->stream));
+    if ((r = run_batch(c, nb, mode, false))) return r;
+    KLS_CK(c, cudaMemcpyAsync(det_ri + 2 * b, c->d_det, nb * sizeof(double2),
+                              cudaMemcpyDeviceToHost, c->stream));
+    if (log_abs)
+      KLS_CK(c, cudaMemcpyAsync(log_abs + b, c->d_logabs, nb * sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream));
+    KLS_CK(c, cudaStreamSynchronize(c->stream));
+    if ((r = collect_timing(c))) return r;
+  }
+  return KLS_OK;
+}
+
+// 2x2 solve J x = F by LU with partial pivoting (the order LAPACK dgesv uses
+// for Julia's J \ F).  Returns false on an exactly singular factor.
+bool solve2(const double J[2][2], const double F[2], double x[2]) {
+  double a00 = J[0][0], a01 = J[0][1], a10 = J[1][0], a11 = J[1][1];
+  double f0 = F[0], f1 = F[1];
+  if (std::fabs(a10) > std::fabs(a00)) {
+    std::swap(a00, a10); std::swap(a01, a11); std::swap(f0, f1);
+  }
+  if (a00 == 0.0) return false;
+  double l = a10 * (1.0 / a00);
+  double u11 = a11 - l * a01;
+  if (u11 == 0.0) return false;
+  double y1 = f1 - l * f0;
+  x[1] = y1 / u11;
+  x[0] = (f0 - a01 * x[1]) / a00;
+  return true;
+}
+
+}  // namespace
+
+// ======================================================================
+extern "C" {
+
+const char* kls_create_error(void) { return g_create_err.c_str(); }
+
+const char* kls_last_error(const kls_ctx* ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
+
+int kls_create(const kls_config* cfg, int device, kls_ctx** out) {
+  if (!out) return kls_fail(nullptr, KLS_ERR_CONFIG, "out is NULL");
+  *out = nullptr;
+  std::string msg;
+  int r = validate(cfg, msg);
+  if (r) return kls_fail(nullptr, r, msg);
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return kls_fail(nullptr, KLS_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= ndev) return kls_fail(nullptr, KLS_ERR_CONFIG, "bad device index");
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10)
+    return kls_fail(nullptr, KLS_ERR_UNSUPPORTED, "libkls.so is built for sm_100a (B200)");
+  kls_ctx* c = new kls_ctx();
+  c->cfg = *cfg;
+  c->device = device;
+  if ((e = cudaSetDevice(device)) != cudaSuccess || (e = cudaStreamCreateWithFlags(
+      &c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    delete c;
+    return kls_fail(nullptr, KLS_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e));
+  }
+  c->own_stream = c->stream;
+  for (auto& ev : c->ev) cudaEventCreate(&ev);
+  c->NR = cfg->NR; c->Ne = cfg->Ne; c->NPh = cfg->NR * cfg->Ne;
+  c->n_l = cfg->l_max - cfg->l_min + 1;
+  c->Na = cfg->N_alpha;
+  c->Na_pad = ((cfg->N_alpha + KLS_TILE - 1) / KLS_TILE) * KLS_TILE;
+  c->nw = cfg->nw; c->nwa = cfg->nwa; c->nwai = (cfg->nw - 1) / (cfg->nwa - 1);
+  c->K = (int64_t)c->NPh * c->n_l;
+  c->K_pad = ((c->K + KLS_KROW_ALIGN - 1) / KLS_KROW_ALIGN) * KLS_KROW_ALIGN;
+  c->splits = kls_choose_splits(c);
+
+  size_t need = (size_t)2 * c->K_pad * c->Na_pad * sizeof(double);
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  if (need > fr) {
+    char buf[200];
+    snprintf(buf, sizeof buf, "W table needs %.2f GB, device has %.2f GB free", need / 1e9,
+             fr / 1e9);
+    kls_destroy(c);
+    return kls_fail(nullptr, KLS_ERR_OOM, buf);
+  }
+  if ((r = dalloc(c, &c->d_cosw, c->nw)) || (r = dalloc(c, &c->d_sinw, c->nw)) ||
+      (r = dalloc(c, &c->d_of, (size_t)OF_COUNT * c->NPh)) ||
+      (r = dalloc(c, &c->d_SRC, c->NR)) || (r = dalloc(c, &c->d_valid, c->NPh)) ||
+      (r = dalloc(c, &c->d_w1, (size_t)c->NPh * c->nwa)) ||
+      (r = dalloc(c, &c->d_ra, (size_t)c->NPh * c->nwa)) ||
+      (r = dalloc(c, &c->d_pha, (size_t)c->NPh * c->nwa)) ||
+      (r = dalloc(c, &c->d_alpha, c->Na)) || (r = dalloc(c, &c->d_dalpha, c->Na)) ||
+      (r = dalloc(c, &c->d_N, c->Na)) || (r = dalloc(c, &c->d_Gk, c->K_pad)) ||
+      (r = dalloc(c, &c->d_Ok, c->K_pad)) || (r = dalloc(c, &c->d_F0l, c->K_pad)) ||
+      (r = dalloc(c, &c->d_Wre, (size_t)c->K_pad * c->Na_pad)) ||
+      (r = dalloc(c, &c->d_Wim, (size_t)c->K_pad * c->Na_pad)) ||
+      (r = dalloc(c, &c->d_M, (size_t)c->Na * c->Na))) {
+    std::string m = c->err;
+    kls_destroy(c);
+    return kls_fail(nullptr, r, m);
+  }
+  *out = c;
+  return KLS_OK;
+}
+
+int kls_destroy(kls_ctx* c) {
+  if (!c) return KLS_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  kls_mixed_free(c);
+  void* ptrs[] = {c->d_cosw, c->d_sinw, c->d_of, c->d_SRC, c->d_valid, c->d_w1, c->d_ra,
+                  c->d_pha, c->d_alpha, c->d_dalpha, c->d_N, c->d_Gk, c->d_Ok, c->d_F0l,
+                  c->d_Wre, c->d_Wim, c->d_omega, c->d_wt, c->d_part, c->d_A, c->d_M,
+                  c->d_det, c->d_logabs};
+  for (void* p : ptrs) dfree(p);
+  for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return KLS_OK;
+}
+
+int kls_get_dims(const kls_ctx* c, kls_dims* d) {
+  if (!c || !d) return KLS_ERR_CONFIG;
+  d->NPh = c->NPh; d->n_l = c->n_l; d->N_alpha = c->Na; d->N_alpha_pad = c->Na_pad;
+  d->K = c->K; d->K_pad = c->K_pad; d->nwa = c->nwa; d->device_bytes = c->device_bytes;
+  return KLS_OK;
+}
+
+int kls_set_stream(kls_ctx* c, void* s) {
+  if (!c) return KLS_ERR_CONFIG;
+  c->stream = s ? (cudaStream_t)s : c->own_stream;
+  return KLS_OK;
+}
+
+int kls_precompute(kls_ctx* c) {
+  if (!c) return KLS_ERR_CONFIG;
+  KLS_CK(c, cudaSetDevice(c->device));
+  int r;
+  if ((r = kls_run_orbits(c))) return r;
+  if ((r = kls_run_basis(c))) return r;
+  KLS_CK(c, cudaStreamSynchronize(c->stream));
+  c->precomputed = true;
+  return KLS_OK;
+}
+
+int kls_prepare_mixed(kls_ctx* c) {
+  int r = check_ready(c);
+  if (r) return r;
+  return kls_mixed_prepare(c);
+}
+
+int kls_export_orbits(kls_ctx* c, double* Om1, double* Om2, double* jac, double* F0,
+                      double* FE, double* FL, double* DJ, double* w1, double* ra, double* pha) {
+  int r = check_ready(c);
+  if (r) return r;
+  const size_t n = c->NPh;
+  struct { double* h; int f; } fl[] = {{Om1, OF_OM1}, {Om2, OF_OM2}, {jac, OF_JAC}, {F0, OF_F0},
+                                       {FE, OF_FE},   {FL, OF_FL},   {DJ, OF_DJ}};
+  for (auto& x : fl)
+    if (x.h) KLS_CK(c, cudaMemcpy(x.h, c->d_of + (size_t)x.f * n, n * sizeof(double),
+                                  cudaMemcpyDeviceToHost));
+  // [p][j] on the device is the reference's column-major [nwa, NR, Ne]
+  if (w1) KLS_CK(c, cudaMemcpy(w1, c->d_w1, n * c->nwa * sizeof(double), cudaMemcpyDeviceToHost));
+  if (ra) KLS_CK(c, cudaMemcpy(ra, c->d_ra, n * c->nwa * sizeof(double), cudaMemcpyDeviceToHost));
+  if (pha) KLS_CK(c, cudaMemcpy(pha, c->d_pha, n * c->nwa * sizeof(double), cudaMemcpyDeviceToHost));
+  return KLS_OK;
+}
+
+int kls_export_grids(kls_ctx* c, double* Rc, double* e, double* E, double* L_m, double* S_RC,
+                     double* S_e) {
+  int r = check_ready(c);
+  if (r) return r;
+  const size_t n = c->NPh;
+  struct { double* h; int f; } fl[] = {{Rc, OF_RC}, {e, OF_E_ECC}, {E, OF_ENERGY}, {L_m, OF_LM},
+                                       {S_e, OF_SE}};
+  for (auto& x : fl)
+    if (x.h) KLS_CK(c, cudaMemcpy(x.h, c->d_of + (size_t)x.f * n, n * sizeof(double),
+                                  cudaMemcpyDeviceToHost));
+  if (S_RC) KLS_CK(c, cudaMemcpy(S_RC, c->d_SRC, c->NR * sizeof(double), cudaMemcpyDeviceToHost));
+  return KLS_OK;
+}
+
+int kls_export_alpha(kls_ctx* c, double* alpha, double* dalpha, double* Nk) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (alpha) KLS_CK(c, cudaMemcpy(alpha, c->d_alpha, c->Na * sizeof(double), cudaMemcpyDeviceToHost));
+  if (dalpha) KLS_CK(c, cudaMemcpy(dalpha, c->d_dalpha, c->Na * sizeof(double), cudaMemcpyDeviceToHost));
+  if (Nk) KLS_CK(c, cudaMemcpy(Nk, c->d_N, c->Na * sizeof(double), cudaMemcpyDeviceToHost));
+  return KLS_OK;
+}
+
+int kls_export_resonant(kls_ctx* c, double* F0l, double* Ores) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (F0l) KLS_CK(c, cudaMemcpy(F0l, c->d_F0l, c->K * sizeof(double), cudaMemcpyDeviceToHost));
+  if (Ores) KLS_CK(c, cudaMemcpy(Ores, c->d_Ok, c->K * sizeof(double), cudaMemcpyDeviceToHost));
+  return KLS_OK;
+}
+
+int kls_export_W(kls_ctx* c, int il0, int nl, double* W) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (il0 < 0 || nl < 0 || il0 + nl > c->n_l || !W)
+    return kls_fail(c, KLS_ERR_CONFIG, "bad harmonic range for kls_export_W");
+  const size_t rows = c->NPh, ld = c->Na_pad;
+  std::vector<double> re(rows * ld), im(rows * ld);
+  for (int q = 0; q < nl; ++q) {
+    size_t r0 = (size_t)(il0 + q) * rows;
+    KLS_CK(c, cudaMemcpy(re.data(), c->d_Wre + r0 * ld, rows * ld * sizeof(double),
+                         cudaMemcpyDeviceToHost));
+    KLS_CK(c, cudaMemcpy(im.data(), c->d_Wim + r0 * ld, rows * ld * sizeof(double),
+                         cudaMemcpyDeviceToHost));
+    // reference layout [NPh, N_alpha, n_l], column-major, interleaved complex
+    double* blk = W + (size_t)2 * q * rows * c->Na;
+    for (int a = 0; a < c->Na; ++a)
+      for (size_t p = 0; p < rows; ++p) {
+        blk[2 * (p + rows * a)] = re[p * ld + a];
+        blk[2 * (p + rows * a) + 1] = im[p * ld + a];
+      }
+  }
+  return KLS_OK;
+}
+
+int kls_det_batch(kls_ctx* c, const double* omega_ri, int n, int mode, double* det_ri,
+                  double* log_abs) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (n < 0 || (n > 0 && (!omega_ri || !det_ri)))
+    return kls_fail(c, KLS_ERR_CONFIG, "bad arguments to kls_det_batch");
+  return det_batch_host(c, omega_ri, n, mode, det_ri, log_abs);
+}
+
+int kls_det_batch_device(kls_ctx* c, const double* d_omega, int n, int mode, double* d_det,
+                         double* d_log_abs) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (n < 0 || (n > 0 && (!d_omega || !d_det)))
+    return kls_fail(c, KLS_ERR_CONFIG, "bad arguments to kls_det_batch_device");
+  if (c->timing) std::fill(c->stage_ms, c->stage_ms + 4, 0.f);
+  for (int b = 0; b < n; b += WS_CHUNK) {
+    int nb = std::min(WS_CHUNK, n - b);
+    if ((r = ensure_ws(c, nb))) return r;
+    KLS_CK(c, cudaMemcpyAsync(c->d_omega, d_omega + 2 * b, 2 * nb * sizeof(double),
+                              cudaMemcpyDeviceToDevice, c->stream));
+    if ((r = run_batch(c, nb, mode, false))) return r;
+    KLS_CK(c, cudaMemcpyAsync(d_det + 2 * b, c->d_det, nb * sizeof(double2),
+                              cudaMemcpyDeviceToDevice, c->stream));
+    if (d_log_abs)
+      KLS_CK(c, cudaMemcpyAsync(d_log_abs + b, c->d_logabs, nb * sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
+    if (c->timing) {
+      // stage times need the events of every chunk; keep the device busy otherwise
+      if ((r = collect_timing(c))) return r;
+    }
+  }
+  return KLS_OK;
+}
+
+int kls_build_M(kls_ctx* c, double wr, double wi, int mode, double* M) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (!M) return kls_fail(c, KLS_ERR_CONFIG, "M is NULL");
+  if ((r = ensure_ws(c, 1))) return r;
+  double om[2] = {wr, wi};
+  KLS_CK(c, cudaMemcpyAsync(c->d_omega, om, sizeof om, cudaMemcpyHostToDevice, c->stream));
+  if ((r = run_batch(c, 1, mode, true))) return r;
+  std::vector<double2> h((size_t)c->Na * c->Na);
+  KLS_CK(c, cudaMemcpyAsync(h.data(), c->d_M, h.size() * sizeof(double2), cudaMemcpyDeviceToHost,
+                            c->stream));
+  KLS_CK(c, cudaStreamSynchronize(c->stream));
+  const int N = c->Na;
+  for (int b = 0; b < N; ++b)
+    for (int a = 0; a < N; ++a) {   // device [b][a] -> host column-major (b + N a)
+      M[2 * (b + (size_t)N * a)] = h[(size_t)b * N + a].x;
+      M[2 * (b + (size_t)N * a) + 1] = h[(size_t)b * N + a].y;
+    }
+  return KLS_OK;
+}
+
+int kls_scan(kls_ctx* c, const kls_scan_cfg* sc, double* det_grid, double* log_abs_grid,
+             double* Op0, double* g0) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (!sc || sc->n_Op < 1 || sc->n_gamma < 1 || !det_grid)
+    return kls_fail(c, KLS_ERR_CONFIG, "bad scan configuration");
+  const int nO = sc->n_Op, nG = sc->n_gamma, n = nO * nG;
+  std::vector<double> om(2 * (size_t)n), la((size_t)n);
+  // column-major det_grid[i_gamma, j_Op] (GridScan.jl:47, :101-104)
+  for (int j = 0; j < nO; ++j) {
+    double Op = kls_lin(sc->Omega_p_min, sc->Omega_p_max, nO, j);
+    for (int i = 0; i < nG; ++i) {
+      double g = kls_lin(sc->gamma_min, sc->gamma_max, nG, i);
+      om[2 * ((size_t)i + (size_t)nG * j)] = c->cfg.m * Op;
+      om[2 * ((size_t)i + (size_t)nG * j) + 1] = g;
+    }
+  }
+  if ((r = det_batch_host(c, om.data(), n, sc->mode, det_grid, la.data()))) return r;
+  if (log_abs_grid) std::copy(la.begin(), la.end(), log_abs_grid);
+  // argmin |det| in column-major order, first occurrence; NaN wins as in Julia
+  int best = 0;
+  double bv = INFINITY;
+  bool nan = false;
+  for (int q = 0; q < n; ++q) {
+    double v = std::hypot(det_grid[2 * q], det_grid[2 * q + 1]);
+    if (std::isnan(v)) { best = q; nan = true; break; }
+    if (v < bv) { bv = v; best = q; }
+  }
+  (void)nan;
+  int i = best % nG, j = best / nG;
+  if (Op0) *Op0 = kls_lin(sc->Omega_p_min, sc->Omega_p_max, nO, j);
+  if (g0) *g0 = kls_lin(sc->gamma_min, sc->gamma_max, nG, i);
+  return KLS_OK;
+}
+
+int kls_newton(kls_ctx* c, double Op_init, double g_init, const kls_newton_cfg* nc,
+               kls_newton_result* res, double* history) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (!nc || !res || nc->max_iter < 1) return kls_fail(c, KLS_ERR_CONFIG, "bad Newton arguments");
+  const double m = (double)c->cfg.m, tol = nc->tol, delta = nc->delta;
+  double Op = Op_init, g = g_init;
+  bool converged = false;
+  int iteration = 0, evals = 0;
+  double last_w[2] = {NAN, NAN}, last_det[2] = {NAN, NAN};
+  auto det1 = [&](double wr, double wi, double* d) -> int {
+    double w[2] = {wr, wi};
+    int q = det_batch_host(c, w, 1, nc->mode, d, nullptr);
+    if (q) return q;
+    ++evals;
+    last_w[0] = wr; last_w[1] = wi; last_det[0] = d[0]; last_det[1] = d[1];
+    return KLS_OK;
+  };
+  std::memset(res, 0, sizeof *res);
+  for (int it = 1; it <= nc->max_iter; ++it) {
+    iteration = it;
+    double d[2];
+    if ((r = det1(m * Op, g, d))) return r;
+    double F[2] = {d[0], d[1]};
+    double rn = std::hypot(F[0], F[1]);
+    if (history) {
+      history[3 * (it - 1)] = Op;
+      history[3 * (it - 1) + 1] = g;
+      history[3 * (it - 1) + 2] = std::hypot(d[0], d[1]);
+    }
+    if (rn < tol) { converged = true; break; }
+    // finite-difference Jacobian (NewtonSolver.jl:98-109): one batched launch
+    double w2[4] = {m * (Op + delta), g, m * Op, g + delta}, d2[4];
+    if ((r = det_batch_host(c, w2, 2, nc->mode, d2, nullptr))) return r;
+    evals += 2;
+    double J[2][2] = {{(d2[0] - d[0]) / delta, (d2[2] - d[0]) / delta},
+                      {(d2[1] - d[1]) / delta, (d2[3] - d[1]) / delta}};
+    double x[2];
+    if (!solve2(J, F, x)) {
+      res->Omega_p = Op; res->gamma = g; res->iterations = iteration; res->converged = 0;
+      res->det_evals = evals;
+      return kls_fail(c, KLS_ERR_SINGULAR, "singular finite-difference Jacobian");
+    }
+    double dx0 = -x[0], dx1 = -x[1];
+    if (nc->use_line_search) {
+      double a = 1.0;
+      for (int ls = 1; ls <= nc->max_line_search; ++ls) {
+        double Opn = Op + a * dx0, gn = g + a * dx1;
+        if (gn < 1e-4 || Opn < 0.0 || Opn > 1.0) { a *= 0.5; continue; }
+        double dn[2];
+        if ((r = det1(m * Opn, gn, dn))) return r;
+        if (std::hypot(dn[0], dn[1]) < rn) { Op = Opn; g = gn; break; }
+        a *= 0.5;
+        if (ls == nc->max_line_search) { Op += dx0; g += dx1; }
+      }
+    } else {
+      Op += dx0;
+      g += dx1;
+    }
+    g = std::max(g, 1e-4);
+    Op = std::min(std::max(Op, 0.0), 1.0);
+  }
+  // final evaluation (NewtonSolver.jl:160-161); the kernels are deterministic,
+  // so an omega that was just evaluated is not recomputed
+  double dfin[2];
+  if (last_w[0] == m * Op && last_w[1] == g) {
+    dfin[0] = last_det[0]; dfin[1] = last_det[1];
+  } else if ((r = det1(m * Op, g, dfin))) {
+    return r;
+  }
+  res->Omega_p = Op; res->gamma = g; res->omega_re = m * Op; res->omega_im = g;
+  res->det_re = dfin[0]; res->det_im = dfin[1];
+  res->iterations = iteration; res->converged = converged ? 1 : 0; res->det_evals = evals;
+  return KLS_OK;
+}
+
+int kls_enable_timing(kls_ctx* c, int on) {
+  if (!c) return KLS_ERR_CONFIG;
+  c->timing = on != 0;
+  return KLS_OK;
+}
+
+int kls_get_stage_ms(kls_ctx* c, float* ms4) {
+  if (!c || !ms4) return KLS_ERR_CONFIG;
+  for (int i = 0; i < 4; ++i) ms4[i] = c->stage_ms[i];
+  return KLS_OK;
+}
+
+int64_t kls_launch_count(const kls_ctx* c) { return c ? c->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// Internal declarations shared by the libkls.so translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include "kls.h"
+
+#define KLS_PI 3.14159265358979323846
+
+// Contraction tile geometry (FP64 path): the W table rows are padded to a
+// multiple of KLS_TILE so that alpha tiles never need masking.
+constexpr int KLS_TILE = 64;
+constexpr int KLS_KROW_ALIGN = 64;   // K rows padded to a multiple of this
+
+// Per-orbit scalar fields written by the orbit kernel (struct of arrays,
+// each NPh doubles, orbit index p = iR + NR*ie as in the reference).
+enum OrbitField {
+  OF_RC = 0, OF_E_ECC, OF_V, OF_R1, OF_R2, OF_ENERGY, OF_LM, OF_L2M, OF_SGNL, OF_SE,
+  OF_OM1, OF_OM2, OF_JAC, OF_F0, OF_FE, OF_FL, OF_DJ,
+  OF_COUNT
+};
+
+struct kls_mixed;   // split-BF16 tables (kls_mixed.cu)
+
+struct kls_ctx {
+  kls_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream all work is launched on
+  cudaStream_t own_stream = nullptr;  // the context's own stream
+  std::string err;
+
+  // dimensions
+  int NR = 0, Ne = 0, NPh = 0, n_l = 0, Na = 0, Na_pad = 0, nwa = 0, nw = 0, nwai = 0;
+  int64_t K = 0, K_pad = 0;
+  bool precomputed = false;
+  int64_t device_bytes = 0;
+
+  // omega-independent device data
+  double* d_cosw = nullptr;   // [nw]
+  double* d_sinw = nullptr;   // [nw]
+  double* d_of = nullptr;     // [OF_COUNT][NPh]
+  double* d_SRC = nullptr;    // [NR]
+  int* d_valid = nullptr;     // [NPh]  orbit usable for W (all samples finite)
+  double* d_w1 = nullptr;     // [NPh][nwa]
+  double* d_ra = nullptr;
+  double* d_pha = nullptr;
+  double* d_alpha = nullptr;  // [Na]
+  double* d_dalpha = nullptr; // [Na]
+  double* d_N = nullptr;      // [Na]
+  double* d_Gk = nullptr;     // [K_pad]  DJ * F0l per row k = il*NPh + p
+  double* d_Ok = nullptr;     // [K_pad]  Omega_res per row
+  double* d_F0l = nullptr;    // [K_pad]  F0l per row (export only)
+  double* d_Wre = nullptr;    // [K_pad][Na_pad]
+  double* d_Wim = nullptr;
+
+  // per-batch workspace (grown on demand)
+  int ws_omega = 0;           // omegas the workspace holds
+  int splits = 1;             // K splits of the contraction (fixed per context)
+  double* d_omega = nullptr;  // [ws_omega][2]
+  double2* d_wt = nullptr;    // [ws_omega][K_pad]
+  double2* d_part = nullptr;  // [ws_omega][splits][Na_pad][Na_pad]
+  double2* d_A = nullptr;     // [ws_omega][Na][Na]  I - M (row-major), overwritten by LU
+  double2* d_M = nullptr;     // [Na][Na] optional M export (row-major beta, alpha)
+  double2* d_det = nullptr;   // [ws_omega]
+  double* d_logabs = nullptr; // [ws_omega]
+  double* h_pinned = nullptr; // pinned staging for omegas/dets
+  int h_pinned_cap = 0;
+
+  kls_mixed* mixed = nullptr;
+
+  // instrumentation
+  int64_t launches = 0;
+  bool timing = false;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float stage_ms[4] = {0, 0, 0, 0};
+};
+
+// ---- helpers -------------------------------------------------------------
+int kls_fail(kls_ctx* c, int code, const std::string& msg);
+int kls_cuda_fail(kls_ctx* c, cudaError_t e, const char* what);
+#define KLS_CK(ctx, call)                                                   \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) return kls_cuda_fail((ctx), e_, #call);          \
+  } while (0)
+#define KLS_LAUNCHED(ctx)                                                   \
+  do {                                                                      \
+    (ctx)->launches++;                                                      \
+    cudaError_t e_ = cudaGetLastError();                                    \
+    if (e_ != cudaSuccess) return kls_cuda_fail((ctx), e_, "kernel launch"); \
+  } while (0)
+
+// numpy-style linspace point: a + i*(b-a)/(n-1), the last point exactly b
+__host__ __device__ inline double kls_lin(double a, double b, int n, int i) {
+  if (n <= 1) return a;
+  if (i == n - 1) return b;
+  double step = (b - a) / (double)(n - 1);
+  return a + (double)i * step;
+}
+
+// ---- stage entry points (host side, launch on ctx->stream) ---------------
+int kls_run_orbits(kls_ctx* c);
+int kls_run_basis(kls_ctx* c);
+int kls_run_weights(kls_ctx* c, int n);
+int kls_run_contract_f64(kls_ctx* c, int n, int splits);
+int kls_run_reduce(kls_ctx* c, int n, int splits, bool export_M);
+int kls_run_lu(kls_ctx* c, int n);
+int kls_choose_splits(const kls_ctx* c);
+// mixed-precision path (kls_mixed.cu)
+int kls_mixed_prepare(kls_ctx* c);
+int kls_mixed_contract(kls_ctx* c, int n, int splits);
+void kls_mixed_free(kls_ctx* c);

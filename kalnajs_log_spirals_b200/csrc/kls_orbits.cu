@@ -1,0 +1,312 @@
+// OrbitIntegration on the device: phase-space grid, per-orbit radial time
+// integral (Omega_1), azimuthal phase integral (Omega_2), subsampled
+// trajectory (w1, r, theta), Jacobian of (Rc, v) -> (E, L) and the
+// Toomre-Zang distribution function with its E and L derivatives.
+//
+// Follows src/KalnajsLogSpiral/OrbitIntegration.jl:102-382 and
+// src/KalnajsLogSpiral/Models.jl:40-169 of the reference.  One CTA per
+// orbit; the reference's sequential cumsum over nw points
+// (OrbitIntegration.jl:277-294) becomes a chunked block-wide prefix scan:
+// each thread sums a contiguous chunk, the chunk sums are scanned, and a
+// second pass re-evaluates the chunk to emit the running sums at the
+// subsample points 1:nwai:nw.
+#include "kls_internal.cuh"
+#include <cmath>
+
+namespace {
+
+constexpr int ORB_THREADS = 512;
+
+struct OrbitParams {
+  int NR, Ne, nw, nwa, nwai, Ia_last;
+  double Rc_min, Rc_max, v_min;
+  double L0, q1, qz, sigma_r0, DF_const;
+  int n_zang;
+  double dw;
+};
+
+__device__ double rc_1d(const OrbitParams& P, int i) {
+  double a = log10(P.Rc_min), b = log10(P.Rc_max);
+  return pow(10.0, kls_lin(a, b, P.NR, i));
+}
+
+// trapezoid weight of point i of a sequence (OrbitIntegration.jl:63-74)
+__device__ double trap_w(double xm, double x0, double xp, int i, int n) {
+  if (n < 2) return 0.0;
+  if (i == 0) return (xp - x0) / 2;
+  if (i == n - 1) return (x0 - xm) / 2;
+  return (xp - xm) / 2;
+}
+
+// Simpson weight of v point ie (OrbitIntegration.jl:79-95): falls back to
+// the trapezoid rule for n < 3 or even n
+__device__ double simpson_w(const OrbitParams& P, int ie) {
+  int n = P.Ne;
+  auto v = [&](int i) { return kls_lin(P.v_min, 1.0, n, i); };
+  if (n < 3 || (n % 2) == 0) {
+    double xm = ie > 0 ? v(ie - 1) : 0.0, xp = ie < n - 1 ? v(ie + 1) : 0.0;
+    return trap_w(xm, v(ie), xp, ie, n);
+  }
+  double dx = v(1) - v(0);
+  if (ie == 0 || ie == n - 1) return dx / 3;
+  return (ie % 2 == 1) ? 4 * dx / 3 : 2 * dx / 3;
+}
+
+__device__ double taper(const OrbitParams& P, double L) {
+  if (P.n_zang == 0) return 1.0;
+  double La = fabs(L);
+  if (La < 1e-12) return 0.0;
+  return 1.0 / (1.0 + pow(P.L0 / La, (double)P.n_zang));
+}
+
+__device__ double df0(const OrbitParams& P, double E, double L) {
+  double La = fabs(L);
+  if (La < 1e-12) return 0.0;
+  double s2 = P.sigma_r0 * P.sigma_r0;
+  double r = P.DF_const * exp(-E / s2) * pow(La, P.qz) * taper(P, L);
+  return isfinite(r) ? r : 0.0;
+}
+
+// Radial-integrand pieces at point i of the w grid: x, svr (time) and
+// svr_phi (phase) before endpoint extrapolation.
+struct PointVals { double x, svr, svp; };
+
+__device__ __forceinline__ PointVals point_vals(double rs, double drs, double E, double L2,
+                                                bool nonradial, double cw, double sw) {
+  PointVals v;
+  v.x = rs - drs * cw;
+  if (nonradial) {
+    double vr2 = 2.0 * (E - log(v.x)) * v.x * v.x - L2;
+    double rvr = sqrt(fmax(0.0, vr2));
+    v.svr = sw * v.x / rvr;
+    v.svp = sw / rvr;
+  } else {
+    double vr2 = 2.0 * (E - log(v.x));
+    double vr = sqrt(fmax(0.0, vr2));
+    v.svr = sw / vr;
+    v.svp = 0.0;
+  }
+  return v;
+}
+
+template <typename T>
+__device__ T block_exclusive_scan(T val, T* sh, T* total) {
+  // sh: blockDim.x entries
+  int t = threadIdx.x;
+  sh[t] = val;
+  __syncthreads();
+  for (int off = 1; off < blockDim.x; off <<= 1) {
+    T add = (t >= off) ? sh[t - off] : T(0);
+    __syncthreads();
+    sh[t] += add;
+    __syncthreads();
+  }
+  T incl = sh[t];
+  if (total) *total = sh[blockDim.x - 1];
+  __syncthreads();
+  return incl - val;  // exclusive
+}
+
+__global__ void __launch_bounds__(ORB_THREADS)
+orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __restrict__ sinw,
+             double* __restrict__ of, int NPh, double* __restrict__ SRC, int* __restrict__ valid,
+             double* __restrict__ w1o, double* __restrict__ rao, double* __restrict__ phao) {
+  __shared__ double sh_t[ORB_THREADS];
+  __shared__ double sh_p[ORB_THREADS];
+  __shared__ double sh_misc[4];
+  const int p = blockIdx.x;
+  const int iR = p % P.NR, ie = p / P.NR;
+  const int tid = threadIdx.x;
+
+  // ---- grid scalars (OrbitIntegration.jl:102-170), computed redundantly
+  const double Rc = rc_1d(P, iR);
+  double v = kls_lin(P.v_min, 1.0, P.Ne, ie);
+  if (fabs(v) < 1e-14) v = 1e-12;
+  const double sg = (v > 0) ? 1.0 : ((v < 0) ? -1.0 : 0.0);
+  const double ecc = 1.0 - fabs(v);
+  const double R1 = Rc * (1.0 - ecc), R2 = Rc * (1.0 + ecc);
+  double E;
+  if (fabs(R2 * R2 - R1 * R1) > 1e-14) {
+    E = (log(R2) * (R2 * R2) - log(R1) * (R1 * R1)) / (R2 * R2 - R1 * R1);
+  } else {
+    E = Rc * (1.0 / Rc) / 2 + log(Rc);
+  }
+  if (!isfinite(E)) E = log(R2);
+  double L2 = 2.0 * (E - log(R2)) * (R2 * R2);
+  if (L2 < 1e-14) L2 = 0.0;
+  const double L = sqrt(L2) * sg;
+
+  const double kap = sqrt(2.0) / Rc, Om = 1.0 / Rc;
+  const int nw = P.nw, nwa = P.nwa, nwai = P.nwai;
+  double* w1p = w1o + (size_t)p * nwa;
+  double* rap = rao + (size_t)p * nwa;
+  double* php = phao + (size_t)p * nwa;
+  bool fin = true;
+  double Om1 = 0.0, Om2 = 0.0;
+
+  if (fabs(ecc) < 1e-10 || ecc < 0.01) {
+    // circular (:222-229) and epicyclic (:232-241) branches
+    Om1 = kap;
+    Om2 = Om * sg;
+    const bool circ = fabs(ecc) < 1e-10;
+    const double a_j = (R2 - R1) / 2;
+    for (int j = tid; j < nwa; j += blockDim.x) {
+      int i = j * nwai;
+      double wa = kls_lin(1e-8, KLS_PI - 1e-8, nw, i);
+      double r, ph;
+      if (circ) {
+        r = Rc;
+        ph = wa * Om2 / Om1;
+      } else {
+        r = Rc - a_j * cosw[i];
+        ph = wa * Om2 / Om1 + 2 * Om / kap * a_j / Rc * sinw[i] * sg;
+      }
+      w1p[j] = wa; rap[j] = r; php[j] = ph;
+      fin = fin && isfinite(wa) && isfinite(r) && isfinite(ph);
+    }
+  } else {
+    // general orbit (:244-302)
+    const double rs = (R1 + R2) / 2, drs = (R2 - R1) / 2;
+    const bool nonradial = L2 > 1e-12;
+    const bool phase_int = (fabs(1.0 - ecc) > 1e-10) && nonradial;
+    const double dtc = drs * P.dw;
+    // svr / svr_phi with the reference's endpoint extrapolation
+    auto vals_at = [&](int i, double& x, double& svr, double& svp) {
+      PointVals a = point_vals(rs, drs, E, L2, nonradial, cosw[i], sinw[i]);
+      x = a.x; svr = a.svr; svp = a.svp;
+      if (i == 0 || i == nw - 1) {
+        int i1 = (i == 0) ? 1 : nw - 2, i2 = (i == 0) ? 2 : nw - 3;
+        PointVals b = point_vals(rs, drs, E, L2, nonradial, cosw[i1], sinw[i1]);
+        PointVals c = point_vals(rs, drs, E, L2, nonradial, cosw[i2], sinw[i2]);
+        if (i == nw - 1 || nonradial) svr = 2.0 * b.svr - c.svr;
+        svp = 2.0 * b.svp - c.svp;
+      }
+    };
+    const int chunk = (nw + blockDim.x - 1) / blockDim.x;
+    const int i0 = tid * chunk, i1 = min(nw, i0 + chunk);
+    // pass 1: chunk sums of dt2 and dt4
+    double st = 0.0, sp = 0.0;
+    if (i0 < i1) {
+      double x, svr, svp;
+      double prev_t = 0.0, prev_p = 0.0;
+      if (i0 > 0) {
+        vals_at(i0 - 1, x, svr, svp);
+        prev_t = dtc * svr;
+        prev_p = dtc * svp / x;
+      }
+      for (int i = i0; i < i1; ++i) {
+        vals_at(i, x, svr, svp);
+        double dt1 = dtc * svr, dt3 = dtc * svp / x;
+        if (i > 0) { st += (prev_t + dt1) / 2; sp += (prev_p + dt3) / 2; }
+        prev_t = dt1; prev_p = dt3;
+      }
+    }
+    double tot_t, tot_p;
+    double pre_t = block_exclusive_scan(st, sh_t, &tot_t);
+    double pre_p = block_exclusive_scan(sp, sh_p, &tot_p);
+    Om1 = KLS_PI / tot_t;
+    // pass 2: running sums at subsample points
+    if (i0 < i1) {
+      double x, svr, svp;
+      double prev_t = 0.0, prev_p = 0.0;
+      double rt = pre_t, rp = pre_p;
+      if (i0 > 0) {
+        vals_at(i0 - 1, x, svr, svp);
+        prev_t = dtc * svr;
+        prev_p = dtc * svp / x;
+      }
+      for (int i = i0; i < i1; ++i) {
+        vals_at(i, x, svr, svp);
+        double dt1 = dtc * svr, dt3 = dtc * svp / x;
+        if (i > 0) { rt += (prev_t + dt1) / 2; rp += (prev_p + dt3) / 2; }
+        prev_t = dt1; prev_p = dt3;
+        if (i % nwai == 0 && i <= P.Ia_last) {
+          int j = i / nwai;
+          double ph;
+          if (phase_int) ph = L * rp;
+          else ph = (j == 0) ? 0.0 : (KLS_PI / 2) * 1.0 * sg;
+          double wv = rt * Om1;
+          w1p[j] = wv; rap[j] = x; php[j] = ph;
+          fin = fin && isfinite(wv) && isfinite(x) && isfinite(ph);
+          if (i == P.Ia_last) sh_misc[0] = ph;
+        }
+      }
+    }
+    __syncthreads();
+    Om2 = Om1 * sh_misc[0] / KLS_PI;
+  }
+  int all_fin = __syncthreads_and(fin ? 1 : 0);
+
+  if (tid == 0) {
+    // Jacobian (OrbitIntegration.jl:341-382)
+    double jac = 0.0;
+    if (fabs(R2 - R1) > 1e-12 && fabs(L) > 1e-12) {
+      double V1 = log(R1), V2 = log(R2), dV1 = 1.0 / R1, dV2 = 1.0 / R2;
+      double t1 = 2 * (E - V1) * R1 - dV1 * (R1 * R1);
+      double t2 = 2 * (E - V2) * R2 - dV2 * (R2 * R2);
+      double den = R2 * R2 - R1 * R1;
+      double dj = fabs(t1 * t2 / den);
+      jac = 2 * dj * Rc / Om1 / fabs(L);
+    }
+    if (fabs(L) <= 1e-12) {
+      double DelE = 2.0 * (E - log(R1));
+      jac = sqrt(fmax(DelE, 0.0)) * (1.0 / R2) * 2 * Rc / Om1;
+      if (!isfinite(jac)) jac = 0.0;
+    }
+    // DF and derivatives (Models.jl:137-169), NaN -> 0 (:331-333)
+    double F0 = df0(P, E, L);
+    double FE = -F0 / (P.sigma_r0 * P.sigma_r0);
+    double FL = 0.0;
+    if (fabs(L) >= 1e-12) FL = F0 * (P.qz + P.n_zang - P.n_zang * taper(P, L)) / fabs(L);
+    if (!isfinite(F0)) F0 = 0.0;
+    if (!isfinite(FE)) FE = 0.0;
+    if (!isfinite(FL)) FL = 0.0;
+    // S_RC and S_e quadrature weights (OrbitIntegration.jl:111-123)
+    double um = iR > 0 ? log(rc_1d(P, iR - 1)) : 0.0;
+    double up = iR < P.NR - 1 ? log(rc_1d(P, iR + 1)) : 0.0;
+    double src = Rc * trap_w(um, log(Rc), up, iR, P.NR);
+    double se = simpson_w(P, ie);
+    if (ie == 0) SRC[iR] = src;
+    double vals[OF_COUNT] = {Rc, ecc, v, R1, R2, E, L, L2, sg, se,
+                             Om1, Om2, jac, F0, FE, FL, src * se * jac};
+    for (int f = 0; f < OF_COUNT; ++f) of[(size_t)f * NPh + p] = vals[f];
+    double ratio = Om2 / Om1;
+    valid[p] = (all_fin && isfinite(ratio)) ? 1 : 0;
+  }
+}
+
+__global__ void sincos_table_kernel(int nw, double* cosw, double* sinw) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nw) {
+    double w = kls_lin(1e-8, KLS_PI - 1e-8, nw, i);
+    double s, c;
+    sincos(w, &s, &c);
+    cosw[i] = c; sinw[i] = s;
+  }
+}
+
+}  // namespace
+
+int kls_run_orbits(kls_ctx* c) {
+  const kls_config& k = c->cfg;
+  OrbitParams P{};
+  P.NR = c->NR; P.Ne = c->Ne; P.nw = c->nw; P.nwa = c->nwa; P.nwai = c->nwai;
+  P.Ia_last = (c->nwa - 1) * c->nwai;
+  P.Rc_min = k.Rc_min; P.Rc_max = k.Rc_max; P.v_min = k.v_min;
+  P.L0 = k.L0; P.q1 = k.q1; P.qz = k.q1 - 1.0; P.n_zang = k.n_zang;
+  P.sigma_r0 = 1.0 / std::sqrt(k.q1);
+  // DF normalisation (Models.jl:53-54), Gamma of a real argument
+  P.DF_const = 1.0 / (2.0 * KLS_PI * std::pow(2.0, P.qz / 2.0) * std::sqrt(KLS_PI) *
+                      std::tgamma((P.qz + 1.0) / 2.0) * std::pow(P.sigma_r0, P.qz + 2.0));
+  double w0 = kls_lin(1e-8, KLS_PI - 1e-8, c->nw, 0);
+  double w1 = kls_lin(1e-8, KLS_PI - 1e-8, c->nw, 1);
+  P.dw = w1 - w0;
+
+  sincos_table_kernel<<<(c->nw + 255) / 256, 256, 0, c->stream>>>(c->nw, c->d_cosw, c->d_sinw);
+  KLS_LAUNCHED(c);
+  orbit_kernel<<<c->NPh, ORB_THREADS, 0, c->stream>>>(P, c->d_cosw, c->d_sinw, c->d_of, c->NPh,
+                                                      c->d_SRC, c->d_valid, c->d_w1, c->d_ra,
+                                                      c->d_pha);
+  KLS_LAUNCHED(c);
+  return KLS_OK;
+}

@@ -1,0 +1,178 @@
+"""GPU parity: libkls.so against the oracle and the reference's published roots.
+
+Tolerances (FP64 throughout): orbit fields, grids and N_m 1e-12 relative to
+each array's max; the W table 1e-12 relative to max|W|; M(omega) entries
+1e-11 relative to max|M|; det(I - M) 1e-11 relative; Newton roots 1e-10
+absolute in Omega_p and gamma.
+"""
+import numpy as np
+import pytest
+
+import kalnajs_log_spirals_b200 as K
+from oracle import np_oracle as O
+from tests.conftest import load_case
+from tests.golden.make_fixtures import BASE, CASES
+
+pytestmark = pytest.mark.gpu
+
+
+def kconfig(**kw) -> K.KalnajsConfig:
+    c = K.KalnajsConfig()
+    for f in ("m", "G"):
+        if f in kw:
+            setattr(c.physics, f, kw[f])
+    for f in ("L0", "n_zang", "q1"):
+        if f in kw:
+            setattr(c.model, f, kw[f])
+    for f in ("NR", "Ne", "Rc_min", "Rc_max", "v_min", "N_alpha", "alpha_max", "l_min",
+              "l_max", "nw", "nwa"):
+        if f in kw:
+            setattr(c.grid, f, kw[f])
+    return c
+
+
+def relmax(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    s = float(np.max(np.abs(b))) if b.size else 0.0
+    return float(np.max(np.abs(a - b))) / (s if s > 0 else 1.0)
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request, lib_path):
+    name = request.param
+    over = {**BASE, **CASES[name]}
+    pc = K.precompute_all(kconfig(**over))
+    yield name, load_case(name), pc
+    pc.close()
+
+
+def test_orbits_and_grids(case):
+    name, ref, pc = case
+    o = pc.orbit_data
+    cm = lambda a: np.asarray(a).reshape(-1, order="F")
+    for k in ("Omega_1", "Omega_2", "jacobian", "F0", "FE", "FL"):
+        assert relmax(cm(getattr(o, k)), ref[k]) < 1e-12, (name, k)
+    for k in ("w1", "ra", "pha"):
+        assert relmax(cm(getattr(o, k)), ref[k]) < 1e-12, (name, k)
+    for k in ("Rc", "e", "E", "L_m", "S_e"):
+        assert relmax(cm(getattr(o.grids, k)), ref["grid_" + k]) < 1e-12, (name, k)
+    assert relmax(o.grids.S_RC, ref["grid_S_RC"]) < 1e-12
+    assert relmax(pc.DJ_vec, ref["DJ"]) < 1e-12
+
+
+def test_alpha_and_N_kernel(case):
+    name, ref, pc = case
+    assert relmax(pc.alpha_arr, ref["alpha"]) < 1e-15
+    assert relmax(pc.d_alpha, ref["d_alpha"]) < 1e-14
+    assert relmax(pc.N_kernel, ref["N_kernel"]) < 1e-13
+
+
+def test_resonant_rows(case):
+    name, ref, pc = case
+    assert relmax(pc.F0l_all.reshape(-1, order="F"), ref["F0l"]) < 1e-12
+    assert relmax(pc.Omega_res.reshape(-1, order="F"), ref["Omega_res"]) < 1e-12
+
+
+def test_W_table(case):
+    name, ref, pc = case
+    W = pc.W_l_mat
+    assert W.shape == ref["W"].shape
+    assert relmax(W, ref["W"]) < 1e-12, name
+
+
+def test_M_and_det(case):
+    name, ref, pc = case
+    M = K.build_M_matrix(ref["omegas"][0], pc)
+    assert relmax(M, ref["M0"]) < 1e-11, name
+    d = K.compute_determinant_batched(ref["omegas"], pc)
+    assert np.all(np.abs(d - ref["dets"]) <= 1e-11 * np.abs(ref["dets"])), name
+
+
+def test_batch_composition_is_bitwise_stable(case):
+    name, ref, pc = case
+    om = np.array([0.88 + 0.12j, 0.7 + 0.2j, 0.91 + 0.02j, 1.3 + 0.4j] * 5)
+    a = K.compute_determinant_batched(om, pc, batch_size=len(om))
+    b = np.array([K.compute_determinant(w, pc) for w in om[:4]])
+    assert np.array_equal(a[:4], b)
+    assert np.array_equal(a[:4], a[4:8])
+
+
+# ---------------------------------------------------------------------------
+# end-to-end roots
+# ---------------------------------------------------------------------------
+SMALL = dict(m=2, G=1.0, L0=1.0, n_zang=4, q1=7, NR=61, Ne=21, Rc_min=0.01, Rc_max=10.0,
+             v_min=0.01, N_alpha=101, alpha_max=10.0, l_min=-10, l_max=10, nw=10001, nwa=201)
+
+
+def test_newton_reproduces_published_root(lib_path):
+    """convergence_table.txt:13 (MATLAB, 10 decimals): 0.4397142267, 0.1230663944."""
+    c = kconfig(**SMALL)
+    c.newton.tol = 1e-12
+    c.newton.use_line_search = False
+    pc = K.precompute_all(c)
+    r = K.newton_search(c, pc, None, K.GPUType.NVIDIA, "Float64", 0.44, 0.13)
+    pc.close()
+    assert r.converged
+    assert abs(r.Omega_p - 0.4397142267) <= 6e-11
+    assert abs(r.gamma - 0.1230663944) <= 6e-11
+    # the oracle's root from the same start
+    oc = O.OracleConfig(**SMALL)
+    opc = O.precompute_all(oc)
+    ro = O.newton_search(lambda w: O.compute_det(opc, w), 2, 0.44, 0.13, tol=1e-12)
+    assert abs(r.Omega_p - ro.Omega_p) <= 1e-10 and abs(r.gamma - ro.gamma) <= 1e-10
+
+
+def test_newton_line_search_and_history(lib_path):
+    c = kconfig(**SMALL)
+    c.newton.tol = 1e-12
+    c.newton.use_line_search = True
+    pc = K.precompute_all(c)
+    r = K.newton_search(c, pc, None, K.GPUType.NVIDIA, "Float64", 0.44, 0.13)
+    pc.close()
+    oc = O.OracleConfig(**SMALL)
+    opc = O.precompute_all(oc)
+    ro = O.newton_search(lambda w: O.compute_det(opc, w), 2, 0.44, 0.13, tol=1e-12,
+                         use_line_search=True)
+    assert r.converged and r.iterations == ro.iterations
+    assert np.allclose(r.history[:, :2], ro.history[:, :2], rtol=0, atol=1e-10)
+
+
+def test_grid_scan_matches_oracle(lib_path):
+    c = kconfig(**{**SMALL, "NR": 31, "Ne": 11, "N_alpha": 41, "nw": 2001, "nwa": 101})
+    c.scan.n_Op, c.scan.n_gamma = 9, 5
+    pc = K.precompute_all(c)
+    dg, Op0, g0 = K.grid_scan(c, pc)
+    oc = O.OracleConfig(**{**SMALL, "NR": 31, "Ne": 11, "N_alpha": 41, "nw": 2001, "nwa": 101})
+    opc = O.precompute_all(oc)
+    s = c.scan
+    odg, oOp, og = O.grid_scan(lambda w: O.compute_det(opc, w), 2, s.n_Op, s.n_gamma,
+                               s.Omega_p_min, s.Omega_p_max, s.gamma_min, s.gamma_max)
+    pc.close()
+    assert dg.shape == (5, 9)
+    assert np.all(np.abs(dg - odg) <= 1e-11 * np.abs(odg))
+    assert (Op0, g0) == (oOp, og)
+
+
+@pytest.mark.slow
+def test_size_s_newton_matches_oracle(lib_path):
+    """Benchmark size S: NR=101, Ne=21, N_alpha=101 on [-30,30], l=+-25, nw=100001."""
+    import os
+    from tests.conftest import ROOT
+    c = K.load_config(os.path.join(ROOT, "configs", "size_s.toml"))
+    c = K.load_model(c, os.path.join(ROOT, "models", "kalnajs_zang4.toml"))
+    pc = K.precompute_all(c)
+    r = K.newton_search(c, pc, None, K.GPUType.NVIDIA, "Float64")
+    g = c.grid
+    oc = O.OracleConfig(m=2, G=1.0, L0=1.0, n_zang=4, q1=7, NR=g.NR, Ne=g.Ne, Rc_min=g.Rc_min,
+                        Rc_max=g.Rc_max, v_min=g.v_min, N_alpha=g.N_alpha,
+                        alpha_max=g.alpha_max, l_min=g.l_min, l_max=g.l_max, nw=g.nw,
+                        nwa=g.nwa)
+    opc = O.precompute_all(oc)
+    ro = O.newton_search(lambda w: O.compute_det(opc, w), 2, c.reference.Omega_p,
+                         c.reference.gamma, tol=c.newton.tol, delta=c.newton.delta)
+    # M entries at the root, relative to max|M|
+    M = K.build_M_matrix(ro.omega, pc)
+    pc.close()
+    assert relmax(M, O.build_M(opc, ro.omega)) < 1e-11
+    assert r.converged and ro.converged
+    assert abs(r.Omega_p - ro.Omega_p) <= 1e-10 and abs(r.gamma - ro.gamma) <= 1e-10
