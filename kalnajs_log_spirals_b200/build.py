@@ -23,6 +23,9 @@ LIB = os.path.join(PKG, "libkls.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v",
               "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
+# per-file extra flags: the orbit integrals are ill-conditioned near turning
+# points, so they keep the reference's separate multiply/add roundings
+EXTRA_FLAGS = {"kls_orbits.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -41,7 +44,8 @@ def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), _headers_mtime()):
         return obj
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", src, "-o", obj]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *EXTRA_FLAGS.get(os.path.basename(src), []), "-c", src,
+           "-o", obj]
     res = subprocess.run(cmd, capture_output=True, text=True)
     log = os.path.join(BUILD, os.path.basename(src) + ".log")
     with open(log, "w") as f:

@@ -10,6 +10,11 @@
 // each thread sums a contiguous chunk, the chunk sums are scanned, and a
 // second pass re-evaluates the chunk to emit the running sums at the
 // subsample points 1:nwai:nw.
+//
+// This translation unit is compiled without FMA contraction (-fmad=false)
+// and keeps the reference's association order: v_r^2 = 2(E - ln x) x^2 - L^2
+// cancels like 1/e^2 near the turning points of near-circular orbits, so a
+// one-ulp change in any term moves Omega_1 by up to ~1e-10 relative.
 #include "kls_internal.cuh"
 #include <cmath>
 
@@ -76,7 +81,8 @@ __device__ __forceinline__ PointVals point_vals(double rs, double drs, double E,
   PointVals v;
   v.x = rs - drs * cw;
   if (nonradial) {
-    double vr2 = 2.0 * (E - log(v.x)) * v.x * v.x - L2;
+    // (2 (E - V(x))) * x^2 - L^2, the reference's association order
+    double vr2 = 2.0 * (E - log(v.x)) * (v.x * v.x) - L2;
     double rvr = sqrt(fmax(0.0, vr2));
     v.svr = sw * v.x / rvr;
     v.svp = sw / rvr;

@@ -81,6 +81,12 @@ class OracleConfig:
         return self.NR * self.Ne
 
 
+# ln x along the orbit integrals; the fixture generator swaps in a perturbed
+# version to measure how sensitive the reference algorithm is to last-ulp
+# differences between math libraries
+orbit_log: Callable[[np.ndarray], np.ndarray] = np.log
+
+
 def linspace(a: float, b: float, n: int) -> np.ndarray:
     """``range(a, b, length=n)``: a + i*step with the last point exactly b."""
     return np.linspace(a, b, n)
@@ -300,13 +306,13 @@ def compute_orbits(c: OracleConfig, model: ToomreZang, g: Grids) -> Orbits:
                 drs = (r2 - r1) / 2
                 xs = rs - drs * cosw
                 if L2_j > 1e-12:
-                    vr_sq = 2.0 * (E_i - np.log(xs)) * xs ** 2 - L2_j
+                    vr_sq = 2.0 * (E_i - orbit_log(xs)) * xs ** 2 - L2_j
                     rvr = np.sqrt(np.maximum(0.0, vr_sq))
                     svr = sinw * xs / rvr
                     svr[0] = 2.0 * svr[1] - svr[2]
                     svr[-1] = 2.0 * svr[-2] - svr[-3]
                 else:
-                    vr_sq = 2.0 * (E_i - np.log(xs))
+                    vr_sq = 2.0 * (E_i - orbit_log(xs))
                     rvr = np.sqrt(np.maximum(0.0, vr_sq))
                     svr = sinw / rvr
                     svr[-1] = 2.0 * svr[-2] - svr[-3]

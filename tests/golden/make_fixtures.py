@@ -67,9 +67,29 @@ def make(name: str, over: dict) -> dict:
     return out
 
 
+def sensitivity(name: str, over: dict, base: dict) -> dict:
+    """|change| of every array when ln x along the orbits is off by 2 ulps.
+
+    The radial-velocity integrand 1/v_r with v_r^2 = 2(E - ln x) x^2 - L^2
+    cancels like 1/e^2 near the turning points of near-circular orbits, so
+    math libraries that differ in the last bit of ln give visibly different
+    Omega_1, Omega_2, w1 and theta.  The GPU tests allow a small multiple of
+    this change on top of a fixed FP64 floor.
+    """
+    orig = O.orbit_log
+    O.orbit_log = lambda x: orig(x) * (1.0 + 4.440892098500626e-16)
+    try:
+        pert = make(name, over)
+    finally:
+        O.orbit_log = orig
+    return {"sens_" + k: np.abs(np.asarray(pert[k]) - np.asarray(v))
+            for k, v in base.items() if k not in ("config", "omegas")}
+
+
 def main() -> None:
     for name, over in CASES.items():
         d = make(name, over)
+        d.update(sensitivity(name, over, d))
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **d)
         print(f"wrote {path}: W {d['W'].shape}, dets {d['dets']}")
