@@ -235,7 +235,8 @@ int kls_create(const kls_config* cfg, int device, kls_ctx** out) {
   }
   if ((r = dalloc(c, &c->d_cosw, c->nw)) || (r = dalloc(c, &c->d_sinw, c->nw)) ||
       (r = dalloc(c, &c->d_of, (size_t)OF_COUNT * c->NPh)) ||
-      (r = dalloc(c, &c->d_SRC, c->NR)) || (r = dalloc(c, &c->d_valid, c->NPh)) ||
+      (r = dalloc(c, &c->d_SRC, c->NR)) || (r = dalloc(c, &c->d_rc, c->NR)) ||
+      (r = dalloc(c, &c->d_valid, c->NPh)) ||
       (r = dalloc(c, &c->d_w1, (size_t)c->NPh * c->nwa)) ||
       (r = dalloc(c, &c->d_ra, (size_t)c->NPh * c->nwa)) ||
       (r = dalloc(c, &c->d_pha, (size_t)c->NPh * c->nwa)) ||
@@ -258,7 +259,7 @@ int kls_destroy(kls_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   kls_mixed_free(c);
-  void* ptrs[] = {c->d_cosw, c->d_sinw, c->d_of, c->d_SRC, c->d_valid, c->d_w1, c->d_ra,
+  void* ptrs[] = {c->d_cosw, c->d_sinw, c->d_of, c->d_SRC, c->d_rc, c->d_valid, c->d_w1, c->d_ra,
                   c->d_pha, c->d_alpha, c->d_dalpha, c->d_N, c->d_Gk, c->d_Ok, c->d_F0l,
                   c->d_Wre, c->d_Wim, c->d_omega, c->d_wt, c->d_part, c->d_A, c->d_M,
                   c->d_det, c->d_logabs};

@@ -201,23 +201,16 @@ __device__ double ln_abs_gamma(double x, double y) {
   return re + acc;
 }
 
-__global__ void alpha_kernel(int Na, double amax, int m, double* alpha, double* dalpha,
-                             double* Nk) {
+// N_m(alpha) = |Gamma(z1)|^2 / |Gamma(z3)|^2 * pi * d_alpha,
+// z1 = (m + 1/2 + i alpha)/2, z3 = (m + 3/2 + i alpha)/2
+__global__ void n_kernel(int Na, int m, const double* __restrict__ alpha,
+                         const double* __restrict__ dalpha, double* __restrict__ Nk) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Na) return;
-  double a = kls_lin(-amax, amax, Na, i);
-  double am = i > 0 ? kls_lin(-amax, amax, Na, i - 1) : 0.0;
-  double ap = i < Na - 1 ? kls_lin(-amax, amax, Na, i + 1) : 0.0;
-  double da;
-  if (Na < 2) da = 0.0;
-  else if (i == 0) da = (ap - a) / 2;
-  else if (i == Na - 1) da = (a - am) / 2;
-  else da = (ap - am) / 2;
+  double a = alpha[i];
   double l1 = ln_abs_gamma((m + 0.5) / 2, a / 2);
   double l3 = ln_abs_gamma((m + 1.5) / 2, a / 2);
-  alpha[i] = a;
-  dalpha[i] = da;
-  Nk[i] = exp(2.0 * (l1 - l3)) * KLS_PI * da;
+  Nk[i] = exp(2.0 * (l1 - l3)) * KLS_PI * dalpha[i];
 }
 
 __global__ void rows_kernel(int NPh, int n_l, int l_min, int m, int64_t K, int64_t K_pad,
@@ -242,8 +235,10 @@ __global__ void rows_kernel(int NPh, int n_l, int l_min, int m, int64_t K, int64
 
 int kls_run_basis(kls_ctx* c) {
   const kls_config& k = c->cfg;
-  alpha_kernel<<<(c->Na + 127) / 128, 128, 0, c->stream>>>(c->Na, k.alpha_max, k.m, c->d_alpha,
-                                                          c->d_dalpha, c->d_N);
+  int r = kls_upload_alpha(c);
+  if (r) return r;
+  n_kernel<<<(c->Na + 127) / 128, 128, 0, c->stream>>>(c->Na, k.m, c->d_alpha, c->d_dalpha,
+                                                      c->d_N);
   KLS_LAUNCHED(c);
   rows_kernel<<<(unsigned)((c->K_pad + 255) / 256), 256, 0, c->stream>>>(
       c->NPh, c->n_l, k.l_min, k.m, c->K, c->K_pad, c->d_of, c->d_Gk, c->d_Ok, c->d_F0l);

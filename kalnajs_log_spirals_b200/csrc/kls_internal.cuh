@@ -40,6 +40,7 @@ struct kls_ctx {
   double* d_sinw = nullptr;   // [nw]
   double* d_of = nullptr;     // [OF_COUNT][NPh]
   double* d_SRC = nullptr;    // [NR]
+  double* d_rc = nullptr;     // [NR] guiding-centre radii (host C-library pow)
   int* d_valid = nullptr;     // [NPh]  orbit usable for W (all samples finite)
   double* d_w1 = nullptr;     // [NPh][nwa]
   double* d_ra = nullptr;
@@ -100,6 +101,7 @@ __host__ __device__ inline double kls_lin(double a, double b, int n, int i) {
 
 // ---- stage entry points (host side, launch on ctx->stream) ---------------
 int kls_run_orbits(kls_ctx* c);
+int kls_upload_alpha(kls_ctx* c);
 int kls_run_basis(kls_ctx* c);
 int kls_run_weights(kls_ctx* c, int n);
 int kls_run_contract_f64(kls_ctx* c, int n, int splits);

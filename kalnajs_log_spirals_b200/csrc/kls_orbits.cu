@@ -17,6 +17,7 @@
 // one-ulp change in any term moves Omega_1 by up to ~1e-10 relative.
 #include "kls_internal.cuh"
 #include <cmath>
+#include <vector>
 
 namespace {
 
@@ -30,13 +31,8 @@ struct OrbitParams {
   double dw;
 };
 
-__device__ double rc_1d(const OrbitParams& P, int i) {
-  double a = log10(P.Rc_min), b = log10(P.Rc_max);
-  return pow(10.0, kls_lin(a, b, P.NR, i));
-}
-
 // trapezoid weight of point i of a sequence (OrbitIntegration.jl:63-74)
-__device__ double trap_w(double xm, double x0, double xp, int i, int n) {
+__host__ __device__ double trap_w(double xm, double x0, double xp, int i, int n) {
   if (n < 2) return 0.0;
   if (i == 0) return (xp - x0) / 2;
   if (i == n - 1) return (x0 - xm) / 2;
@@ -115,7 +111,8 @@ __device__ T block_exclusive_scan(T val, T* sh, T* total) {
 
 __global__ void __launch_bounds__(ORB_THREADS)
 orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __restrict__ sinw,
-             double* __restrict__ of, int NPh, double* __restrict__ SRC, int* __restrict__ valid,
+             const double* __restrict__ rc_tab, const double* __restrict__ SRC,
+             double* __restrict__ of, int NPh, int* __restrict__ valid,
              double* __restrict__ w1o, double* __restrict__ rao, double* __restrict__ phao) {
   __shared__ double sh_t[ORB_THREADS];
   __shared__ double sh_p[ORB_THREADS];
@@ -125,7 +122,7 @@ orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __res
   const int tid = threadIdx.x;
 
   // ---- grid scalars (OrbitIntegration.jl:102-170), computed redundantly
-  const double Rc = rc_1d(P, iR);
+  const double Rc = rc_tab[iR];
   double v = kls_lin(P.v_min, 1.0, P.Ne, ie);
   if (fabs(v) < 1e-14) v = 1e-12;
   const double sg = (v > 0) ? 1.0 : ((v < 0) ? -1.0 : 0.0);
@@ -267,27 +264,14 @@ orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __res
     if (!isfinite(F0)) F0 = 0.0;
     if (!isfinite(FE)) FE = 0.0;
     if (!isfinite(FL)) FL = 0.0;
-    // S_RC and S_e quadrature weights (OrbitIntegration.jl:111-123)
-    double um = iR > 0 ? log(rc_1d(P, iR - 1)) : 0.0;
-    double up = iR < P.NR - 1 ? log(rc_1d(P, iR + 1)) : 0.0;
-    double src = Rc * trap_w(um, log(Rc), up, iR, P.NR);
+    // S_e quadrature weight (OrbitIntegration.jl:119-123); S_RC from the host
+    double src = SRC[iR];
     double se = simpson_w(P, ie);
-    if (ie == 0) SRC[iR] = src;
     double vals[OF_COUNT] = {Rc, ecc, v, R1, R2, E, L, L2, sg, se,
                              Om1, Om2, jac, F0, FE, FL, src * se * jac};
     for (int f = 0; f < OF_COUNT; ++f) of[(size_t)f * NPh + p] = vals[f];
     double ratio = Om2 / Om1;
     valid[p] = (all_fin && isfinite(ratio)) ? 1 : 0;
-  }
-}
-
-__global__ void sincos_table_kernel(int nw, double* cosw, double* sinw) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nw) {
-    double w = kls_lin(1e-8, KLS_PI - 1e-8, nw, i);
-    double s, c;
-    sincos(w, &s, &c);
-    cosw[i] = c; sinw[i] = s;
   }
 }
 
@@ -308,11 +292,48 @@ int kls_run_orbits(kls_ctx* c) {
   double w1 = kls_lin(1e-8, KLS_PI - 1e-8, c->nw, 1);
   P.dw = w1 - w0;
 
-  sincos_table_kernel<<<(c->nw + 255) / 256, 256, 0, c->stream>>>(c->nw, c->d_cosw, c->d_sinw);
+  // Tables shared by every orbit, from the host C library: the w grid's cos
+  // and sin, the log-spaced guiding-centre radii and their trapezoid weights
+  // S_RC = Rc * trapz(ln Rc) (OrbitIntegration.jl:111-113, :188-193).  Near
+  // a turning point x = rs - drs cos w cancels catastrophically, so the table
+  // values, not just their accuracy, decide the last bits of Omega_1.
+  std::vector<double> cw(c->nw), sw(c->nw), rc(c->NR), src(c->NR);
+  for (int i = 0; i < c->nw; ++i) {
+    double w = kls_lin(1e-8, KLS_PI - 1e-8, c->nw, i);
+    cw[i] = std::cos(w);
+    sw[i] = std::sin(w);
+  }
+  const double la = std::log10(k.Rc_min), lb = std::log10(k.Rc_max);
+  for (int i = 0; i < c->NR; ++i) rc[i] = std::pow(10.0, kls_lin(la, lb, c->NR, i));
+  for (int i = 0; i < c->NR; ++i) {
+    double um = i > 0 ? std::log(rc[i - 1]) : 0.0;
+    double up = i < c->NR - 1 ? std::log(rc[i + 1]) : 0.0;
+    src[i] = rc[i] * trap_w(um, std::log(rc[i]), up, i, c->NR);
+  }
+  KLS_CK(c, cudaMemcpyAsync(c->d_cosw, cw.data(), c->nw * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+  KLS_CK(c, cudaMemcpyAsync(c->d_sinw, sw.data(), c->nw * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+  KLS_CK(c, cudaMemcpyAsync(c->d_rc, rc.data(), c->NR * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+  KLS_CK(c, cudaMemcpyAsync(c->d_SRC, src.data(), c->NR * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+  orbit_kernel<<<c->NPh, ORB_THREADS, 0, c->stream>>>(P, c->d_cosw, c->d_sinw, c->d_rc, c->d_SRC,
+                                                      c->d_of, c->NPh, c->d_valid, c->d_w1,
+                                                      c->d_ra, c->d_pha);
   KLS_LAUNCHED(c);
-  orbit_kernel<<<c->NPh, ORB_THREADS, 0, c->stream>>>(P, c->d_cosw, c->d_sinw, c->d_of, c->NPh,
-                                                      c->d_SRC, c->d_valid, c->d_w1, c->d_ra,
-                                                      c->d_pha);
-  KLS_LAUNCHED(c);
+  // the host vectors must outlive the asynchronous copies
+  KLS_CK(c, cudaStreamSynchronize(c->stream));
+  return KLS_OK;
+}
+
+int kls_upload_alpha(kls_ctx* c) {
+  // alpha grid and its trapezoid weights (BasisFunctions.jl:106-107)
+  std::vector<double> a(c->Na), d(c->Na);
+  for (int i = 0; i < c->Na; ++i) a[i] = kls_lin(-c->cfg.alpha_max, c->cfg.alpha_max, c->Na, i);
+  for (int i = 0; i < c->Na; ++i)
+    d[i] = trap_w(i > 0 ? a[i - 1] : 0.0, a[i], i < c->Na - 1 ? a[i + 1] : 0.0, i, c->Na);
+  KLS_CK(c, cudaMemcpy(c->d_alpha, a.data(), c->Na * sizeof(double), cudaMemcpyHostToDevice));
+  KLS_CK(c, cudaMemcpy(c->d_dalpha, d.data(), c->Na * sizeof(double), cudaMemcpyHostToDevice));
   return KLS_OK;
 }

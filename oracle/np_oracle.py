@@ -87,6 +87,11 @@ class OracleConfig:
 orbit_log: Callable[[np.ndarray], np.ndarray] = np.log
 
 
+def _ln(x):
+    """ln of the potential V = ln r along grids, orbits and Jacobian."""
+    return orbit_log(x)
+
+
 def linspace(a: float, b: float, n: int) -> np.ndarray:
     """``range(a, b, length=n)``: a + i*step with the last point exactly b."""
     return np.linspace(a, b, n)
@@ -210,8 +215,10 @@ class Grids:
 
 def compute_grids(c: OracleConfig, model: ToomreZang) -> Grids:
     NR, Ne = c.NR, c.Ne
-    Rc_1d = 10.0 ** linspace(math.log10(c.Rc_min), math.log10(c.Rc_max), NR)
-    uRc = np.log(Rc_1d)
+    # the C library's pow and log (the device uses the same host-computed grid)
+    Rc_1d = np.array([10.0 ** float(x) for x in linspace(math.log10(c.Rc_min),
+                                                          math.log10(c.Rc_max), NR)])
+    uRc = np.array([math.log(x) for x in Rc_1d])
     S_RC = Rc_1d * trapezoid_coef(uRc)
     v_arr = linspace(c.v_min, 1.0, Ne)
     S_e = np.tile(simpson_coef(v_arr), (NR, 1))
@@ -226,15 +233,15 @@ def compute_grids(c: OracleConfig, model: ToomreZang) -> Grids:
     for iR in range(NR):
         for ie in range(Ne):
             r1, r2 = R1[iR, ie], R2[iR, ie]
-            V1, V2 = math.log(r1), math.log(r2)
+            V1, V2 = _ln(r1), _ln(r2)
             if abs(r2 ** 2 - r1 ** 2) > 1e-14:
                 E[iR, ie] = (V2 * r2 ** 2 - V1 * r1 ** 2) / (r2 ** 2 - r1 ** 2)
             else:
                 r = Rc[iR, ie]
-                E[iR, ie] = r * (1.0 / r) / 2 + math.log(r)
+                E[iR, ie] = r * (1.0 / r) / 2 + _ln(r)
             if not math.isfinite(E[iR, ie]):
-                E[iR, ie] = math.log(R2[iR, ie])
-    L2_m = 2.0 * (E - np.log(R2)) * R2 ** 2
+                E[iR, ie] = _ln(R2[iR, ie])
+    L2_m = 2.0 * (E - _ln(R2)) * R2 ** 2
     L2_m[L2_m < 1e-14] = 0.0
     L_m = np.sqrt(L2_m) * SGNL
     return Grids(Rc, e, v, R1, R2, E, L_m, L2_m, SGNL, S_RC, S_e)
@@ -306,13 +313,13 @@ def compute_orbits(c: OracleConfig, model: ToomreZang, g: Grids) -> Orbits:
                 drs = (r2 - r1) / 2
                 xs = rs - drs * cosw
                 if L2_j > 1e-12:
-                    vr_sq = 2.0 * (E_i - orbit_log(xs)) * xs ** 2 - L2_j
+                    vr_sq = 2.0 * (E_i - _ln(xs)) * xs ** 2 - L2_j
                     rvr = np.sqrt(np.maximum(0.0, vr_sq))
                     svr = sinw * xs / rvr
                     svr[0] = 2.0 * svr[1] - svr[2]
                     svr[-1] = 2.0 * svr[-2] - svr[-3]
                 else:
-                    vr_sq = 2.0 * (E_i - orbit_log(xs))
+                    vr_sq = 2.0 * (E_i - _ln(xs))
                     rvr = np.sqrt(np.maximum(0.0, vr_sq))
                     svr = sinw / rvr
                     svr[-1] = 2.0 * svr[-2] - svr[-3]
@@ -361,14 +368,14 @@ def compute_jacobian(g: Grids, Om1: np.ndarray) -> np.ndarray:
             E_val, L_val, om1 = g.E[iR, ie], g.L_m[iR, ie], Om1[iR, ie]
             j = 0.0
             if abs(r2 - r1) > 1e-12 and abs(L_val) > 1e-12:
-                V1, V2 = math.log(r1), math.log(r2)
+                V1, V2 = _ln(r1), _ln(r2)
                 dV1, dV2 = 1.0 / r1, 1.0 / r2
                 t1 = 2 * (E_val - V1) * r1 - dV1 * r1 ** 2
                 t2 = 2 * (E_val - V2) * r2 - dV2 * r2 ** 2
                 den = r2 ** 2 - r1 ** 2
                 j = 2 * abs(t1 * t2 / den) * rc / om1 / abs(L_val)
             if abs(L_val) <= 1e-12:
-                DelE = 2.0 * (E_val - math.log(r1))
+                DelE = 2.0 * (E_val - _ln(r1))
                 with np.errstate(all="ignore"):
                     j = math.sqrt(max(DelE, 0.0)) * (1.0 / r2) * 2 * rc / om1 if om1 != 0 else math.inf
                 if not math.isfinite(j):

@@ -12,7 +12,7 @@ def test_fixture_regenerates(name):
     ref = load_case(name)
     new = make(name, CASES[name])
     for k, v in ref.items():
-        if k == "config":
+        if k == "config" or k.startswith("sens_"):
             continue
         a, b = np.asarray(new[k]), np.asarray(v)
         assert a.shape == b.shape, k

@@ -179,19 +179,15 @@ def test_size_s_newton_matches_oracle(lib_path):
     from tests.conftest import ROOT
     c = K.load_config(os.path.join(ROOT, "configs", "size_s.toml"))
     c = K.load_model(c, os.path.join(ROOT, "models", "kalnajs_zang4.toml"))
+    ref = load_case("size_s")          # oracle outputs, tests/golden/make_size_s.py
     pc = K.precompute_all(c)
     r = K.newton_search(c, pc, None, K.GPUType.NVIDIA, "Float64")
-    g = c.grid
-    oc = O.OracleConfig(m=2, G=1.0, L0=1.0, n_zang=4, q1=7, NR=g.NR, Ne=g.Ne, Rc_min=g.Rc_min,
-                        Rc_max=g.Rc_max, v_min=g.v_min, N_alpha=g.N_alpha,
-                        alpha_max=g.alpha_max, l_min=g.l_min, l_max=g.l_max, nw=g.nw,
-                        nwa=g.nwa)
-    opc = O.precompute_all(oc)
-    ro = O.newton_search(lambda w: O.compute_det(opc, w), 2, c.reference.Omega_p,
-                         c.reference.gamma, tol=c.newton.tol, delta=c.newton.delta)
-    # M entries at the root, relative to max|M|
-    M = K.build_M_matrix(ro.omega, pc)
+    M = K.build_M_matrix(complex(ref["omega_root"][0]), pc)
+    d = K.compute_determinant_batched(ref["omegas"], pc)
     pc.close()
-    assert relmax(M, O.build_M(opc, ro.omega)) < 1e-11
-    assert r.converged and ro.converged
-    assert abs(r.Omega_p - ro.Omega_p) <= 1e-10 and abs(r.gamma - ro.gamma) <= 1e-10
+    assert r.converged and r.iterations == int(ref["iterations"][0])
+    assert abs(r.Omega_p - ref["root"][0]) <= 1e-10 and abs(r.gamma - ref["root"][1]) <= 1e-10
+    ok, worst = close(M, ref, "M0", 1e-11)
+    assert ok, (worst, relmax(M, ref["M0"]))
+    tol = 1e-11 * np.abs(ref["dets"]) + 4 * ref["sens_dets"]
+    assert np.all(np.abs(d - ref["dets"]) <= tol)
