@@ -236,7 +236,11 @@ def ours(args):
     t_pre = time.perf_counter() - t0
     lib, h = pc.ctx.lib, pc.ctx.h
     dims = pc.ctx.dims
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library launches on it and the events are
+    # recorded on it (the legacy default stream has handle 0, which the
+    # C ABI reads as "the context's own stream")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     _lib.check(h, lib.kls_set_stream(h, C.c_void_p(stream.cuda_stream)))
 
     nb = 3
