@@ -296,7 +296,7 @@ def ours(args):
     # ---- per-kernel durations (separate pass, library events on the same stream)
     _lib.check(h, lib.kls_enable_timing(h, 1))
     stage = np.zeros(4)
-    reps = max(2, min(args.steps, 4))
+    reps = max(1, min(args.steps, 4))
     for s in range(reps):
         dev_step(args.warmup + s)
         torch.cuda.synchronize()

@@ -21,10 +21,11 @@
 
 namespace {
 
+// not volatile: the scheduler may interleave independent DMMAs
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -163,13 +164,20 @@ contract_kernel(ContractParams P, const double* __restrict__ Wre, const double* 
         br[j] = dr * xr + di * xi;
         bi[j] = di * xr - dr * xi;
       }
+      // two passes of 32 independent DMMAs: each accumulator's second
+      // update issues 32 instructions after its first
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           dmma(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
-          dmma(cr[i][j][0], cr[i][j][1], na[i], bi[j]);
           dmma(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
+        }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          dmma(cr[i][j][0], cr[i][j][1], na[i], bi[j]);
           dmma(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
         }
     }
