@@ -360,7 +360,7 @@ def ours(args):
                    "K": dims.K, "omegas_per_step": nb, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (W table %.1f GB in HBM)" % (
                        2 * 8 * dims.K_pad * dims.N_alpha_pad / 1e9)},
-        "roofline": {"bound": "fp64", "kernel": "contract_kernel (DMMA m8n8k4)",
+        "roofline": {"bound": "tensor", "kernel": "contract_kernel (FP64 DMMA m8n8k4 on the tensor pipe)",
                      "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                      "frac": achieved / peak64,
                      "peak_note": "of measured: cuBLAS DGEMM 8192^3 best-of-5 in this run",

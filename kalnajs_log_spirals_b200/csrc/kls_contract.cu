@@ -222,16 +222,26 @@ __global__ void reduce_kernel(int Na, int Na_pad, int splits, double G,
 
 }  // namespace
 
-// The split count depends on the table only, never on the batch size, so a
-// determinant is bitwise identical whichever batch it is evaluated in.
+// The split count depends on the table and the device only, never on the
+// batch size, so a determinant is bitwise identical whichever batch it is
+// evaluated in.  It is chosen so that tiles * splits fills just under a
+// whole number q of waves (q the smallest giving >= 16 splits): then n
+// omegas take n * q rounds with every round nearly full.
 int kls_choose_splits(const kls_ctx* c) {
   const int tiles = (c->Na_pad / KLS_TILE) * (c->Na_pad / KLS_TILE);
-  const int target = 148 * 2 * 2;                   // two waves of 2 CTAs per SM at n = 1
-  int s = (target + tiles - 1) / tiles;
+  int sms = 148, per_sm = 2;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  cudaFuncSetAttribute(contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CT_SMEM);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contract_kernel, CT_THREADS,
+                                                    CT_SMEM) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int slots = sms * per_sm;
+  int q = std::max(1, (16 * tiles + slots - 1) / slots);
+  int s = (q * slots) / tiles;
   int64_t max_s = c->K_pad / (CT_BK * 8);            // at least 8 slabs per split
   if (s > max_s) s = (int)max_s;
   if (s < 1) s = 1;
-  if (s > 64) s = 64;
+  if (s > 256) s = 256;
   return s;
 }
 
