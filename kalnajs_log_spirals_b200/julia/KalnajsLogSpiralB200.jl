@@ -1,0 +1,143 @@
+# KalnajsLogSpiralB200.jl — Julia binding of libkls.so with the reference
+# package's API (src/KalnajsLogSpiral.jl:23-43).  It reuses the reference's
+# Configuration module for TOML parsing and replaces precompute_all,
+# to_device, compute_determinant(_batched), grid_scan and newton_search with
+# ccalls into libkls.so (include/kls.h).  Not exercised in this repository's
+# tests (no Julia toolchain in the build image); the Python mirror in
+# kalnajs_log_spirals_b200/api.py calls the same entry points.
+module KalnajsLogSpiralB200
+
+const LIBKLS = get(ENV, "LIBKLS", joinpath(@__DIR__, "..", "libkls.so"))
+
+const KLS_MODE_FP64 = Int32(0)
+const KLS_MODE_MIXED = Int32(1)
+
+# kls_config (include/kls.h), field order and C types
+struct KlsConfig
+    m::Int32; G::Float64; L0::Float64; n_zang::Int32; q1::Float64
+    NR::Int32; Ne::Int32; Rc_min::Float64; Rc_max::Float64; v_min::Float64
+    N_alpha::Int32; alpha_max::Float64; l_min::Int32; l_max::Int32
+    nw::Int32; nwa::Int32
+end
+
+struct KlsNewtonCfg
+    max_iter::Int32; tol::Float64; delta::Float64
+    use_line_search::Int32; max_line_search::Int32; mode::Int32
+end
+
+mutable struct KlsNewtonResult
+    Omega_p::Float64; gamma::Float64; omega_re::Float64; omega_im::Float64
+    det_re::Float64; det_im::Float64; iterations::Int32; converged::Int32; det_evals::Int32
+end
+KlsNewtonResult() = KlsNewtonResult(0, 0, 0, 0, 0, 0, 0, 0, 0)
+
+struct KlsScanCfg
+    n_Op::Int32; n_gamma::Int32; Omega_p_min::Float64; Omega_p_max::Float64
+    gamma_min::Float64; gamma_max::Float64; mode::Int32; batch::Int32
+end
+
+struct NewtonResult{T<:AbstractFloat}
+    Omega_p::T; gamma::T; omega::Complex{T}; det_val::Complex{T}
+    iterations::Int; converged::Bool; history::Matrix{T}
+end
+
+mutable struct PrecomputedData
+    handle::Ptr{Cvoid}
+    m::Int; G::Float64; N_alpha::Int; n_l::Int; NPh::Int
+end
+
+struct DevicePrecomputed
+    precomp::PrecomputedData
+    mode::Int32
+end
+
+function check(h, code)
+    code == 0 && return
+    msg = h == C_NULL ? unsafe_string(ccall((:kls_create_error, LIBKLS), Cstring, ())) :
+                        unsafe_string(ccall((:kls_last_error, LIBKLS), Cstring, (Ptr{Cvoid},), h))
+    error("libkls status $code: $msg")
+end
+
+function kls_config(config, model)
+    g = config.grid
+    KlsConfig(config.physics.m, config.physics.G, config.model.L0, config.model.n_zang,
+              Float64(config.model.q1), g.NR, g.Ne, g.Rc_min, g.Rc_max, g.v_min, g.N_alpha,
+              g.alpha_max, g.l_min, g.l_max, g.nw, g.nwa)
+end
+
+"precompute_all (BasisFunctions.jl:73): grids, orbits, W_l, N_m on the GPU."
+function precompute_all(config, model, backend; verbose::Bool=false, device::Int=0)
+    cfg = Ref(kls_config(config, model))
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(C_NULL, ccall((:kls_create, LIBKLS), Cint, (Ref{KlsConfig}, Cint, Ref{Ptr{Cvoid}}),
+                        cfg, device, h))
+    check(h[], ccall((:kls_precompute, LIBKLS), Cint, (Ptr{Cvoid},), h[]))
+    pc = PrecomputedData(h[], config.physics.m, config.physics.G, config.grid.N_alpha,
+                         config.grid.l_max - config.grid.l_min + 1, config.grid.NR * config.grid.Ne)
+    finalizer(p -> ccall((:kls_destroy, LIBKLS), Cint, (Ptr{Cvoid},), p.handle), pc)
+    return pc
+end
+
+"to_device (BasisFunctions.jl:397): Float64 -> plain FP64, Float32 -> split-BF16 form."
+function to_device(precomp::PrecomputedData, gpu_type, Tgpu::Type)
+    mode = Tgpu === Float64 ? KLS_MODE_FP64 : KLS_MODE_MIXED
+    if mode == KLS_MODE_MIXED
+        check(precomp.handle, ccall((:kls_prepare_mixed, LIBKLS), Cint, (Ptr{Cvoid},), precomp.handle))
+    end
+    return DevicePrecomputed(precomp, mode)
+end
+
+modeof(d) = d === nothing ? KLS_MODE_FP64 : d.mode
+
+"compute_determinant_batched (MatrixBuilder.jl:215)."
+function compute_determinant_batched(omegas::Vector{ComplexF64}, precomp::PrecomputedData,
+                                     devprecomp, gpu_type, Tcpu::Type; batch_size::Int=100)
+    out = Vector{ComplexF64}(undef, length(omegas))
+    for s in 1:batch_size:length(omegas)
+        e = min(s + batch_size - 1, length(omegas))
+        om = omegas[s:e]
+        det = Vector{ComplexF64}(undef, length(om))
+        check(precomp.handle, ccall((:kls_det_batch, LIBKLS), Cint,
+              (Ptr{Cvoid}, Ptr{ComplexF64}, Cint, Cint, Ptr{ComplexF64}, Ptr{Float64}),
+              precomp.handle, om, length(om), modeof(devprecomp), det, C_NULL))
+        out[s:e] .= det
+    end
+    return out
+end
+
+"compute_determinant (MatrixBuilder.jl:197)."
+compute_determinant(omega::ComplexF64, precomp::PrecomputedData, devprecomp, gpu_type, Tcpu::Type) =
+    compute_determinant_batched([omega], precomp, devprecomp, gpu_type, Tcpu)[1]
+
+"grid_scan (GridScan.jl:25) -> (det_grid, Omega_p_init, gamma_init)."
+function grid_scan(config, precomp::PrecomputedData, devprecomp, gpu_type, Tcpu::Type;
+                   verbose::Bool=false, gpu_devices::Vector{Int}=Int[])
+    s = config.scan
+    sc = Ref(KlsScanCfg(s.n_Op, s.n_gamma, s.Omega_p_min, s.Omega_p_max, s.gamma_min,
+                        s.gamma_max, modeof(devprecomp), 0))
+    det_grid = Matrix{ComplexF64}(undef, s.n_gamma, s.n_Op)
+    Op0 = Ref(0.0); g0 = Ref(0.0)
+    check(precomp.handle, ccall((:kls_scan, LIBKLS), Cint,
+          (Ptr{Cvoid}, Ref{KlsScanCfg}, Ptr{ComplexF64}, Ptr{Float64}, Ref{Float64}, Ref{Float64}),
+          precomp.handle, sc, det_grid, C_NULL, Op0, g0))
+    return det_grid, Op0[], g0[]
+end
+
+"newton_search (NewtonSolver.jl:36) -> NewtonResult."
+function newton_search(config, precomp::PrecomputedData, devprecomp, gpu_type, Tcpu::Type,
+                       Omega_p_init::Real, gamma_init::Real; verbose::Bool=false)
+    n = config.newton
+    nc = Ref(KlsNewtonCfg(n.max_iter, n.tol, n.delta, n.use_line_search, n.max_line_search,
+                          modeof(devprecomp)))
+    res = Ref(KlsNewtonResult())
+    hist = zeros(Float64, 3, n.max_iter)          # row-major (iter, 3) on the C side
+    check(precomp.handle, ccall((:kls_newton, LIBKLS), Cint,
+          (Ptr{Cvoid}, Cdouble, Cdouble, Ref{KlsNewtonCfg}, Ref{KlsNewtonResult}, Ptr{Float64}),
+          precomp.handle, Omega_p_init, gamma_init, nc, res, hist))
+    r = res[]
+    h = permutedims(hist[:, 1:r.iterations])
+    return NewtonResult{Float64}(r.Omega_p, r.gamma, complex(r.omega_re, r.omega_im),
+                                 complex(r.det_re, r.det_im), r.iterations, r.converged != 0, h)
+end
+
+end # module
