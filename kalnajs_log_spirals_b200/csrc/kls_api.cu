@@ -113,7 +113,11 @@ int run_batch(kls_ctx* c, int n, int mode, bool export_M) {
     return kls_fail(c, KLS_ERR_CONFIG, "unknown precision mode");
   }
   if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[2], c->stream));
-  if ((r = kls_run_reduce(c, n, splits, export_M))) return r;
+  if (mode == KLS_MODE_MIXED) {
+    if ((r = kls_mixed_reduce(c, n, export_M))) return r;
+  } else if ((r = kls_run_reduce(c, n, splits, export_M))) {
+    return r;
+  }
   if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[3], c->stream));
   if ((r = kls_run_lu(c, n))) return r;
   if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[4], c->stream));
@@ -158,6 +162,7 @@ int det_batch_host(kls_ctx* c, const double* omega_ri, int n, int mode, double* 
       KLS_CK(c, cudaMemcpyAsync(log_abs + b, c->d_logabs, nb * sizeof(double),
                                 cudaMemcpyDeviceToHost, c->stream));
     KLS_CK(c, cudaStreamSynchronize(c->stream));
+    if (mode == KLS_MODE_MIXED && (r = kls_mixed_check(c))) return r;
     if ((r = collect_timing(c))) return r;
   }
   return KLS_OK;
@@ -419,6 +424,7 @@ int kls_build_M(kls_ctx* c, double wr, double wi, int mode, double* M) {
   KLS_CK(c, cudaMemcpyAsync(h.data(), c->d_M, h.size() * sizeof(double2), cudaMemcpyDeviceToHost,
                             c->stream));
   KLS_CK(c, cudaStreamSynchronize(c->stream));
+  if (mode == KLS_MODE_MIXED && (r = kls_mixed_check(c))) return r;
   const int N = c->Na;
   for (int b = 0; b < N; ++b)
     for (int a = 0; a < N; ++a) {   // device [b][a] -> host column-major (b + N a)

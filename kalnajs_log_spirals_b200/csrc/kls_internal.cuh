@@ -111,4 +111,6 @@ int kls_choose_splits(const kls_ctx* c);
 // mixed-precision path (kls_mixed.cu)
 int kls_mixed_prepare(kls_ctx* c);
 int kls_mixed_contract(kls_ctx* c, int n, int splits);
+int kls_mixed_reduce(kls_ctx* c, int n, bool export_M);
+int kls_mixed_check(kls_ctx* c);     // pipeline timeout flag of the last launches
 void kls_mixed_free(kls_ctx* c);

@@ -1,17 +1,576 @@
-// Split-BF16 tensor-core contraction (KLS_MODE_MIXED).
+// Split-BF16 tensor-core contraction (KLS_MODE_MIXED) on tcgen05 / TMEM.
+//
+// M(omega) = W^T diag(w(omega)) conj(W) as one real GEMM per omega:
+//
+//   X = [Re W | Im W]                 (rows c in [0, 2 Npad), K-major, omega-independent)
+//   Y = [U_r | U_i], U = w * conj(W)  (rows n = 2 a + part, K-major, per omega)
+//   P = X Y^T (2 Npad x 2 Npad, FP32 in TMEM)
+//   M_r[b,a] = P[b, 2a] - P[Npad+b, 2a+1],  M_i[b,a] = P[b, 2a+1] + P[Npad+b, 2a]
+//
+// Both operands are split error-free into BF16 high and low parts
+// (x = hi + lo to ~2^-17 relative) and P accumulates hi*hi + hi*lo + lo*hi
+// with FP32 accumulation (the lo*lo term, ~2^-18 relative, is dropped).
+// The weights w(omega), the split-K reduction, the LU and the determinant
+// stay FP64.
+//
+// Table: Xh/Xl [2 Npad][K_pad] BF16, built once by split_table_kernel from
+// the FP64 table.  Contraction CTA (one per SM, 12 warps):
+//   warp 0      TMA: X tile 128 rows x 64 k (hi and lo), 128B swizzle
+//   warp 1      MMA issuer: tcgen05.mma kind::f16, M=128 N=128 K=16,
+//               3 products per k-step per omega, accumulators in TMEM
+//   warp 2      TMEM allocation / release
+//   warps 4-11  producers: U = w conj(W) in FP32 from the table, split to
+//               BF16 hi/lo, written 128B-swizzled (K-major) for 2 omegas
+//   warps 0-3   epilogue: tcgen05.ld -> FP32 partial tiles per K split
+// Pipeline: 2 shared-memory stages with full/empty mbarriers; every wait is
+// bounded by %globaltimer and aborts the CTA cleanly (error flag, TMEM freed).
 #include "kls_internal.cuh"
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <algorithm>
+#include <cstring>
 
-struct kls_mixed {};
+namespace {
 
-int kls_mixed_prepare(kls_ctx* c) {
-  return kls_fail(c, KLS_ERR_UNSUPPORTED, "mixed-precision contraction not built yet");
+constexpr int MX_BM = 128;                 // X rows per CTA
+constexpr int MX_AB = 64;                  // alphas per CTA -> 128 Y rows per omega
+constexpr int MX_BN = 2 * MX_AB;           // 128
+constexpr int MX_OMEGA = 2;                // omegas per CTA
+constexpr int MX_BK = 64;                  // k per stage: one 128-byte swizzle row of BF16
+constexpr int MX_STAGES = 2;
+constexpr int MX_PRODUCERS = 256;          // warps 4..11
+constexpr int MX_THREADS = 128 + MX_PRODUCERS;
+constexpr int MX_TILE_X = MX_BM * MX_BK * 2;            // 16 KB per part
+constexpr int MX_TILE_Y = MX_BN * MX_BK * 2;            // 16 KB per part per omega
+constexpr int MX_STAGE_BYTES = 2 * MX_TILE_X + 2 * MX_OMEGA * MX_TILE_Y;   // 96 KB
+constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + 1024;       // + alignment
+constexpr int MX_TMEM_COLS = 256;          // MX_OMEGA * MX_BN fp32 columns
+constexpr unsigned long long MX_WAIT_NS = 2000000000ull;   // 2 s per wait
+
+struct MixedParams {
+  int Npad;            // N_alpha_pad
+  int rows;            // 2 * Npad
+  int64_t K_pad;
+  int nkb_total;       // K_pad / MX_BK
+  int kb_per_split;
+  int splits;
+  int n_omega;
+  int tiles_m, tiles_a;
+};
+
+// ---- small PTX helpers ----------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t a) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false when the CTA is aborting or the wait timed out.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort,
+                                          int* err, int code) {
+  unsigned long long t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if (mbar_try(a, parity)) return true;
+    if (*abort) return false;
+    if ((it & 63) == 0) {
+      unsigned long long t = globaltimer();
+      if (t0 == 0) t0 = t;
+      else if (t - t0 > MX_WAIT_NS) {
+        *abort = 1;
+        atomicCAS(err, 0, code);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-int kls_mixed_contract(kls_ctx* c, int, int) {
-  return kls_fail(c, KLS_ERR_UNSUPPORTED, "mixed-precision contraction not built yet");
+// K-major, 128-byte swizzle UMMA shared-memory descriptor (sm100 format):
+// start >> 4 in [0,14), LBO >> 4 in [16,30) (unused here), SBO = 1024 B
+// (8 rows of 128 B) >> 4 in [32,46), version 1 at [46,48), layout
+// SWIZZLE_128B = 2 at [61,64).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)2 << 61;
+  return d;
+}
+// kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major,
+// N >> 3 at [17,23), M >> 4 at [24,29).
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                     uint32_t acc) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
+}
+#define TMEM_LD32(taddr, r)                                                                      \
+  asm volatile(                                                                                  \
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13," \
+      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"        \
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),     \
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),              \
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),           \
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),           \
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),           \
+        "=r"(r[31])                                                                              \
+      : "r"(taddr))
+
+// ---- error-free split of the FP64 table --------------------------------------
+__device__ __forceinline__ void split2(double v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn((float)v);
+  lo = __float2bfloat16_rn((float)(v - (double)__bfloat162float(hi)));
+}
+
+// [K_pad][Npad] FP64 planes -> X{h,l}[2 Npad][K_pad] (row a: Re, row Npad + a: Im)
+__global__ void split_table_kernel(const double* __restrict__ Wre, const double* __restrict__ Wim,
+                                   int Npad, int64_t K_pad, __nv_bfloat16* __restrict__ Xh,
+                                   __nv_bfloat16* __restrict__ Xl) {
+  __shared__ double tr[32][33], ti[32][33];
+  const int64_t k0 = (int64_t)blockIdx.x * 32;
+  const int a0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int i = ty; i < 32; i += 8) {
+    tr[i][tx] = Wre[(size_t)(k0 + i) * Npad + a0 + tx];
+    ti[i][tx] = Wim[(size_t)(k0 + i) * Npad + a0 + tx];
+  }
+  __syncthreads();
+  for (int i = ty; i < 32; i += 8) {
+    __nv_bfloat16 h, l;
+    split2(tr[tx][i], h, l);
+    size_t o = (size_t)(a0 + i) * K_pad + k0 + tx;
+    Xh[o] = h;
+    Xl[o] = l;
+    split2(ti[tx][i], h, l);
+    o = (size_t)(Npad + a0 + i) * K_pad + k0 + tx;
+    Xh[o] = h;
+    Xl[o] = l;
+  }
+}
+
+// ---- contraction -------------------------------------------------------------
+__device__ __forceinline__ float bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
+__device__ __forceinline__ uint32_t pack_split(float a, float b, uint32_t& lo) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);          // .x = a (low half)
+  float ha = __low2float(h), hb = __high2float(h);
+  __nv_bfloat162 l = __floats2bfloat162_rn(a - ha, b - hb);
+  lo = *reinterpret_cast<uint32_t*>(&l);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+// byte offset of the 16-byte chunk (row n, k-chunk c) in a K-major SW128 tile
+__device__ __forceinline__ uint32_t sw128_off(int n, int c) {
+  return (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4));
+}
+
+__global__ void __launch_bounds__(MX_THREADS, 1)
+mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
+                      const __grid_constant__ CUtensorMap tm_l, MixedParams P,
+                      const __nv_bfloat16* __restrict__ Xh, const __nv_bfloat16* __restrict__ Xl,
+                      const double2* __restrict__ wt, float* __restrict__ part,
+                      int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_full_x[MX_STAGES], bar_full_y[MX_STAGES],
+      bar_empty[MX_STAGES], bar_done;
+  __shared__ uint32_t s_tmem;
+  __shared__ volatile int s_abort;
+
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tile = blockIdx.x, split = blockIdx.y, grp = blockIdx.z;
+  const int tm = tile / P.tiles_a, ta = tile % P.tiles_a;
+  const int m0 = tm * MX_BM;             // first X row
+  const int a0 = ta * MX_AB;             // first alpha
+  const int om0 = grp * MX_OMEGA;
+  const int n_om = min(MX_OMEGA, P.n_omega - om0);
+  const int kb0 = split * P.kb_per_split;
+  const int nkb = max(0, min(P.nkb_total, kb0 + P.kb_per_split) - kb0);
+
+  auto xh_s = [&](int s) { return smem + (size_t)s * MX_STAGE_BYTES; };
+  auto xl_s = [&](int s) { return smem + (size_t)s * MX_STAGE_BYTES + MX_TILE_X; };
+  auto yh_s = [&](int s, int j) {
+    return smem + (size_t)s * MX_STAGE_BYTES + 2 * MX_TILE_X + (size_t)j * MX_TILE_Y;
+  };
+  auto yl_s = [&](int s, int j) {
+    return smem + (size_t)s * MX_STAGE_BYTES + 2 * MX_TILE_X + (size_t)(MX_OMEGA + j) * MX_TILE_Y;
+  };
+
+  if (tid == 0) {
+    s_abort = 0;
+    for (int s = 0; s < MX_STAGES; ++s) {
+      mbar_init(smem_u32(&bar_full_x[s]), 1);
+      mbar_init(smem_u32(&bar_full_y[s]), MX_PRODUCERS);
+      mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    mbar_init(smem_u32(&bar_done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2 && nkb > 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(MX_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  if (nkb > 0) {
+    if (warp == 0) {
+      // ---------------- TMA producer for the X tiles
+      if (lane == 0) {
+        int issued = 0;
+        for (int i = 0; i < nkb; ++i) {
+          const int s = i % MX_STAGES, r = i / MX_STAGES;
+          if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 1)) break;
+          const uint32_t fb = smem_u32(&bar_full_x[s]);
+          mbar_arrive_tx(fb, 2 * MX_TILE_X);
+          const int kx = (kb0 + i) * MX_BK;
+          tma_load_2d(smem_u32(xh_s(s)), &tm_h, kx, m0, fb);
+          tma_load_2d(smem_u32(xl_s(s)), &tm_l, kx, m0, fb);
+          issued = i + 1;
+        }
+        // the last load into each stage must land before the CTA can exit
+        // (immediate on the normal path, bounded on the abort path)
+        for (int i = max(0, issued - MX_STAGES); i < issued; ++i) {
+          volatile int never = 0;
+          mbar_wait(smem_u32(&bar_full_x[i % MX_STAGES]), (i / MX_STAGES) & 1, &never, err, 6);
+        }
+      }
+    } else if (warp == 1) {
+      // ---------------- MMA issuer
+      if (lane == 0) {
+        const uint32_t idesc = idesc_bf16(MX_BM, MX_BN);
+        for (int i = 0; i < nkb; ++i) {
+          const int s = i % MX_STAGES, r = i / MX_STAGES;
+          if (!mbar_wait(smem_u32(&bar_full_x[s]), r & 1, &s_abort, err, 2)) break;
+          if (!mbar_wait(smem_u32(&bar_full_y[s]), r & 1, &s_abort, err, 3)) break;
+          tc_fence_after();
+          const uint64_t dxh = sw128_desc(smem_u32(xh_s(s)));
+          const uint64_t dxl = sw128_desc(smem_u32(xl_s(s)));
+#pragma unroll
+          for (int kk = 0; kk < MX_BK / 16; ++kk) {
+            const uint64_t koff = (uint64_t)(kk * 32) >> 4;    // +32 bytes per k-step
+            for (int j = 0; j < n_om; ++j) {
+              const uint32_t d = tmem + (uint32_t)(j * MX_BN);
+              const uint64_t dyh = sw128_desc(smem_u32(yh_s(s, j))) + koff;
+              const uint64_t dyl = sw128_desc(smem_u32(yl_s(s, j))) + koff;
+              const uint32_t acc0 = (i > 0 || kk > 0) ? 1u : 0u;
+              umma(d, dxh + koff, dyh, idesc, acc0);
+              umma(d, dxh + koff, dyl, idesc, 1u);
+              umma(d, dxl + koff, dyh, idesc, 1u);
+            }
+          }
+          umma_commit(smem_u32(&bar_empty[s]));
+        }
+        // completion of every issued MMA (also on the abort path)
+        umma_commit(smem_u32(&bar_done));
+      }
+    } else if (warp >= 4) {
+      // ---------------- Y producers: U = w conj(W), split, swizzled store
+      const int pt = tid - 128;                 // 0..255
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % MX_STAGES, r = i / MX_STAGES;
+        if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)) break;
+        const int64_t kbase = (int64_t)(kb0 + i) * MX_BK;
+        // 64 alphas x 8 chunks of 8 k = 512 units per omega, 2 per thread
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int unit = pt + u * MX_PRODUCERS;
+          const int al = unit >> 3, c = unit & 7;
+          const int a = a0 + al;
+          const int64_t k = kbase + c * 8;
+          const uint4 ah = *reinterpret_cast<const uint4*>(Xh + (size_t)a * P.K_pad + k);
+          const uint4 alw = *reinterpret_cast<const uint4*>(Xl + (size_t)a * P.K_pad + k);
+          const uint4 bh = *reinterpret_cast<const uint4*>(Xh + (size_t)(P.Npad + a) * P.K_pad + k);
+          const uint4 blw = *reinterpret_cast<const uint4*>(Xl + (size_t)(P.Npad + a) * P.K_pad + k);
+          const uint32_t A_h[4] = {ah.x, ah.y, ah.z, ah.w}, A_l[4] = {alw.x, alw.y, alw.z, alw.w};
+          const uint32_t B_h[4] = {bh.x, bh.y, bh.z, bh.w}, B_l[4] = {blw.x, blw.y, blw.z, blw.w};
+          float wr[8], wi[8];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            wr[2 * q] = bf_lo(A_h[q]) + bf_lo(A_l[q]);
+            wr[2 * q + 1] = bf_hi(A_h[q]) + bf_hi(A_l[q]);
+            wi[2 * q] = bf_lo(B_h[q]) + bf_lo(B_l[q]);
+            wi[2 * q + 1] = bf_hi(B_h[q]) + bf_hi(B_l[q]);
+          }
+          for (int j = 0; j < n_om; ++j) {
+            const double2* wz = wt + (size_t)(om0 + j) * P.K_pad + k;
+            uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const double2 w0 = wz[2 * q], w1 = wz[2 * q + 1];
+              const float d0r = (float)w0.x, d0i = (float)w0.y;
+              const float d1r = (float)w1.x, d1i = (float)w1.y;
+              // w conj(W) = (dr Wr + di Wi) + i (di Wr - dr Wi)
+              const float ur0 = d0r * wr[2 * q] + d0i * wi[2 * q];
+              const float ui0 = d0i * wr[2 * q] - d0r * wi[2 * q];
+              const float ur1 = d1r * wr[2 * q + 1] + d1i * wi[2 * q + 1];
+              const float ui1 = d1i * wr[2 * q + 1] - d1r * wi[2 * q + 1];
+              rh[q] = pack_split(ur0, ur1, rl[q]);
+              ih[q] = pack_split(ui0, ui1, il[q]);
+            }
+            const uint32_t offr = sw128_off(2 * al, c), offi = sw128_off(2 * al + 1, c);
+            *reinterpret_cast<uint4*>(yh_s(s, j) + offr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+            *reinterpret_cast<uint4*>(yl_s(s, j) + offr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+            *reinterpret_cast<uint4*>(yh_s(s, j) + offi) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+            *reinterpret_cast<uint4*>(yl_s(s, j) + offi) = make_uint4(il[0], il[1], il[2], il[3]);
+          }
+        }
+        fence_proxy_async();
+        mbar_arrive(smem_u32(&bar_full_y[s]));
+      }
+    }
+  }
+  __syncwarp();
+
+  // ---------------- epilogue: TMEM -> FP32 partial tiles
+  const size_t R = (size_t)P.rows;
+  if (warp < 4) {
+    bool ok = true;
+    if (nkb > 0) {
+      // every issued MMA has completed once bar_done fires, also when aborting
+      volatile int never = 0;
+      ok = mbar_wait(smem_u32(&bar_done), 0, &never, err, 5);
+      ok = __all_sync(0xffffffffu, ok && !s_abort);
+    }
+    tc_fence_after();
+    const int row = m0 + warp * 32 + lane;
+    for (int j = 0; j < n_om; ++j) {
+      float* out = part + (((size_t)(om0 + j) * P.splits + split) * R + row) * R + 2 * a0;
+      for (int cc = 0; cc < MX_BN / 32; ++cc) {
+        uint32_t v[32];
+        if (nkb > 0 && ok) {
+          const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * MX_BN + cc * 32);
+          TMEM_LD32(taddr, v);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        } else {
+#pragma unroll
+          for (int q = 0; q < 32; ++q) v[q] = 0u;
+        }
+        float4* o4 = reinterpret_cast<float4*>(out + cc * 32);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          o4[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                              __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2 && nkb > 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(MX_TMEM_COLS));
+  }
+}
+
+// ---- reduction of the FP32 partial tiles -----------------------------------------
+__global__ void mixed_reduce_kernel(int Na, int Npad, int splits, double G,
+                                    const double* __restrict__ Nk, const float* __restrict__ part,
+                                    double2* __restrict__ A, double2* __restrict__ Mout) {
+  const int z = blockIdx.y;
+  const size_t R = 2 * (size_t)Npad;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
+    const int b = e / Na, a = e % Na;
+    double mr = 0.0, mi = 0.0;
+    for (int s = 0; s < splits; ++s) {
+      const float* P = part + ((size_t)z * splits + s) * R * R;
+      const double pr_r = P[(size_t)b * R + 2 * a], pr_i = P[(size_t)b * R + 2 * a + 1];
+      const double pi_r = P[(size_t)(Npad + b) * R + 2 * a];
+      const double pi_i = P[(size_t)(Npad + b) * R + 2 * a + 1];
+      mr += pr_r - pi_i;
+      mi += pr_i + pi_r;
+    }
+    const double n = Nk[a];
+    const double Mr = (mr * G) * n, Mi = (mi * G) * n;
+    A[(size_t)z * Na * Na + e] = make_double2((a == b ? 1.0 : 0.0) - Mr, -Mi);
+    if (Mout && z == 0) Mout[e] = make_double2(Mr, Mi);
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+}  // namespace
+
+struct kls_mixed {
+  __nv_bfloat16* Xh = nullptr;
+  __nv_bfloat16* Xl = nullptr;
+  CUtensorMap tm_h, tm_l;
+  float* part = nullptr;
+  size_t part_elems = 0;
+  int* err = nullptr;
+  int splits = 1;
+};
+
+static int mixed_splits(const kls_ctx* c) {
+  const int tiles = (2 * c->Na_pad / MX_BM) * (c->Na_pad / MX_AB);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  int q = std::max(1, (16 * tiles + sms - 1) / sms);
+  int s = (q * sms) / tiles;
+  int nkb = (int)(c->K_pad / MX_BK);
+  s = std::max(1, std::min(s, nkb));
+  return s;
+}
+
+int kls_mixed_prepare(kls_ctx* c) {
+  if (c->mixed) return KLS_OK;
+  if (!c->precomputed) return kls_fail(c, KLS_ERR_STATE, "kls_precompute has not run");
+  if ((2 * c->Na_pad) % MX_BM != 0 || c->Na_pad % MX_AB != 0 || c->K_pad % MX_BK != 0)
+    return kls_fail(c, KLS_ERR_CONFIG, "table padding incompatible with the mixed tiles");
+  kls_mixed* m = new kls_mixed();
+  const size_t rows = 2 * (size_t)c->Na_pad;
+  const size_t n = rows * (size_t)c->K_pad;
+  cudaError_t e;
+  if ((e = cudaMalloc(&m->Xh, n * sizeof(__nv_bfloat16))) != cudaSuccess ||
+      (e = cudaMalloc(&m->Xl, n * sizeof(__nv_bfloat16))) != cudaSuccess ||
+      (e = cudaMalloc(&m->err, sizeof(int))) != cudaSuccess) {
+    cudaFree(m->Xh); cudaFree(m->Xl); cudaFree(m->err);
+    delete m;
+    return kls_cuda_fail(c, e, "cudaMalloc (split table)");
+  }
+  c->device_bytes += (int64_t)(2 * n * sizeof(__nv_bfloat16));
+  c->mixed = m;
+  KLS_CK(c, cudaMemsetAsync(m->err, 0, sizeof(int), c->stream));
+  dim3 grid((unsigned)(c->K_pad / 32), c->Na_pad / 32);
+  split_table_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(c->d_Wre, c->d_Wim, c->Na_pad, c->K_pad,
+                                                          m->Xh, m->Xl);
+  KLS_LAUNCHED(c);
+  // TMA descriptors over X{h,l}: dims {K_pad, rows}, box {64 k, 128 rows}, 128B swizzle
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  KLS_CK(c, cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (!fn || q != cudaDriverEntryPointSuccess)
+    return kls_fail(c, KLS_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  EncodeTiledFn encode = (EncodeTiledFn)fn;
+  cuuint64_t dims[2] = {(cuuint64_t)c->K_pad, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)c->K_pad * sizeof(__nv_bfloat16)};
+  cuuint32_t box[2] = {MX_BK, MX_BM};
+  cuuint32_t estr[2] = {1, 1};
+  for (int t = 0; t < 2; ++t) {
+    CUresult r = encode(t == 0 ? &m->tm_h : &m->tm_l, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                        t == 0 ? (void*)m->Xh : (void*)m->Xl, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return kls_fail(c, KLS_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  }
+  m->splits = mixed_splits(c);
+  KLS_CK(c, cudaFuncSetAttribute(mixed_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)MX_SMEM));
+  KLS_CK(c, cudaStreamSynchronize(c->stream));
+  return KLS_OK;
+}
+
+int kls_mixed_contract(kls_ctx* c, int n, int) {
+  kls_mixed* m = c->mixed;
+  const size_t R = 2 * (size_t)c->Na_pad;
+  const size_t need = (size_t)n * m->splits * R * R;
+  if (need > m->part_elems) {
+    cudaFree(m->part);
+    m->part = nullptr;
+    m->part_elems = 0;
+    KLS_CK(c, cudaMalloc(&m->part, need * sizeof(float)));
+    m->part_elems = need;
+  }
+  MixedParams P{};
+  P.Npad = c->Na_pad;
+  P.rows = (int)R;
+  P.K_pad = c->K_pad;
+  P.nkb_total = (int)(c->K_pad / MX_BK);
+  P.splits = m->splits;
+  P.kb_per_split = (P.nkb_total + m->splits - 1) / m->splits;
+  P.n_omega = n;
+  P.tiles_m = (int)(R / MX_BM);
+  P.tiles_a = c->Na_pad / MX_AB;
+  dim3 grid(P.tiles_m * P.tiles_a, m->splits, (n + MX_OMEGA - 1) / MX_OMEGA);
+  mixed_contract_kernel<<<grid, MX_THREADS, MX_SMEM, c->stream>>>(m->tm_h, m->tm_l, P, m->Xh,
+                                                                  m->Xl, c->d_wt, m->part, m->err);
+  KLS_LAUNCHED(c);
+  return KLS_OK;
+}
+
+int kls_mixed_reduce(kls_ctx* c, int n, bool export_M) {
+  kls_mixed* m = c->mixed;
+  int blocks = std::min((c->Na * c->Na + 255) / 256, 1024);
+  mixed_reduce_kernel<<<dim3(blocks, n), 256, 0, c->stream>>>(
+      c->Na, c->Na_pad, m->splits, c->cfg.G, c->d_N, m->part, c->d_A, export_M ? c->d_M : nullptr);
+  KLS_LAUNCHED(c);
+  return KLS_OK;
+}
+
+int kls_mixed_check(kls_ctx* c) {
+  if (!c->mixed) return KLS_OK;
+  int h = 0;
+  KLS_CK(c, cudaMemcpy(&h, c->mixed->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    cudaMemset(c->mixed->err, 0, sizeof(int));
+    return kls_fail(c, KLS_ERR_CUDA, "mixed contraction pipeline timed out (code " +
+                                         std::to_string(h) + ")");
+  }
+  return KLS_OK;
 }
 
 void kls_mixed_free(kls_ctx* c) {
+  if (!c->mixed) return;
+  cudaFree(c->mixed->Xh);
+  cudaFree(c->mixed->Xl);
+  cudaFree(c->mixed->part);
+  cudaFree(c->mixed->err);
   delete c->mixed;
   c->mixed = nullptr;
 }
