@@ -4,26 +4,31 @@
 //
 //   X = [Re W | Im W]                 (rows c in [0, 2 Npad), K-major, omega-independent)
 //   Y = [U_r | U_i], U = w * conj(W)  (rows n = 2 a + part, K-major, per omega)
-//   P = X Y^T (2 Npad x 2 Npad, FP32 in TMEM)
+//   P = X Y^T (2 Npad x 2 Npad)
 //   M_r[b,a] = P[b, 2a] - P[Npad+b, 2a+1],  M_i[b,a] = P[b, 2a+1] + P[Npad+b, 2a]
 //
 // Both operands are split error-free into BF16 high and low parts
-// (x = hi + lo to ~2^-17 relative) and P accumulates hi*hi + hi*lo + lo*hi
-// with FP32 accumulation (the lo*lo term, ~2^-18 relative, is dropped).
-// The weights w(omega), the split-K reduction, the LU and the determinant
-// stay FP64.
+// (x = hi + lo to ~2^-17 relative) and P accumulates hi*hi + hi*lo + lo*hi on
+// the tensor cores with FP32 accumulation in TMEM (the lo*lo term, ~2^-18
+// relative, is dropped).  FP32 accumulation error grows with the length of
+// the accumulation chain, so TMEM is flushed every MX_CHUNK_KB k-blocks into
+// an FP64 partial in global memory (deterministic order); the split-K
+// reduction, the weights w(omega), the LU and the determinant are FP64.
 //
 // Table: Xh/Xl [2 Npad][K_pad] BF16, built once by split_table_kernel from
-// the FP64 table.  Contraction CTA (one per SM, 12 warps):
-//   warp 0      TMA: X tile 128 rows x 64 k (hi and lo), 128B swizzle
-//   warp 1      MMA issuer: tcgen05.mma kind::f16, M=128 N=128 K=16,
-//               3 products per k-step per omega, accumulators in TMEM
-//   warp 2      TMEM allocation / release
-//   warps 4-11  producers: U = w conj(W) in FP32 from the table, split to
-//               BF16 hi/lo, written 128B-swizzled (K-major) for 2 omegas
-//   warps 0-3   epilogue: tcgen05.ld -> FP32 partial tiles per K split
-// Pipeline: 2 shared-memory stages with full/empty mbarriers; every wait is
-// bounded by %globaltimer and aborts the CTA cleanly (error flag, TMEM freed).
+// the FP64 table.  Contraction CTA (one per SM, 16 warps):
+//   warp 0       TMA: X tile 128 rows x 64 k (hi, lo; 128B swizzle) and the
+//                FP32 weights of the stage (bulk copy)
+//   warp 1       MMA issuer: tcgen05.mma kind::f16 M=128 N=128 K=16, 3
+//                products per k-step per omega, 2 TMEM accumulator buffers
+//   warp 2       TMEM allocation / release (512 columns)
+//   warps 4-11   producers: U = w conj(W) in FP32 from the table rows of the
+//                CTA's alpha block (prefetched one stage ahead), split to
+//                BF16 hi/lo, stored 128B-swizzled (K-major) for 2 omegas
+//   warps 12-15  drain: per chunk, tcgen05.ld -> add into the FP64 partial
+// Every mbarrier wait is bounded by %globaltimer; a timeout aborts the CTA
+// (error flag for the host), and TMEM is released only after all issued MMAs
+// have completed.
 #include "kls_internal.cuh"
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -38,13 +43,17 @@ constexpr int MX_BN = 2 * MX_AB;           // 128
 constexpr int MX_OMEGA = 2;                // omegas per CTA
 constexpr int MX_BK = 64;                  // k per stage: one 128-byte swizzle row of BF16
 constexpr int MX_STAGES = 2;
+constexpr int MX_CHUNK_KB = 32;            // k-blocks per TMEM accumulation chunk
 constexpr int MX_PRODUCERS = 256;          // warps 4..11
-constexpr int MX_THREADS = 128 + MX_PRODUCERS;
+constexpr int MX_DRAIN0 = 12;              // first drain warp (warps 12..15)
+constexpr int MX_THREADS = 512;
 constexpr int MX_TILE_X = MX_BM * MX_BK * 2;            // 16 KB per part
 constexpr int MX_TILE_Y = MX_BN * MX_BK * 2;            // 16 KB per part per omega
-constexpr int MX_STAGE_BYTES = 2 * MX_TILE_X + 2 * MX_OMEGA * MX_TILE_Y;   // 96 KB
-constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + 1024;       // + alignment
-constexpr int MX_TMEM_COLS = 256;          // MX_OMEGA * MX_BN fp32 columns
+constexpr int MX_W_BYTES = MX_BK * 8;                   // float2 weights per omega per stage
+constexpr int MX_STAGE_BYTES = 2 * MX_TILE_X + 2 * MX_OMEGA * MX_TILE_Y + 1024;  // 97 KB + w
+constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + 1024;            // + alignment
+constexpr int MX_ACC_COLS = MX_OMEGA * MX_BN;          // 256 fp32 columns per buffer
+constexpr int MX_TMEM_COLS = 2 * MX_ACC_COLS;          // 512
 constexpr unsigned long long MX_WAIT_NS = 2000000000ull;   // 2 s per wait
 
 struct MixedParams {
@@ -55,7 +64,7 @@ struct MixedParams {
   int kb_per_split;
   int splits;
   int n_omega;
-  int tiles_m, tiles_a;
+  int tiles_a;
 };
 
 // ---- small PTX helpers ----------------------------------------------------
@@ -93,12 +102,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile 
   unsigned long long t0 = 0;
   for (uint32_t it = 0;; ++it) {
     if (mbar_try(a, parity)) return true;
-    if (*abort) return false;
+    if (abort && *abort) return false;
     if ((it & 63) == 0) {
       unsigned long long t = globaltimer();
       if (t0 == 0) t0 = t;
       else if (t - t0 > MX_WAIT_NS) {
-        *abort = 1;
+        if (abort) *abort = 1;
         atomicCAS(err, 0, code);
         return false;
       }
@@ -154,6 +163,14 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       "l"((uint64_t)map), "r"(x), "r"(y), "r"(mbar)
       : "memory");
 }
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"((uint64_t)src), "r"(bytes), "r"(mbar)
+      : "memory");
+}
 #define TMEM_LD32(taddr, r)                                                                      \
   asm volatile(                                                                                  \
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13," \
@@ -198,6 +215,15 @@ __global__ void split_table_kernel(const double* __restrict__ Wre, const double*
   }
 }
 
+__global__ void weights32_kernel(int64_t total, const double2* __restrict__ wt,
+                                 float2* __restrict__ wt32) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double2 v = wt[i];
+    wt32[i] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
 // ---- contraction -------------------------------------------------------------
 __device__ __forceinline__ float bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
@@ -217,11 +243,11 @@ __global__ void __launch_bounds__(MX_THREADS, 1)
 mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
                       const __grid_constant__ CUtensorMap tm_l, MixedParams P,
                       const __nv_bfloat16* __restrict__ Xh, const __nv_bfloat16* __restrict__ Xl,
-                      const double2* __restrict__ wt, float* __restrict__ part,
+                      const float2* __restrict__ wt32, double* __restrict__ part,
                       int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t bar_full_x[MX_STAGES], bar_full_y[MX_STAGES],
-      bar_empty[MX_STAGES], bar_done;
+  __shared__ __align__(8) uint64_t bar_full_x[MX_STAGES], bar_full_w[MX_STAGES],
+      bar_full_y[MX_STAGES], bar_empty[MX_STAGES], bar_acc_full[2], bar_acc_empty[2], bar_done;
   __shared__ uint32_t s_tmem;
   __shared__ volatile int s_abort;
 
@@ -235,6 +261,7 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   const int n_om = min(MX_OMEGA, P.n_omega - om0);
   const int kb0 = split * P.kb_per_split;
   const int nkb = max(0, min(P.nkb_total, kb0 + P.kb_per_split) - kb0);
+  const int nch = (nkb + MX_CHUNK_KB - 1) / MX_CHUNK_KB;
 
   auto xh_s = [&](int s) { return smem + (size_t)s * MX_STAGE_BYTES; };
   auto xl_s = [&](int s) { return smem + (size_t)s * MX_STAGE_BYTES + MX_TILE_X; };
@@ -244,13 +271,22 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   auto yl_s = [&](int s, int j) {
     return smem + (size_t)s * MX_STAGE_BYTES + 2 * MX_TILE_X + (size_t)(MX_OMEGA + j) * MX_TILE_Y;
   };
+  auto w_s = [&](int s, int j) {
+    return reinterpret_cast<float2*>(smem + (size_t)s * MX_STAGE_BYTES + 2 * MX_TILE_X +
+                                     2 * MX_OMEGA * MX_TILE_Y) + j * MX_BK;
+  };
 
   if (tid == 0) {
     s_abort = 0;
     for (int s = 0; s < MX_STAGES; ++s) {
       mbar_init(smem_u32(&bar_full_x[s]), 1);
+      mbar_init(smem_u32(&bar_full_w[s]), 1);
       mbar_init(smem_u32(&bar_full_y[s]), MX_PRODUCERS);
       mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&bar_acc_full[b]), 1);
+      mbar_init(smem_u32(&bar_acc_empty[b]), 128);
     }
     mbar_init(smem_u32(&bar_done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -265,147 +301,183 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
+  const size_t R = (size_t)P.rows;
 
-  if (nkb > 0) {
-    if (warp == 0) {
-      // ---------------- TMA producer for the X tiles
-      if (lane == 0) {
-        int issued = 0;
-        for (int i = 0; i < nkb; ++i) {
-          const int s = i % MX_STAGES, r = i / MX_STAGES;
-          if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 1)) break;
-          const uint32_t fb = smem_u32(&bar_full_x[s]);
-          mbar_arrive_tx(fb, 2 * MX_TILE_X);
-          const int kx = (kb0 + i) * MX_BK;
-          tma_load_2d(smem_u32(xh_s(s)), &tm_h, kx, m0, fb);
-          tma_load_2d(smem_u32(xl_s(s)), &tm_l, kx, m0, fb);
-          issued = i + 1;
-        }
-        // the last load into each stage must land before the CTA can exit
-        // (immediate on the normal path, bounded on the abort path)
-        for (int i = max(0, issued - MX_STAGES); i < issued; ++i) {
-          volatile int never = 0;
-          mbar_wait(smem_u32(&bar_full_x[i % MX_STAGES]), (i / MX_STAGES) & 1, &never, err, 6);
-        }
-      }
-    } else if (warp == 1) {
-      // ---------------- MMA issuer
-      if (lane == 0) {
-        const uint32_t idesc = idesc_bf16(MX_BM, MX_BN);
-        for (int i = 0; i < nkb; ++i) {
-          const int s = i % MX_STAGES, r = i / MX_STAGES;
-          if (!mbar_wait(smem_u32(&bar_full_x[s]), r & 1, &s_abort, err, 2)) break;
-          if (!mbar_wait(smem_u32(&bar_full_y[s]), r & 1, &s_abort, err, 3)) break;
-          tc_fence_after();
-          const uint64_t dxh = sw128_desc(smem_u32(xh_s(s)));
-          const uint64_t dxl = sw128_desc(smem_u32(xl_s(s)));
-#pragma unroll
-          for (int kk = 0; kk < MX_BK / 16; ++kk) {
-            const uint64_t koff = (uint64_t)(kk * 32) >> 4;    // +32 bytes per k-step
-            for (int j = 0; j < n_om; ++j) {
-              const uint32_t d = tmem + (uint32_t)(j * MX_BN);
-              const uint64_t dyh = sw128_desc(smem_u32(yh_s(s, j))) + koff;
-              const uint64_t dyl = sw128_desc(smem_u32(yl_s(s, j))) + koff;
-              const uint32_t acc0 = (i > 0 || kk > 0) ? 1u : 0u;
-              umma(d, dxh + koff, dyh, idesc, acc0);
-              umma(d, dxh + koff, dyl, idesc, 1u);
-              umma(d, dxl + koff, dyh, idesc, 1u);
-            }
-          }
-          umma_commit(smem_u32(&bar_empty[s]));
-        }
-        // completion of every issued MMA (also on the abort path)
-        umma_commit(smem_u32(&bar_done));
-      }
-    } else if (warp >= 4) {
-      // ---------------- Y producers: U = w conj(W), split, swizzled store
-      const int pt = tid - 128;                 // 0..255
+  if (warp == 0) {
+    // ---------------- TMA: X tiles + stage weights
+    if (lane == 0 && nkb > 0) {
+      int issued = 0;
       for (int i = 0; i < nkb; ++i) {
         const int s = i % MX_STAGES, r = i / MX_STAGES;
-        if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)) break;
-        const int64_t kbase = (int64_t)(kb0 + i) * MX_BK;
-        // 64 alphas x 8 chunks of 8 k = 512 units per omega, 2 per thread
+        if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 1)) break;
+        const int64_t kx = (int64_t)(kb0 + i) * MX_BK;
+        const uint32_t wb = smem_u32(&bar_full_w[s]);
+        mbar_arrive_tx(wb, n_om * MX_W_BYTES);
+        for (int j = 0; j < n_om; ++j)
+          bulk_load(smem_u32(w_s(s, j)), wt32 + (size_t)(om0 + j) * P.K_pad + kx, MX_W_BYTES, wb);
+        const uint32_t fb = smem_u32(&bar_full_x[s]);
+        mbar_arrive_tx(fb, 2 * MX_TILE_X);
+        tma_load_2d(smem_u32(xh_s(s)), &tm_h, (int)kx, m0, fb);
+        tma_load_2d(smem_u32(xl_s(s)), &tm_l, (int)kx, m0, fb);
+        issued = i + 1;
+      }
+      // the last copies into each stage land before the CTA may exit
+      for (int i = max(0, issued - MX_STAGES); i < issued; ++i) {
+        mbar_wait(smem_u32(&bar_full_x[i % MX_STAGES]), (i / MX_STAGES) & 1, nullptr, err, 6);
+        mbar_wait(smem_u32(&bar_full_w[i % MX_STAGES]), (i / MX_STAGES) & 1, nullptr, err, 6);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0 && nkb > 0) {
+      const uint32_t idesc = idesc_bf16(MX_BM, MX_BN);
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % MX_STAGES, r = i / MX_STAGES;
+        const int ch = i / MX_CHUNK_KB, b = ch & 1;
+        const bool first = (i % MX_CHUNK_KB) == 0;
+        const bool last = (i % MX_CHUNK_KB) == MX_CHUNK_KB - 1 || i == nkb - 1;
+        if (first && !mbar_wait(smem_u32(&bar_acc_empty[b]), ((ch >> 1) & 1) ^ 1, &s_abort, err, 7))
+          break;
+        if (!mbar_wait(smem_u32(&bar_full_x[s]), r & 1, &s_abort, err, 2)) break;
+        if (!mbar_wait(smem_u32(&bar_full_y[s]), r & 1, &s_abort, err, 3)) break;
+        tc_fence_after();
+        const uint64_t dxh = sw128_desc(smem_u32(xh_s(s)));
+        const uint64_t dxl = sw128_desc(smem_u32(xl_s(s)));
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int unit = pt + u * MX_PRODUCERS;
-          const int al = unit >> 3, c = unit & 7;
-          const int a = a0 + al;
-          const int64_t k = kbase + c * 8;
-          const uint4 ah = *reinterpret_cast<const uint4*>(Xh + (size_t)a * P.K_pad + k);
-          const uint4 alw = *reinterpret_cast<const uint4*>(Xl + (size_t)a * P.K_pad + k);
-          const uint4 bh = *reinterpret_cast<const uint4*>(Xh + (size_t)(P.Npad + a) * P.K_pad + k);
-          const uint4 blw = *reinterpret_cast<const uint4*>(Xl + (size_t)(P.Npad + a) * P.K_pad + k);
-          const uint32_t A_h[4] = {ah.x, ah.y, ah.z, ah.w}, A_l[4] = {alw.x, alw.y, alw.z, alw.w};
-          const uint32_t B_h[4] = {bh.x, bh.y, bh.z, bh.w}, B_l[4] = {blw.x, blw.y, blw.z, blw.w};
-          float wr[8], wi[8];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            wr[2 * q] = bf_lo(A_h[q]) + bf_lo(A_l[q]);
-            wr[2 * q + 1] = bf_hi(A_h[q]) + bf_hi(A_l[q]);
-            wi[2 * q] = bf_lo(B_h[q]) + bf_lo(B_l[q]);
-            wi[2 * q + 1] = bf_hi(B_h[q]) + bf_hi(B_l[q]);
-          }
+        for (int kk = 0; kk < MX_BK / 16; ++kk) {
+          const uint64_t koff = (uint64_t)(kk * 32) >> 4;    // +32 bytes per k-step
           for (int j = 0; j < n_om; ++j) {
-            const double2* wz = wt + (size_t)(om0 + j) * P.K_pad + k;
-            uint32_t rh[4], rl[4], ih[4], il[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const double2 w0 = wz[2 * q], w1 = wz[2 * q + 1];
-              const float d0r = (float)w0.x, d0i = (float)w0.y;
-              const float d1r = (float)w1.x, d1i = (float)w1.y;
-              // w conj(W) = (dr Wr + di Wi) + i (di Wr - dr Wi)
-              const float ur0 = d0r * wr[2 * q] + d0i * wi[2 * q];
-              const float ui0 = d0i * wr[2 * q] - d0r * wi[2 * q];
-              const float ur1 = d1r * wr[2 * q + 1] + d1i * wi[2 * q + 1];
-              const float ui1 = d1i * wr[2 * q + 1] - d1r * wi[2 * q + 1];
-              rh[q] = pack_split(ur0, ur1, rl[q]);
-              ih[q] = pack_split(ui0, ui1, il[q]);
-            }
-            const uint32_t offr = sw128_off(2 * al, c), offi = sw128_off(2 * al + 1, c);
-            *reinterpret_cast<uint4*>(yh_s(s, j) + offr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-            *reinterpret_cast<uint4*>(yl_s(s, j) + offr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
-            *reinterpret_cast<uint4*>(yh_s(s, j) + offi) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-            *reinterpret_cast<uint4*>(yl_s(s, j) + offi) = make_uint4(il[0], il[1], il[2], il[3]);
+            const uint32_t d = tmem + (uint32_t)(b * MX_ACC_COLS + j * MX_BN);
+            const uint64_t dyh = sw128_desc(smem_u32(yh_s(s, j))) + koff;
+            const uint64_t dyl = sw128_desc(smem_u32(yl_s(s, j))) + koff;
+            umma(d, dxh + koff, dyh, idesc, (first && kk == 0) ? 0u : 1u);
+            umma(d, dxh + koff, dyl, idesc, 1u);
+            umma(d, dxl + koff, dyh, idesc, 1u);
           }
         }
-        fence_proxy_async();
-        mbar_arrive(smem_u32(&bar_full_y[s]));
+        umma_commit(smem_u32(&bar_empty[s]));
+        if (last) umma_commit(smem_u32(&bar_acc_full[b]));
       }
+      // completion of every issued MMA (also on the abort path)
+      umma_commit(smem_u32(&bar_done));
+    }
+  } else if (warp >= 4 && warp < MX_DRAIN0) {
+    // ---------------- producers: U = w conj(W), split, swizzled store
+    const int pt = tid - 128;                 // 0..255
+    // 64 alphas x 8 chunks of 8 k = 512 units, 2 per thread
+    int al_u[2], c_u[2];
+    const __nv_bfloat16* rows_u[2][4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int unit = pt + u * MX_PRODUCERS;
+      al_u[u] = unit >> 3;
+      c_u[u] = unit & 7;
+      const size_t a = (size_t)(a0 + al_u[u]);
+      rows_u[u][0] = Xh + a * P.K_pad;
+      rows_u[u][1] = Xl + a * P.K_pad;
+      rows_u[u][2] = Xh + (P.Npad + a) * P.K_pad;
+      rows_u[u][3] = Xl + (P.Npad + a) * P.K_pad;
+    }
+    uint4 pre[2][4];
+    auto prefetch = [&](int i) {
+      const int64_t kb = (int64_t)(kb0 + i) * MX_BK;
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          pre[u][q] = __ldg(reinterpret_cast<const uint4*>(rows_u[u][q] + kb + c_u[u] * 8));
+    };
+    if (nkb > 0) prefetch(0);
+    for (int i = 0; i < nkb; ++i) {
+      const int s = i % MX_STAGES, r = i / MX_STAGES;
+      if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)) break;
+      if (!mbar_wait(smem_u32(&bar_full_w[s]), r & 1, &s_abort, err, 8)) break;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const uint32_t A_h[4] = {pre[u][0].x, pre[u][0].y, pre[u][0].z, pre[u][0].w};
+        const uint32_t A_l[4] = {pre[u][1].x, pre[u][1].y, pre[u][1].z, pre[u][1].w};
+        const uint32_t B_h[4] = {pre[u][2].x, pre[u][2].y, pre[u][2].z, pre[u][2].w};
+        const uint32_t B_l[4] = {pre[u][3].x, pre[u][3].y, pre[u][3].z, pre[u][3].w};
+        float wr[8], wi[8];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          wr[2 * q] = bf_lo(A_h[q]) + bf_lo(A_l[q]);
+          wr[2 * q + 1] = bf_hi(A_h[q]) + bf_hi(A_l[q]);
+          wi[2 * q] = bf_lo(B_h[q]) + bf_lo(B_l[q]);
+          wi[2 * q + 1] = bf_hi(B_h[q]) + bf_hi(B_l[q]);
+        }
+        const int al = al_u[u], c = c_u[u];
+        const uint32_t offr = sw128_off(2 * al, c), offi = sw128_off(2 * al + 1, c);
+        for (int j = 0; j < n_om; ++j) {
+          const float4* wz = reinterpret_cast<const float4*>(w_s(s, j) + c * 8);
+          uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float4 w = wz[q];            // weights of k = 2q, 2q+1 in this chunk
+            // w conj(W) = (dr Wr + di Wi) + i (di Wr - dr Wi)
+            const float ur0 = w.x * wr[2 * q] + w.y * wi[2 * q];
+            const float ui0 = w.y * wr[2 * q] - w.x * wi[2 * q];
+            const float ur1 = w.z * wr[2 * q + 1] + w.w * wi[2 * q + 1];
+            const float ui1 = w.w * wr[2 * q + 1] - w.z * wi[2 * q + 1];
+            rh[q] = pack_split(ur0, ur1, rl[q]);
+            ih[q] = pack_split(ui0, ui1, il[q]);
+          }
+          *reinterpret_cast<uint4*>(yh_s(s, j) + offr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+          *reinterpret_cast<uint4*>(yl_s(s, j) + offr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+          *reinterpret_cast<uint4*>(yh_s(s, j) + offi) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+          *reinterpret_cast<uint4*>(yl_s(s, j) + offi) = make_uint4(il[0], il[1], il[2], il[3]);
+        }
+      }
+      fence_proxy_async();
+      mbar_arrive(smem_u32(&bar_full_y[s]));
+      if (i + 1 < nkb) prefetch(i + 1);
+    }
+  } else if (warp >= MX_DRAIN0) {
+    // ---------------- drain: TMEM chunk -> FP64 partial (row per thread)
+    const int q = warp & 3;                   // TMEM lane quadrant of this warp
+    const int row = m0 + q * 32 + lane;
+    for (int ch = 0; ch < max(nch, 1); ++ch) {
+      const int b = ch & 1;
+      bool ok = nkb > 0;
+      if (ok) ok = mbar_wait(smem_u32(&bar_acc_full[b]), (ch >> 1) & 1, &s_abort, err, 9);
+      ok = __all_sync(0xffffffffu, ok);
+      if (nkb > 0 && !ok) break;
+      tc_fence_after();
+      for (int j = 0; j < n_om; ++j) {
+        double* out = part + (((size_t)(om0 + j) * P.splits + split) * R + row) * R + 2 * a0;
+        for (int cc = 0; cc < MX_BN / 32; ++cc) {
+          uint32_t v[32];
+          if (nkb > 0) {
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) +
+                                   (uint32_t)(b * MX_ACC_COLS + j * MX_BN + cc * 32);
+            TMEM_LD32(taddr, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          } else {
+#pragma unroll
+            for (int t = 0; t < 32; ++t) v[t] = 0u;
+          }
+          double2* o2 = reinterpret_cast<double2*>(out + cc * 32);
+#pragma unroll
+          for (int t = 0; t < 16; ++t) {
+            double2 acc = make_double2((double)__uint_as_float(v[2 * t]),
+                                       (double)__uint_as_float(v[2 * t + 1]));
+            if (ch > 0) {
+              const double2 old = o2[t];
+              acc.x += old.x;
+              acc.y += old.y;
+            }
+            o2[t] = acc;
+          }
+        }
+      }
+      tc_fence_before();
+      if (nkb > 0) mbar_arrive(smem_u32(&bar_acc_empty[b]));
     }
   }
   __syncwarp();
-
-  // ---------------- epilogue: TMEM -> FP32 partial tiles
-  const size_t R = (size_t)P.rows;
-  if (warp < 4) {
-    bool ok = true;
-    if (nkb > 0) {
-      // every issued MMA has completed once bar_done fires, also when aborting
-      volatile int never = 0;
-      ok = mbar_wait(smem_u32(&bar_done), 0, &never, err, 5);
-      ok = __all_sync(0xffffffffu, ok && !s_abort);
-    }
-    tc_fence_after();
-    const int row = m0 + warp * 32 + lane;
-    for (int j = 0; j < n_om; ++j) {
-      float* out = part + (((size_t)(om0 + j) * P.splits + split) * R + row) * R + 2 * a0;
-      for (int cc = 0; cc < MX_BN / 32; ++cc) {
-        uint32_t v[32];
-        if (nkb > 0 && ok) {
-          const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * MX_BN + cc * 32);
-          TMEM_LD32(taddr, v);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        } else {
-#pragma unroll
-          for (int q = 0; q < 32; ++q) v[q] = 0u;
-        }
-        float4* o4 = reinterpret_cast<float4*>(out + cc * 32);
-#pragma unroll
-        for (int q = 0; q < 8; ++q)
-          o4[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
-                              __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
-      }
-    }
+  // all MMAs have completed before TMEM is released (bounded; ignores abort)
+  if (warp == 2 && nkb > 0) {
+    mbar_wait(smem_u32(&bar_done), 0, nullptr, err, 5);
   }
   tc_fence_before();
   __syncthreads();
@@ -416,9 +488,9 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   }
 }
 
-// ---- reduction of the FP32 partial tiles -----------------------------------------
+// ---- reduction of the FP64 partial tiles -----------------------------------------
 __global__ void mixed_reduce_kernel(int Na, int Npad, int splits, double G,
-                                    const double* __restrict__ Nk, const float* __restrict__ part,
+                                    const double* __restrict__ Nk, const double* __restrict__ part,
                                     double2* __restrict__ A, double2* __restrict__ Mout) {
   const int z = blockIdx.y;
   const size_t R = 2 * (size_t)Npad;
@@ -426,12 +498,11 @@ __global__ void mixed_reduce_kernel(int Na, int Npad, int splits, double G,
     const int b = e / Na, a = e % Na;
     double mr = 0.0, mi = 0.0;
     for (int s = 0; s < splits; ++s) {
-      const float* P = part + ((size_t)z * splits + s) * R * R;
-      const double pr_r = P[(size_t)b * R + 2 * a], pr_i = P[(size_t)b * R + 2 * a + 1];
-      const double pi_r = P[(size_t)(Npad + b) * R + 2 * a];
-      const double pi_i = P[(size_t)(Npad + b) * R + 2 * a + 1];
-      mr += pr_r - pi_i;
-      mi += pr_i + pi_r;
+      const double* P = part + ((size_t)z * splits + s) * R * R;
+      const double2 pr = *reinterpret_cast<const double2*>(P + (size_t)b * R + 2 * a);
+      const double2 pi = *reinterpret_cast<const double2*>(P + (size_t)(Npad + b) * R + 2 * a);
+      mr += pr.x - pi.y;
+      mi += pr.y + pi.x;
     }
     const double n = Nk[a];
     const double Mr = (mr * G) * n, Mi = (mi * G) * n;
@@ -451,8 +522,10 @@ struct kls_mixed {
   __nv_bfloat16* Xh = nullptr;
   __nv_bfloat16* Xl = nullptr;
   CUtensorMap tm_h, tm_l;
-  float* part = nullptr;
+  double* part = nullptr;       // FP64 partials [n][splits][2 Npad][2 Npad]
   size_t part_elems = 0;
+  float2* wt32 = nullptr;       // FP32 weights [n][K_pad]
+  size_t wt32_elems = 0;
   int* err = nullptr;
   int splits = 1;
 };
@@ -524,9 +597,20 @@ int kls_mixed_contract(kls_ctx* c, int n, int) {
     cudaFree(m->part);
     m->part = nullptr;
     m->part_elems = 0;
-    KLS_CK(c, cudaMalloc(&m->part, need * sizeof(float)));
+    KLS_CK(c, cudaMalloc(&m->part, need * sizeof(double)));
     m->part_elems = need;
   }
+  const size_t nw = (size_t)n * c->K_pad;
+  if (nw > m->wt32_elems) {
+    cudaFree(m->wt32);
+    m->wt32 = nullptr;
+    m->wt32_elems = 0;
+    KLS_CK(c, cudaMalloc(&m->wt32, nw * sizeof(float2)));
+    m->wt32_elems = nw;
+  }
+  weights32_kernel<<<(unsigned)std::min<size_t>((nw + 255) / 256, 4096), 256, 0, c->stream>>>(
+      (int64_t)nw, c->d_wt, m->wt32);
+  KLS_LAUNCHED(c);
   MixedParams P{};
   P.Npad = c->Na_pad;
   P.rows = (int)R;
@@ -535,11 +619,10 @@ int kls_mixed_contract(kls_ctx* c, int n, int) {
   P.splits = m->splits;
   P.kb_per_split = (P.nkb_total + m->splits - 1) / m->splits;
   P.n_omega = n;
-  P.tiles_m = (int)(R / MX_BM);
   P.tiles_a = c->Na_pad / MX_AB;
-  dim3 grid(P.tiles_m * P.tiles_a, m->splits, (n + MX_OMEGA - 1) / MX_OMEGA);
+  dim3 grid((unsigned)((R / MX_BM) * P.tiles_a), m->splits, (n + MX_OMEGA - 1) / MX_OMEGA);
   mixed_contract_kernel<<<grid, MX_THREADS, MX_SMEM, c->stream>>>(m->tm_h, m->tm_l, P, m->Xh,
-                                                                  m->Xl, c->d_wt, m->part, m->err);
+                                                                  m->Xl, m->wt32, m->part, m->err);
   KLS_LAUNCHED(c);
   return KLS_OK;
 }
@@ -570,6 +653,7 @@ void kls_mixed_free(kls_ctx* c) {
   cudaFree(c->mixed->Xh);
   cudaFree(c->mixed->Xl);
   cudaFree(c->mixed->part);
+  cudaFree(c->mixed->wt32);
   cudaFree(c->mixed->err);
   delete c->mixed;
   c->mixed = nullptr;
