@@ -115,7 +115,8 @@ int kls_create(const kls_config* cfg, int device, kls_ctx** out);
 int kls_destroy(kls_ctx* ctx);
 /* Message of the last failing call on this context (never NULL). */
 const char* kls_last_error(const kls_ctx* ctx);
-/* Message for failures of kls_create, where no context exists yet. */
+/* Message for failures of calls without a context (kls_create,
+ * kls_det_lu_static). */
 const char* kls_create_error(void);
 int kls_get_dims(const kls_ctx* ctx, kls_dims* out);
 /* Launch subsequent work on this cudaStream_t (NULL = the context's own). */
@@ -166,6 +167,22 @@ int kls_scan(kls_ctx* ctx, const kls_scan_cfg* sc, double* det_grid_ri,
  * (Omega_p, gamma, |det|) per iteration, may be NULL.                      */
 int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cfg* nc,
                kls_newton_result* res, double* history);
+
+/* Determinants of n_matrices caller-supplied complex N x N matrices (device
+ * memory, row-major, interleaved re,im; the input is not modified) into
+ * d_det_ri (n complex) and d_log_abs (n doubles, may be NULL), launched on
+ * `stream` (NULL = legacy default stream); no host synchronisation.  No
+ * counterpart in the reference.  It allocates nothing: it is for callers that
+ * must not allocate device memory themselves, e.g. a host whose pool allocator
+ * owns the whole GPU, or a loop that cannot take cudaMalloc's implicit device
+ * synchronisation.  Scratch is a fixed 16 MiB array inside libkls.so (held on
+ * every GPU that loads the library until exit), so n_matrices * N * N must not
+ * exceed 1,048,576; larger requests return KLS_ERR_CONFIG.  The first call on
+ * a device looks up the array's device address (make it before any stream
+ * capture).  Calls whose kernels overlap on one GPU race on the shared
+ * scratch.  Errors are described by kls_create_error().                    */
+int kls_det_lu_static(const double* d_A_ri, int n_matrices, int N, double* d_det_ri,
+                      double* d_log_abs, void* stream);
 
 /* ---- instrumentation ----------------------------------------------------- */
 /* Per-stage device time (ms) of the last det batch when timing is enabled:

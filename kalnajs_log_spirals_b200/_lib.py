@@ -90,6 +90,7 @@ SIGNATURES = {
     "kls_scan": (C.c_int, [_P, C.POINTER(kls_scan_cfg), _D, _D, _D, _D]),
     "kls_newton": (C.c_int, [_P, C.c_double, C.c_double, C.POINTER(kls_newton_cfg),
                              C.POINTER(kls_newton_result), _D]),
+    "kls_det_lu_static": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_launch_count": (C.c_int64, [_P]),
