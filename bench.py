@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--model", default=os.path.join(ROOT, "models", "kalnajs_zang4.toml"))
     ap.add_argument("--no-newton", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--accuracy-points", type=int, default=200)
     return ap.parse_args()
 
 
@@ -218,6 +220,7 @@ def ours(args):
     import torch
     import kalnajs_log_spirals_b200 as K
     from kalnajs_log_spirals_b200 import _lib
+    from kalnajs_log_spirals_b200.api import newton_search_hybrid
 
     rank, local, world = dist_env()
     torch.cuda.set_device(local)
@@ -229,6 +232,14 @@ def ours(args):
     m = cfg.physics.m
 
     peak64 = dgemm_peak_tflops(torch)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak_bf16 = float(peaks.get("bf16_tflops", 1590.0))
+    peak_bf16_note = "of measured (MEASURED_PEAKS.json bf16_tflops, burst)" if "bf16_tflops" in peaks \
+        else "of fallback (1.59 PFLOP/s)"
 
     t0 = time.perf_counter()
     pc = K.precompute_all(cfg, device=local)
@@ -245,17 +256,19 @@ def ours(args):
 
     nb = 3
     flops_per_det = 8.0 * dims.N_alpha ** 2 * dims.K
-    d_om = torch.empty((nb, 2), dtype=torch.float64, device="cuda")
+    # tensor flops of the 3-product split GEMM per determinant (unpadded)
+    mixed_flops_per_det = 3 * 2.0 * (2 * dims.N_alpha) ** 2 * dims.K
     d_det = torch.empty((nb, 2), dtype=torch.float64, device="cuda")
     d_la = torch.empty((nb,), dtype=torch.float64, device="cuda")
-    # all omegas of warm-up + timed steps staged up front
-    all_om = np.array([[ [w.real, w.imag] for w in omegas_for_step(s, rank, m, cfg.reference.Omega_p,
-                        cfg.reference.gamma, cfg.newton.delta)] for s in range(args.warmup + args.steps)])
+    n_steps = args.warmup + args.steps
+    all_om = np.array([[[w.real, w.imag] for w in omegas_for_step(
+        s, rank, m, cfg.reference.Omega_p, cfg.reference.gamma, cfg.newton.delta)]
+        for s in range(n_steps)])
     d_all = torch.tensor(all_om, dtype=torch.float64, device="cuda")
 
-    def dev_step(s):
-        _lib.check(h, lib.kls_det_batch_device(h, C.c_void_p(d_all[s].data_ptr()), nb,
-                                               _lib.KLS_MODE_FP64, C.c_void_p(d_det.data_ptr()),
+    def dev_step(s, mode):
+        _lib.check(h, lib.kls_det_batch_device(h, C.c_void_p(d_all[s % n_steps].data_ptr()), nb,
+                                               mode, C.c_void_p(d_det.data_ptr()),
                                                C.c_void_p(d_la.data_ptr())))
 
     def barrier():
@@ -271,42 +284,44 @@ def ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- device-resident timing --------------------------------------------
-    for s in range(args.warmup):
-        dev_step(s)
-    torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    l0 = lib.kls_launch_count(h)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for s in range(args.warmup, args.warmup + args.steps):
-        dev_step(s)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    launches = lib.kls_launch_count(h) - l0
-    clk = clocks.stop()
-    barrier()
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms)
+    def time_device(mode, sample_clocks=False):
+        for s in range(args.warmup):
+            dev_step(s, mode)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local) if sample_clocks else None
+        l0 = lib.kls_launch_count(h)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for s in range(args.warmup, n_steps):
+            dev_step(s, mode)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        launches = lib.kls_launch_count(h) - l0
+        clk = clocks.stop() if clocks else None
+        barrier()
+        return max_over_ranks(ev0.elapsed_time(ev1)), launches, clk
+
+    def stage_times(mode):
+        _lib.check(h, lib.kls_enable_timing(h, 1))
+        stage = np.zeros(4)
+        reps = max(1, min(args.steps, 4))
+        for s in range(reps):
+            dev_step(args.warmup + s, mode)
+            torch.cuda.synchronize()
+            buf = (C.c_float * 4)()
+            _lib.check(h, lib.kls_get_stage_ms(h, buf))
+            stage += np.array(buf[:])
+        _lib.check(h, lib.kls_enable_timing(h, 0))
+        return stage / reps
+
+    # ---- plain FP64: device-resident timing (headline) ----------------------
+    ms, launches, clk = time_device(_lib.KLS_MODE_FP64, sample_clocks=True)
     ms_per_step = ms / args.steps
     value = world * nb * args.steps / (ms * 1e-3)
-
-    # ---- per-kernel durations (separate pass, library events on the same stream)
-    _lib.check(h, lib.kls_enable_timing(h, 1))
-    stage = np.zeros(4)
-    reps = max(1, min(args.steps, 4))
-    for s in range(reps):
-        dev_step(args.warmup + s)
-        torch.cuda.synchronize()
-        buf = (C.c_float * 4)()
-        _lib.check(h, lib.kls_get_stage_ms(h, buf))
-        stage += np.array(buf[:])
-    _lib.check(h, lib.kls_enable_timing(h, 0))
-    stage /= reps
-    contract_ms = float(stage[1])
-    achieved = nb * flops_per_det / (contract_ms * 1e-3) / 1e12
+    stage = stage_times(_lib.KLS_MODE_FP64)
+    achieved = nb * flops_per_det / (stage[1] * 1e-3) / 1e12
 
     # ---- end to end through the C ABI with host buffers -----------------------
     h_om = np.ascontiguousarray(all_om)
@@ -319,7 +334,7 @@ def ours(args):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for s in range(args.warmup, args.warmup + args.steps):
+    for s in range(args.warmup, n_steps):
         _lib.check(h, lib.kls_det_batch(h, _lib.dptr(h_om[s]), nb, _lib.KLS_MODE_FP64,
                                         _lib.dptr(det_h), _lib.dptr(la_h)))
     e1.record(stream)
@@ -327,16 +342,65 @@ def ours(args):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e = world * nb * args.steps / (e2e_ms * 1e-3)
 
-    # ---- Newton time-to-root from the reference start (plain FP64) ----------
+    # ---- mixed form: split-BF16 tensor-core contraction ------------------------
+    mixed = None
+    if not args.no_mixed:
+        t0 = time.perf_counter()
+        _lib.check(h, lib.kls_prepare_mixed(h))
+        t_split = time.perf_counter() - t0
+        ms_mx, launches_mx, _ = time_device(_lib.KLS_MODE_MIXED)
+        stage_mx = stage_times(_lib.KLS_MODE_MIXED)
+        ach_mx = nb * mixed_flops_per_det / (stage_mx[1] * 1e-3) / 1e12
+        # accuracy against the plain FP64 form on 200 seeded omegas:
+        # Omega_p ~ U[0.3, 0.6], gamma ~ U[0.02, 0.25], omega = m Omega_p + i gamma
+        rng = np.random.default_rng(0)
+        om = m * rng.uniform(0.3, 0.6, args.accuracy_points) + \
+            1j * rng.uniform(0.02, 0.25, args.accuracy_points)
+        d64 = K.compute_determinant_batched(om, pc, None, batch_size=16)
+        dmx = np.empty_like(d64)
+        _lib.check(h, lib.kls_det_batch(h, _lib.dptr(om.view(np.float64)), len(om),
+                                        _lib.KLS_MODE_MIXED, _lib.dptr(dmx.view(np.float64)),
+                                        C.cast(None, C.POINTER(C.c_double))))
+        rel = np.abs(dmx - d64) / np.abs(d64)
+        mixed = {"det_evals_per_s": world * nb * args.steps / (ms_mx * 1e-3),
+                 "ms_per_step": ms_mx / args.steps, "gpu_launches": int(launches_mx),
+                 "split_table_s": t_split,
+                 "roofline": {"bound": "tensor", "kernel": "mixed_contract_kernel (tcgen05 kind::f16, TMEM)",
+                              "achieved": ach_mx, "peak": peak_bf16, "unit": "TFLOP/s",
+                              "frac": ach_mx / peak_bf16, "peak_note": peak_bf16_note,
+                              "algorithmic_flops_per_launch": nb * mixed_flops_per_det,
+                              "traffic": read_traffic("contract_mixed_default.md"),
+                              "stage_ms": {"weights": stage_mx[0], "contract": stage_mx[1],
+                                           "reduce": stage_mx[2], "lu": stage_mx[3]}},
+                 "rel_det_err_vs_fp64": {"points": int(len(om)), "seed": 0,
+                                         "median": float(np.median(rel)),
+                                         "p90": float(np.quantile(rel, 0.9)),
+                                         "max": float(rel.max())}}
+
+    # ---- Newton time-to-root from the reference start -------------------------
     newton = None
     if not args.no_newton:
         barrier()
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         r = K.newton_search(cfg, pc, None, K.GPUType.NVIDIA, "Float64")
-        t_newton = time.perf_counter() - t0
-        newton = {"form": "plain FP64", "time_to_root_s": t_newton, "Omega_p": r.Omega_p,
-                  "gamma": r.gamma, "abs_det": abs(r.det_val), "iterations": r.iterations,
-                  "det_evals": r.det_evals, "converged": r.converged, "tol": cfg.newton.tol}
+        t_plain = time.perf_counter() - t0
+        newton = {"plain_fp64": {"time_to_root_s": t_plain, "Omega_p": r.Omega_p, "gamma": r.gamma,
+                                 "abs_det": abs(r.det_val), "iterations": r.iterations,
+                                 "det_evals": r.det_evals, "converged": r.converged},
+                  "tol": cfg.newton.tol}
+        if not args.no_mixed:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rh = newton_search_hybrid(cfg, pc)
+            t_h = time.perf_counter() - t0
+            newton["mixed_fp64_finish"] = {
+                "time_to_root_s": t_h, "Omega_p": rh.Omega_p, "gamma": rh.gamma,
+                "abs_det": abs(rh.det_val), "converged": rh.converged,
+                "mixed_evals": rh.mixed_evals, "fp64_evals": rh.fp64_evals,
+                "abs_dOmega_p_vs_plain": abs(rh.Omega_p - r.Omega_p),
+                "abs_dgamma_vs_plain": abs(rh.gamma - r.gamma)}
+            newton["speedup_hybrid_vs_plain"] = t_plain / t_h
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -373,6 +437,7 @@ def ours(args):
         "gpu_launches": int(launches),
         "clocks": clk,
         "precompute_s": t_pre,
+        "mixed": mixed,
         "newton": newton,
     }
     print(json.dumps(line), flush=True)

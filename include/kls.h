@@ -168,6 +168,27 @@ int kls_scan(kls_ctx* ctx, const kls_scan_cfg* sc, double* det_grid_ri,
 int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cfg* nc,
                kls_newton_result* res, double* history);
 
+/* Mixed-precision Newton with an FP64 finish (no reference counterpart; it
+ * returns the point at which the reference's own stopping rule,
+ * |det| < nc->tol on the plain FP64 determinant, holds):
+ *   phase 1: Newton on split-BF16 determinants, the finite-difference triple
+ *            (omega, omega + m*mixed_delta, omega + i*mixed_delta) evaluated
+ *            as one batch, until a step is shorter than mixed_step_tol;
+ *   phase 2: FP64 determinant at the current point; stop if |det| < tol,
+ *            else a chord step with the last Jacobian; the Jacobian is
+ *            recomputed in FP64 (step nc->delta) when |det| falls by less
+ *            than 10x per step.                                            */
+typedef struct kls_hybrid_cfg {
+    double  mixed_delta;
+    double  mixed_step_tol;
+    int32_t mixed_max_iter;
+    int32_t fp64_max_iter;
+} kls_hybrid_cfg;
+/* evals[0], evals[1] (may be NULL): mixed and FP64 determinant evaluations. */
+int kls_newton_hybrid(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cfg* nc,
+                      const kls_hybrid_cfg* hc, kls_newton_result* res, int32_t* evals,
+                      double* history);
+
 /* Determinants of n_matrices caller-supplied complex N x N matrices (device
  * memory, row-major, interleaved re,im; the input is not modified) into
  * d_det_ri (n complex) and d_log_abs (n doubles, may be NULL), launched on

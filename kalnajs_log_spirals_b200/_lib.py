@@ -60,6 +60,11 @@ class kls_newton_result(C.Structure):
                 ("iterations", C.c_int32), ("converged", C.c_int32), ("det_evals", C.c_int32)]
 
 
+class kls_hybrid_cfg(C.Structure):
+    _fields_ = [("mixed_delta", C.c_double), ("mixed_step_tol", C.c_double),
+                ("mixed_max_iter", C.c_int32), ("fp64_max_iter", C.c_int32)]
+
+
 class kls_scan_cfg(C.Structure):
     _fields_ = [("n_Op", C.c_int32), ("n_gamma", C.c_int32), ("Omega_p_min", C.c_double),
                 ("Omega_p_max", C.c_double), ("gamma_min", C.c_double),
@@ -90,6 +95,9 @@ SIGNATURES = {
     "kls_scan": (C.c_int, [_P, C.POINTER(kls_scan_cfg), _D, _D, _D, _D]),
     "kls_newton": (C.c_int, [_P, C.c_double, C.c_double, C.POINTER(kls_newton_cfg),
                              C.POINTER(kls_newton_result), _D]),
+    "kls_newton_hybrid": (C.c_int, [_P, C.c_double, C.c_double, C.POINTER(kls_newton_cfg),
+                                    C.POINTER(kls_hybrid_cfg), C.POINTER(kls_newton_result),
+                                    C.POINTER(C.c_int32), _D]),
     "kls_det_lu_static": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),

@@ -486,3 +486,46 @@ def newton_search(config: KalnajsConfig, precomputed: PrecomputedData,
     return NewtonResult(res.Omega_p, res.gamma, complex(res.omega_re, res.omega_im),
                         complex(res.det_re, res.det_im), int(res.iterations),
                         bool(res.converged), h, int(res.det_evals))
+
+
+@dataclass
+class HybridConfig:
+    """Mixed-precision phase parameters of newton_search_hybrid."""
+    mixed_delta: float = 1e-5
+    mixed_step_tol: float = 1e-7
+    mixed_max_iter: int = 12
+    fp64_max_iter: int = 8
+
+
+def newton_search_hybrid(config: KalnajsConfig, precomputed: PrecomputedData,
+                         Omega_p_init: Optional[float] = None,
+                         gamma_init: Optional[float] = None,
+                         hybrid: Optional[HybridConfig] = None) -> NewtonResult:
+    """Split-BF16 Newton, then FP64 chord steps to the reference's stopping rule.
+
+    No reference counterpart: the result satisfies |det(I - M)| < config.newton.tol
+    on the plain FP64 determinant, the same test newton_search applies
+    (NewtonSolver.jl:89); ``det_evals`` counts both precisions and
+    ``history`` has one row per determinant batch.
+    """
+    n = config.newton
+    hc = hybrid or HybridConfig()
+    if Omega_p_init is None:
+        Omega_p_init = config.reference.Omega_p
+    if gamma_init is None:
+        gamma_init = config.reference.gamma
+    precomputed.ctx.call("kls_prepare_mixed")
+    nc = _lib.kls_newton_cfg(int(n.max_iter), float(n.tol), float(n.delta),
+                             int(bool(n.use_line_search)), int(n.max_line_search), KLS_MODE_FP64)
+    h = _lib.kls_hybrid_cfg(float(hc.mixed_delta), float(hc.mixed_step_tol),
+                            int(hc.mixed_max_iter), int(hc.fp64_max_iter))
+    res = _lib.kls_newton_result()
+    ev = (C.c_int32 * 2)()
+    hist = np.zeros((int(n.max_iter), 3))
+    precomputed.ctx.call("kls_newton_hybrid", float(Omega_p_init), float(gamma_init), C.byref(nc),
+                         C.byref(h), C.byref(res), ev, dptr(hist))
+    r = NewtonResult(res.Omega_p, res.gamma, complex(res.omega_re, res.omega_im),
+                     complex(res.det_re, res.det_im), int(res.iterations), bool(res.converged),
+                     hist[:min(res.iterations, int(n.max_iter))].copy(), int(res.det_evals))
+    r.mixed_evals, r.fp64_evals = int(ev[0]), int(ev[1])
+    return r

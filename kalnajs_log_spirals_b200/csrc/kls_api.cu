@@ -545,6 +545,94 @@ int kls_newton(kls_ctx* c, double Op_init, double g_init, const kls_newton_cfg* 
   return KLS_OK;
 }
 
+int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newton_cfg* nc,
+                      const kls_hybrid_cfg* hc, kls_newton_result* res, int32_t* evals,
+                      double* history) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (!nc || !hc || !res || hc->mixed_max_iter < 0 || hc->fp64_max_iter < 1)
+    return kls_fail(c, KLS_ERR_CONFIG, "bad hybrid Newton arguments");
+  const double m = (double)c->cfg.m, tol = nc->tol;
+  double Op = Op_init, g = g_init;
+  int n_mixed = 0, n_fp64 = 0, it_total = 0;
+  std::memset(res, 0, sizeof *res);
+  auto clamp = [&]() {
+    g = std::max(g, 1e-4);
+    Op = std::min(std::max(Op, 0.0), 1.0);
+  };
+  auto hist = [&](double a) {
+    if (history && it_total < nc->max_iter) {
+      history[3 * it_total] = Op;
+      history[3 * it_total + 1] = g;
+      history[3 * it_total + 2] = a;
+    }
+    ++it_total;
+  };
+  // ---- phase 1: split-BF16 Newton, FD triple in one batch
+  double J[2][2] = {{0, 0}, {0, 0}};
+  bool haveJ = false;
+  const double dm = hc->mixed_delta;
+  for (int it = 0; it < hc->mixed_max_iter; ++it) {
+    double w[6] = {m * Op, g, m * (Op + dm), g, m * Op, g + dm}, d[6];
+    if ((r = det_batch_host(c, w, 3, KLS_MODE_MIXED, d, nullptr))) return r;
+    n_mixed += 3;
+    hist(std::hypot(d[0], d[1]));
+    J[0][0] = (d[2] - d[0]) / dm; J[0][1] = (d[4] - d[0]) / dm;
+    J[1][0] = (d[3] - d[1]) / dm; J[1][1] = (d[5] - d[1]) / dm;
+    haveJ = true;
+    double F[2] = {d[0], d[1]}, x[2];
+    if (!solve2(J, F, x)) break;
+    Op -= x[0];
+    g -= x[1];
+    clamp();
+    if (std::hypot(x[0], x[1]) < hc->mixed_step_tol) break;
+  }
+  // ---- phase 2: FP64 determinant, chord steps with the last Jacobian
+  bool converged = false;
+  double dl[2] = {NAN, NAN}, prev = INFINITY;
+  for (int it = 0; it < hc->fp64_max_iter; ++it) {
+    double w[2] = {m * Op, g};
+    if ((r = det_batch_host(c, w, 1, KLS_MODE_FP64, dl, nullptr))) return r;
+    ++n_fp64;
+    const double a = std::hypot(dl[0], dl[1]);
+    hist(a);
+    if (a < tol) { converged = true; break; }
+    if (!haveJ || a > 0.1 * prev) {
+      // Jacobian in FP64 (NewtonSolver.jl:98-109), FD pair in one batch
+      double w2[4] = {m * (Op + nc->delta), g, m * Op, g + nc->delta}, d2[4];
+      if ((r = det_batch_host(c, w2, 2, KLS_MODE_FP64, d2, nullptr))) return r;
+      n_fp64 += 2;
+      J[0][0] = (d2[0] - dl[0]) / nc->delta; J[0][1] = (d2[2] - dl[0]) / nc->delta;
+      J[1][0] = (d2[1] - dl[1]) / nc->delta; J[1][1] = (d2[3] - dl[1]) / nc->delta;
+      haveJ = true;
+    }
+    prev = a;
+    double F[2] = {dl[0], dl[1]}, x[2];
+    if (!solve2(J, F, x)) {
+      res->Omega_p = Op; res->gamma = g; res->iterations = it_total;
+      res->det_evals = n_mixed + n_fp64;
+      return kls_fail(c, KLS_ERR_SINGULAR, "singular Jacobian in the FP64 phase");
+    }
+    Op -= x[0];
+    g -= x[1];
+    clamp();
+  }
+  res->Omega_p = Op; res->gamma = g; res->omega_re = m * Op; res->omega_im = g;
+  if (converged) {
+    res->det_re = dl[0]; res->det_im = dl[1];
+  } else {
+    double w[2] = {m * Op, g};
+    if ((r = det_batch_host(c, w, 1, KLS_MODE_FP64, dl, nullptr))) return r;
+    ++n_fp64;
+    res->det_re = dl[0]; res->det_im = dl[1];
+  }
+  res->iterations = it_total;
+  res->converged = converged ? 1 : 0;
+  res->det_evals = n_mixed + n_fp64;
+  if (evals) { evals[0] = n_mixed; evals[1] = n_fp64; }
+  return KLS_OK;
+}
+
 int kls_enable_timing(kls_ctx* c, int on) {
   if (!c) return KLS_ERR_CONFIG;
   c->timing = on != 0;

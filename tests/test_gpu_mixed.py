@@ -106,16 +106,24 @@ SMALL = dict(m=2, G=1.0, L0=1.0, n_zang=4, q1=7, NR=61, Ne=21, Rc_min=0.01, Rc_m
              v_min=0.01, N_alpha=101, alpha_max=10.0, l_min=-10, l_max=10, nw=10001, nwa=201)
 
 
-def test_mixed_newton_close_to_fp64_root(lib_path):
+def test_mixed_and_hybrid_newton(lib_path):
+    """Mixed-only Newton lands within the split form's accuracy (1e-4); the
+    hybrid (mixed phase + FP64 chord finish) lands on the FP64 root (1e-10)."""
+    from kalnajs_log_spirals_b200.api import newton_search_hybrid
     c = kconfig(**SMALL)
     c.newton.tol = 1e-12
     c.newton.use_line_search = False
     pc = K.precompute_all(c)
     r64 = K.newton_search(c, pc, None, K.GPUType.NVIDIA, "Float64", 0.44, 0.13)
+    rh = newton_search_hybrid(c, pc, 0.44, 0.13)
     dev = K.to_device(pc, K.GPUType.NVIDIA, "Float32")
-    c.newton.tol = 1e-6          # the mixed form's det noise floor is well above 1e-12
-    c.newton.max_iter = 20
-    rmx = K.newton_search(c, pc, dev, K.GPUType.NVIDIA, "Float32", 0.44, 0.13)
+    c2 = kconfig(**SMALL)
+    c2.newton.tol = 1e-6          # the mixed form's det noise is far above 1e-12
+    c2.newton.max_iter = 20
+    c2.newton.use_line_search = False
+    rmx = K.newton_search(c2, pc, dev, K.GPUType.NVIDIA, "Float32", 0.44, 0.13)
     pc.close()
-    assert r64.converged
-    assert abs(rmx.Omega_p - r64.Omega_p) < 1e-5 and abs(rmx.gamma - r64.gamma) < 1e-5
+    assert r64.converged and rh.converged
+    assert abs(rmx.Omega_p - r64.Omega_p) < 1e-4 and abs(rmx.gamma - r64.gamma) < 1e-4
+    assert abs(rh.Omega_p - r64.Omega_p) <= 1e-10 and abs(rh.gamma - r64.gamma) <= 1e-10
+    assert abs(rh.det_val) < 1e-12 and rh.fp64_evals <= 4, (rh.fp64_evals, rh.mixed_evals)
