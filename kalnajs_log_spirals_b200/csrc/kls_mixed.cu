@@ -330,7 +330,11 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   } else if (warp == 1) {
     // ---------------- MMA issuer
     if (lane == 0 && nkb > 0) {
-      const uint32_t idesc = idesc_bf16(MX_BM, MX_BN);
+      // the Y tiles of the CTA's omegas are adjacent in shared memory and the
+      // accumulators adjacent in TMEM, so one MMA with N = 128 * n_om covers all
+      // omegas (the operand reads per MAC bound this kernel: N = 256 halves the
+      // A-tile reads of N = 128)
+      const uint32_t idesc = idesc_bf16(MX_BM, MX_BN * n_om);
       for (int i = 0; i < nkb; ++i) {
         const int s = i % MX_STAGES, r = i / MX_STAGES;
         const int ch = i / MX_CHUNK_KB, b = ch & 1;
@@ -343,17 +347,15 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
         tc_fence_after();
         const uint64_t dxh = sw128_desc(smem_u32(xh_s(s)));
         const uint64_t dxl = sw128_desc(smem_u32(xl_s(s)));
+        const uint32_t d = tmem + (uint32_t)(b * MX_ACC_COLS);
+        const uint64_t dyh0 = sw128_desc(smem_u32(yh_s(s, 0)));
+        const uint64_t dyl0 = sw128_desc(smem_u32(yl_s(s, 0)));
 #pragma unroll
         for (int kk = 0; kk < MX_BK / 16; ++kk) {
           const uint64_t koff = (uint64_t)(kk * 32) >> 4;    // +32 bytes per k-step
-          for (int j = 0; j < n_om; ++j) {
-            const uint32_t d = tmem + (uint32_t)(b * MX_ACC_COLS + j * MX_BN);
-            const uint64_t dyh = sw128_desc(smem_u32(yh_s(s, j))) + koff;
-            const uint64_t dyl = sw128_desc(smem_u32(yl_s(s, j))) + koff;
-            umma(d, dxh + koff, dyh, idesc, (first && kk == 0) ? 0u : 1u);
-            umma(d, dxh + koff, dyl, idesc, 1u);
-            umma(d, dxl + koff, dyh, idesc, 1u);
-          }
+          umma(d, dxh + koff, dyh0 + koff, idesc, (first && kk == 0) ? 0u : 1u);
+          umma(d, dxh + koff, dyl0 + koff, idesc, 1u);
+          umma(d, dxl + koff, dyh0 + koff, idesc, 1u);
         }
         umma_commit(smem_u32(&bar_empty[s]));
         if (last) umma_commit(smem_u32(&bar_acc_full[b]));
@@ -364,14 +366,14 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   } else if (warp >= 4 && warp < MX_DRAIN0) {
     // ---------------- producers: U = w conj(W), split, swizzled store
     const int pt = tid - 128;                 // 0..255
-    // 64 alphas x 8 chunks of 8 k = 512 units, 2 per thread
+    // 64 alphas x 8 chunks of 8 k = 512 units, 2 per thread with the same
+    // k-chunk (alphas al and al + 32), so the stage weights are read once
     int al_u[2], c_u[2];
     const __nv_bfloat16* rows_u[2][4];
 #pragma unroll
     for (int u = 0; u < 2; ++u) {
-      const int unit = pt + u * MX_PRODUCERS;
-      al_u[u] = unit >> 3;
-      c_u[u] = unit & 7;
+      al_u[u] = (pt >> 3) + 32 * u;
+      c_u[u] = pt & 7;
       const size_t a = (size_t)(a0 + al_u[u]);
       rows_u[u][0] = Xh + a * P.K_pad;
       rows_u[u][1] = Xl + a * P.K_pad;
@@ -392,36 +394,40 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
       const int s = i % MX_STAGES, r = i / MX_STAGES;
       if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)) break;
       if (!mbar_wait(smem_u32(&bar_full_w[s]), r & 1, &s_abort, err, 8)) break;
+      // W of both units in FP32 (hi + lo is exact in FP32)
+      float wr[2][8], wi[2][8];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const uint32_t A_h[4] = {pre[u][0].x, pre[u][0].y, pre[u][0].z, pre[u][0].w};
-        const uint32_t A_l[4] = {pre[u][1].x, pre[u][1].y, pre[u][1].z, pre[u][1].w};
-        const uint32_t B_h[4] = {pre[u][2].x, pre[u][2].y, pre[u][2].z, pre[u][2].w};
-        const uint32_t B_l[4] = {pre[u][3].x, pre[u][3].y, pre[u][3].z, pre[u][3].w};
-        float wr[8], wi[8];
+      for (int u = 0; u < 2; ++u)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          wr[2 * q] = bf_lo(A_h[q]) + bf_lo(A_l[q]);
-          wr[2 * q + 1] = bf_hi(A_h[q]) + bf_hi(A_l[q]);
-          wi[2 * q] = bf_lo(B_h[q]) + bf_lo(B_l[q]);
-          wi[2 * q + 1] = bf_hi(B_h[q]) + bf_hi(B_l[q]);
+          const uint32_t ah = (&pre[u][0].x)[q], al = (&pre[u][1].x)[q];
+          const uint32_t bh = (&pre[u][2].x)[q], bl = (&pre[u][3].x)[q];
+          wr[u][2 * q] = bf_lo(ah) + bf_lo(al);
+          wr[u][2 * q + 1] = bf_hi(ah) + bf_hi(al);
+          wi[u][2 * q] = bf_lo(bh) + bf_lo(bl);
+          wi[u][2 * q + 1] = bf_hi(bh) + bf_hi(bl);
         }
-        const int al = al_u[u], c = c_u[u];
-        const uint32_t offr = sw128_off(2 * al, c), offi = sw128_off(2 * al + 1, c);
-        for (int j = 0; j < n_om; ++j) {
-          const float4* wz = reinterpret_cast<const float4*>(w_s(s, j) + c * 8);
+      const int c = c_u[0];
+      for (int j = 0; j < n_om; ++j) {
+        const float4* wz = reinterpret_cast<const float4*>(w_s(s, j) + c * 8);
+        float4 w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[q] = wz[q];   // weights of k = 2q, 2q+1 of the chunk
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int a_l = al_u[u];
           uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            const float4 w = wz[q];            // weights of k = 2q, 2q+1 in this chunk
             // w conj(W) = (dr Wr + di Wi) + i (di Wr - dr Wi)
-            const float ur0 = w.x * wr[2 * q] + w.y * wi[2 * q];
-            const float ui0 = w.y * wr[2 * q] - w.x * wi[2 * q];
-            const float ur1 = w.z * wr[2 * q + 1] + w.w * wi[2 * q + 1];
-            const float ui1 = w.w * wr[2 * q + 1] - w.z * wi[2 * q + 1];
+            const float ur0 = w[q].x * wr[u][2 * q] + w[q].y * wi[u][2 * q];
+            const float ui0 = w[q].y * wr[u][2 * q] - w[q].x * wi[u][2 * q];
+            const float ur1 = w[q].z * wr[u][2 * q + 1] + w[q].w * wi[u][2 * q + 1];
+            const float ui1 = w[q].w * wr[u][2 * q + 1] - w[q].z * wi[u][2 * q + 1];
             rh[q] = pack_split(ur0, ur1, rl[q]);
             ih[q] = pack_split(ui0, ui1, il[q]);
           }
+          const uint32_t offr = sw128_off(2 * a_l, c), offi = sw128_off(2 * a_l + 1, c);
           *reinterpret_cast<uint4*>(yh_s(s, j) + offr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
           *reinterpret_cast<uint4*>(yl_s(s, j) + offr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
           *reinterpret_cast<uint4*>(yh_s(s, j) + offi) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
