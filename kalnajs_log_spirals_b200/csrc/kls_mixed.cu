@@ -17,8 +17,9 @@
 //
 // Table: Xh/Xl [2 Npad][K_pad] BF16, built once by split_table_kernel from
 // the FP64 table.  Contraction CTA (one per SM, 16 warps):
-//   warp 0       TMA: X tile 128 rows x 64 k (hi, lo; 128B swizzle) and the
-//                FP32 weights of the stage (bulk copy)
+//   warp 0       TMA: X tile 128 rows x 64 k (hi, lo; 128B swizzle)
+//   warp 3       bulk copies of the FP32 weights into their own 8-deep ring,
+//                so the producers never wait for them on the critical path
 //   warp 1       MMA issuer: tcgen05.mma kind::f16 M=128 N=128 K=16, 3
 //                products per k-step per omega, 2 TMEM accumulator buffers
 //   warp 2       TMEM allocation / release (512 columns)
@@ -50,8 +51,10 @@ constexpr int MX_THREADS = 512;
 constexpr int MX_TILE_X = MX_BM * MX_BK * 2;            // 16 KB per part
 constexpr int MX_TILE_Y = MX_BN * MX_BK * 2;            // 16 KB per part per omega
 constexpr int MX_W_BYTES = MX_BK * 8;                   // float2 weights per omega per stage
-constexpr int MX_STAGE_BYTES = 2 * MX_TILE_X + 2 * MX_OMEGA * MX_TILE_Y + 1024;  // 97 KB + w
-constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + 1024;            // + alignment
+constexpr int MX_WSTAGES = 8;              // weights ring: filled up to 8 k-blocks ahead
+constexpr int MX_STAGE_BYTES = 2 * MX_TILE_X + 2 * MX_OMEGA * MX_TILE_Y;          // 96 KB
+constexpr int MX_WRING_BYTES = MX_WSTAGES * MX_OMEGA * MX_W_BYTES;                // 8 KB
+constexpr size_t MX_SMEM = (size_t)MX_STAGES * MX_STAGE_BYTES + MX_WRING_BYTES + 1024;
 constexpr int MX_ACC_COLS = MX_OMEGA * MX_BN;          // 256 fp32 columns per buffer
 constexpr int MX_TMEM_COLS = 2 * MX_ACC_COLS;          // 512
 constexpr unsigned long long MX_WAIT_NS = 2000000000ull;   // 2 s per wait
@@ -215,12 +218,17 @@ __global__ void split_table_kernel(const double* __restrict__ Wre, const double*
   }
 }
 
+// FP32 copy of the weights, permuted inside each 64-k block so that the
+// producers' 16-byte reads (k-chunk c of 8, pair q of 2) are conflict-free:
+// k = 8c + 2q + h is stored at position 2 (8q + c) + h of its block.
 __global__ void weights32_kernel(int64_t total, const double2* __restrict__ wt,
                                  float2* __restrict__ wt32) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
-    double2 v = wt[i];
-    wt32[i] = make_float2((float)v.x, (float)v.y);
+    const double2 v = wt[i];
+    const int k = (int)(i & (MX_BK - 1));
+    const int c = k >> 3, q = (k >> 1) & 3, h = k & 1;
+    wt32[(i & ~(int64_t)(MX_BK - 1)) + 2 * (8 * q + c) + h] = make_float2((float)v.x, (float)v.y);
   }
 }
 
@@ -246,8 +254,9 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
                       const float2* __restrict__ wt32, double* __restrict__ part,
                       int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t bar_full_x[MX_STAGES], bar_full_w[MX_STAGES],
-      bar_full_y[MX_STAGES], bar_empty[MX_STAGES], bar_acc_full[2], bar_acc_empty[2], bar_done;
+  __shared__ __align__(8) uint64_t bar_full_x[MX_STAGES], bar_full_y[MX_STAGES],
+      bar_empty[MX_STAGES], bar_w_full[MX_WSTAGES], bar_w_empty[MX_WSTAGES], bar_acc_full[2],
+      bar_acc_empty[2], bar_done;
   __shared__ uint32_t s_tmem;
   __shared__ volatile int s_abort;
 
@@ -271,18 +280,21 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   auto yl_s = [&](int s, int j) {
     return smem + (size_t)s * MX_STAGE_BYTES + 2 * MX_TILE_X + (size_t)(MX_OMEGA + j) * MX_TILE_Y;
   };
-  auto w_s = [&](int s, int j) {
-    return reinterpret_cast<float2*>(smem + (size_t)s * MX_STAGE_BYTES + 2 * MX_TILE_X +
-                                     2 * MX_OMEGA * MX_TILE_Y) + j * MX_BK;
+  auto w_s = [&](int ws, int j) {
+    return reinterpret_cast<float2*>(smem + (size_t)MX_STAGES * MX_STAGE_BYTES +
+                                     (size_t)ws * MX_OMEGA * MX_W_BYTES) + j * MX_BK;
   };
 
   if (tid == 0) {
     s_abort = 0;
     for (int s = 0; s < MX_STAGES; ++s) {
       mbar_init(smem_u32(&bar_full_x[s]), 1);
-      mbar_init(smem_u32(&bar_full_w[s]), 1);
       mbar_init(smem_u32(&bar_full_y[s]), MX_PRODUCERS);
       mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    for (int s = 0; s < MX_WSTAGES; ++s) {
+      mbar_init(smem_u32(&bar_w_full[s]), 1);
+      mbar_init(smem_u32(&bar_w_empty[s]), MX_PRODUCERS);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&bar_acc_full[b]), 1);
@@ -304,17 +316,13 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   const size_t R = (size_t)P.rows;
 
   if (warp == 0) {
-    // ---------------- TMA: X tiles + stage weights
+    // ---------------- TMA: X tiles
     if (lane == 0 && nkb > 0) {
       int issued = 0;
       for (int i = 0; i < nkb; ++i) {
         const int s = i % MX_STAGES, r = i / MX_STAGES;
         if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 1)) break;
         const int64_t kx = (int64_t)(kb0 + i) * MX_BK;
-        const uint32_t wb = smem_u32(&bar_full_w[s]);
-        mbar_arrive_tx(wb, n_om * MX_W_BYTES);
-        for (int j = 0; j < n_om; ++j)
-          bulk_load(smem_u32(w_s(s, j)), wt32 + (size_t)(om0 + j) * P.K_pad + kx, MX_W_BYTES, wb);
         const uint32_t fb = smem_u32(&bar_full_x[s]);
         mbar_arrive_tx(fb, 2 * MX_TILE_X);
         tma_load_2d(smem_u32(xh_s(s)), &tm_h, (int)kx, m0, fb);
@@ -322,10 +330,25 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
         issued = i + 1;
       }
       // the last copies into each stage land before the CTA may exit
-      for (int i = max(0, issued - MX_STAGES); i < issued; ++i) {
+      for (int i = max(0, issued - MX_STAGES); i < issued; ++i)
         mbar_wait(smem_u32(&bar_full_x[i % MX_STAGES]), (i / MX_STAGES) & 1, nullptr, err, 6);
-        mbar_wait(smem_u32(&bar_full_w[i % MX_STAGES]), (i / MX_STAGES) & 1, nullptr, err, 6);
+    }
+  } else if (warp == 3) {
+    // ---------------- weights ring: bulk copies up to MX_WSTAGES k-blocks ahead
+    if (lane == 0 && nkb > 0) {
+      int issued = 0;
+      for (int i = 0; i < nkb; ++i) {
+        const int ws = i % MX_WSTAGES, r = i / MX_WSTAGES;
+        if (!mbar_wait(smem_u32(&bar_w_empty[ws]), (r & 1) ^ 1, &s_abort, err, 10)) break;
+        const int64_t kx = (int64_t)(kb0 + i) * MX_BK;
+        const uint32_t wb = smem_u32(&bar_w_full[ws]);
+        mbar_arrive_tx(wb, n_om * MX_W_BYTES);
+        for (int j = 0; j < n_om; ++j)
+          bulk_load(smem_u32(w_s(ws, j)), wt32 + (size_t)(om0 + j) * P.K_pad + kx, MX_W_BYTES, wb);
+        issued = i + 1;
       }
+      for (int i = max(0, issued - MX_WSTAGES); i < issued; ++i)
+        mbar_wait(smem_u32(&bar_w_full[i % MX_WSTAGES]), (i / MX_WSTAGES) & 1, nullptr, err, 6);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer
@@ -393,7 +416,8 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
     for (int i = 0; i < nkb; ++i) {
       const int s = i % MX_STAGES, r = i / MX_STAGES;
       if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)) break;
-      if (!mbar_wait(smem_u32(&bar_full_w[s]), r & 1, &s_abort, err, 8)) break;
+      const int ws = i % MX_WSTAGES;
+      if (!mbar_wait(smem_u32(&bar_w_full[ws]), (i / MX_WSTAGES) & 1, &s_abort, err, 8)) break;
       // W of both units in FP32 (hi + lo is exact in FP32)
       float wr[2][8], wi[2][8];
 #pragma unroll
@@ -408,11 +432,20 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
           wi[u][2 * q + 1] = bf_hi(bh) + bf_hi(bl);
         }
       const int c = c_u[0];
-      for (int j = 0; j < n_om; ++j) {
-        const float4* wz = reinterpret_cast<const float4*>(w_s(s, j) + c * 8);
-        float4 w[4];
+      // weights of k = 2q, 2q+1 of the chunk, both omegas loaded up front
+      float4 wq[MX_OMEGA][4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) w[q] = wz[q];   // weights of k = 2q, 2q+1 of the chunk
+      for (int j = 0; j < MX_OMEGA; ++j) {
+        // permuted block layout: pair q of chunk c is float4 number 8q + c
+        const float4* wz = reinterpret_cast<const float4*>(w_s(ws, j)) + c;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          wq[j][q] = j < n_om ? wz[8 * q] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int j = 0; j < MX_OMEGA; ++j) {
+        if (j >= n_om) break;
+        const float4* w = wq[j];
 #pragma unroll
         for (int u = 0; u < 2; ++u) {
           const int a_l = al_u[u];
@@ -434,6 +467,7 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
           *reinterpret_cast<uint4*>(yl_s(s, j) + offi) = make_uint4(il[0], il[1], il[2], il[3]);
         }
       }
+      mbar_arrive(smem_u32(&bar_w_empty[ws]));      // weights slot read
       fence_proxy_async();
       mbar_arrive(smem_u32(&bar_full_y[s]));
       if (i + 1 < nkb) prefetch(i + 1);
@@ -450,7 +484,9 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
       if (nkb > 0 && !ok) break;
       tc_fence_after();
       for (int j = 0; j < n_om; ++j) {
-        double* out = part + (((size_t)(om0 + j) * P.splits + split) * R + row) * R + 2 * a0;
+        // partial plane of (omega, split), stored column by column (element
+        // (row, col) at col * R + row): a warp's 32 rows are 256 contiguous bytes
+        double* out = part + ((size_t)(om0 + j) * P.splits + split) * R * R + row;
         for (int cc = 0; cc < MX_BN / 32; ++cc) {
           uint32_t v[32];
           if (nkb > 0) {
@@ -462,17 +498,20 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
 #pragma unroll
             for (int t = 0; t < 32; ++t) v[t] = 0u;
           }
-          double2* o2 = reinterpret_cast<double2*>(out + cc * 32);
+          double* o = out + (size_t)(2 * a0 + cc * 32) * R;
 #pragma unroll
-          for (int t = 0; t < 16; ++t) {
-            double2 acc = make_double2((double)__uint_as_float(v[2 * t]),
-                                       (double)__uint_as_float(v[2 * t + 1]));
+          for (int h = 0; h < 2; ++h) {
+            double old[16];
             if (ch > 0) {
-              const double2 old = o2[t];
-              acc.x += old.x;
-              acc.y += old.y;
+#pragma unroll
+              for (int t = 0; t < 16; ++t) old[t] = o[(size_t)(16 * h + t) * R];
+            } else {
+#pragma unroll
+              for (int t = 0; t < 16; ++t) old[t] = 0.0;
             }
-            o2[t] = acc;
+#pragma unroll
+            for (int t = 0; t < 16; ++t)
+              o[(size_t)(16 * h + t) * R] = old[t] + (double)__uint_as_float(v[16 * h + t]);
           }
         }
       }
@@ -501,19 +540,21 @@ __global__ void mixed_reduce_kernel(int Na, int Npad, int splits, double G,
   const int z = blockIdx.y;
   const size_t R = 2 * (size_t)Npad;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
-    const int b = e / Na, a = e % Na;
+    const int b = e % Na, a = e / Na;          // consecutive threads: consecutive rows b
     double mr = 0.0, mi = 0.0;
     for (int s = 0; s < splits; ++s) {
+      // plane of (omega, split), element (row c, column n) at n * R + c
       const double* P = part + ((size_t)z * splits + s) * R * R;
-      const double2 pr = *reinterpret_cast<const double2*>(P + (size_t)b * R + 2 * a);
-      const double2 pi = *reinterpret_cast<const double2*>(P + (size_t)(Npad + b) * R + 2 * a);
-      mr += pr.x - pi.y;
-      mi += pr.y + pi.x;
+      const double pr_r = P[(size_t)(2 * a) * R + b], pr_i = P[(size_t)(2 * a + 1) * R + b];
+      const double pi_r = P[(size_t)(2 * a) * R + Npad + b];
+      const double pi_i = P[(size_t)(2 * a + 1) * R + Npad + b];
+      mr += pr_r - pi_i;
+      mi += pr_i + pi_r;
     }
     const double n = Nk[a];
     const double Mr = (mr * G) * n, Mi = (mi * G) * n;
-    A[(size_t)z * Na * Na + e] = make_double2((a == b ? 1.0 : 0.0) - Mr, -Mi);
-    if (Mout && z == 0) Mout[e] = make_double2(Mr, Mi);
+    A[(size_t)z * Na * Na + (size_t)b * Na + a] = make_double2((a == b ? 1.0 : 0.0) - Mr, -Mi);
+    if (Mout && z == 0) Mout[(size_t)b * Na + a] = make_double2(Mr, Mi);
   }
 }
 
