@@ -205,6 +205,25 @@ int kls_newton_hybrid(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_ne
 int kls_det_lu_static(const double* d_A_ri, int n_matrices, int N, double* d_det_ri,
                       double* d_log_abs, void* stream);
 
+/* ---- learned root proposer (no reference counterpart) -------------------- *
+ * MLP features (5) -> width (GELU) x (depth - 1) -> outputs (3), FP32 master
+ * weights, BF16 tensor-core GEMMs with FP32 accumulation, Adam; trained and
+ * run on the device by the library's own kernels.  Parameter order (flat
+ * fp32): for each layer, W [out][in] row-major then b [out].               */
+typedef struct kls_mlp kls_mlp;
+int kls_mlp_create(int device, int width, int depth, uint64_t seed, kls_mlp** out);
+int kls_mlp_destroy(kls_mlp* mlp);
+int kls_mlp_num_params(const kls_mlp* mlp, int64_t* n);
+int kls_mlp_get_params(kls_mlp* mlp, float* params);
+int kls_mlp_set_params(kls_mlp* mlp, const float* params);
+/* X [n][5] -> Y [n][3], host buffers. */
+int kls_mlp_forward(kls_mlp* mlp, const float* X, int n, float* Y);
+/* Mean-squared-error loss and its gradient (flat, params order) on one batch. */
+int kls_mlp_grad(kls_mlp* mlp, const float* X, const float* T, int n, float* grads, float* loss);
+/* Adam over shuffled minibatches; loss_hist[e] = mean minibatch loss of epoch e. */
+int kls_mlp_train(kls_mlp* mlp, const float* X, const float* T, int n, int epochs, int batch,
+                  float lr, uint64_t seed, float* loss_hist);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Per-stage device time (ms) of the last det batch when timing is enabled:
  * [0] weights, [1] contraction, [2] reduce/epilogue, [3] LU.               */

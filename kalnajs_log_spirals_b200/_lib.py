@@ -99,6 +99,16 @@ SIGNATURES = {
                                     C.POINTER(kls_hybrid_cfg), C.POINTER(kls_newton_result),
                                     C.POINTER(C.c_int32), _D]),
     "kls_det_lu_static": (C.c_int, [_P, C.c_int, C.c_int, _P, _P, _P]),
+    "kls_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_uint64, C.POINTER(_P)]),
+    "kls_mlp_destroy": (C.c_int, [_P]),
+    "kls_mlp_num_params": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "kls_mlp_get_params": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "kls_mlp_set_params": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "kls_mlp_forward": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float)]),
+    "kls_mlp_grad": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
+                               C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "kls_mlp_train": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
+                                C.c_int, C.c_int, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_launch_count": (C.c_int64, [_P]),

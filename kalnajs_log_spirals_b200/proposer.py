@@ -1,0 +1,168 @@
+"""Learned root proposer (no counterpart in the reference).
+
+A small MLP maps (n_zang, q1, m, Omega_p, gamma) to features of
+det(I - M(omega)) -- (log|det|, sin arg det, cos arg det) -- and proposes a
+Newton start as the minimum of its predicted log|det| over the scan region, in
+place of the reference's grid scan (GridScan.jl:25-88).  FP64 Newton on the
+exact determinant refines every proposal; a proposal counts only if it
+converges to the root the scan-started Newton finds.
+
+The network is trained on the GPU by libkls.so's own BF16 forward/backward
+kernels (kls_mlp_*) on samples that batched scans of seeded random models
+produce.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import time
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+from .config import KalnajsConfig, copy_config
+
+LOG_SCALE = 10.0          # log|det| is learned as log|det| / LOG_SCALE
+
+
+def features(n_zang, q1, m, Omega_p, gamma) -> np.ndarray:
+    """Normalised inputs, float32 [n, 5]."""
+    b = np.broadcast_arrays(*(np.asarray(v, dtype=np.float64) for v in
+                              (n_zang, q1, m, Omega_p, gamma)))
+    x = np.stack([(b[0] - 4.0) / 2.0, (b[1] - 8.0) / 4.0, (b[2] - 2.5) * 2.0,
+                  (b[3] - 0.5) / 0.3, (b[4] - 0.155) / 0.145], axis=-1)
+    return np.ascontiguousarray(x.reshape(-1, 5), dtype=np.float32)
+
+
+def targets(det: np.ndarray, log_abs: Optional[np.ndarray] = None) -> np.ndarray:
+    """(log|det| / LOG_SCALE, sin arg, cos arg), float32 [n, 3]."""
+    d = np.asarray(det, dtype=np.complex128).reshape(-1)
+    la = np.log(np.abs(d)) if log_abs is None else np.asarray(log_abs).reshape(-1)
+    ph = np.angle(d)
+    t = np.stack([la / LOG_SCALE, np.sin(ph), np.cos(ph)], axis=-1)
+    return np.ascontiguousarray(t, dtype=np.float32)
+
+
+class MLP:
+    """kls_mlp handle: width-`width` GELU MLP with `depth` linear layers."""
+
+    def __init__(self, width: int = 256, depth: int = 4, seed: int = 0, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(None, self.lib.kls_mlp_create(device, width, depth, seed, C.byref(h)))
+        self.h = h
+        self.width, self.depth = width, depth
+        n = C.c_int64()
+        self.lib.kls_mlp_num_params(self.h, C.byref(n))
+        self.nparams = int(n.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.kls_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _f(a) -> C.POINTER(C.c_float):
+        return a.ctypes.data_as(C.POINTER(C.c_float))
+
+    def _ck(self, code):
+        if code:
+            raise _lib.KlsError(code, self.lib.kls_create_error().decode())
+
+    def params(self) -> np.ndarray:
+        p = np.empty(self.nparams, dtype=np.float32)
+        self._ck(self.lib.kls_mlp_get_params(self.h, self._f(p)))
+        return p
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.nparams
+        self._ck(self.lib.kls_mlp_set_params(self.h, self._f(p)))
+
+    def forward(self, X: np.ndarray) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.empty((X.shape[0], 3), dtype=np.float32)
+        self._ck(self.lib.kls_mlp_forward(self.h, self._f(X), X.shape[0], self._f(Y)))
+        return Y
+
+    def grad(self, X: np.ndarray, T: np.ndarray) -> Tuple[np.ndarray, float]:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        g = np.empty(self.nparams, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        self._ck(self.lib.kls_mlp_grad(self.h, self._f(X), self._f(T), X.shape[0], self._f(g),
+                                       self._f(loss)))
+        return g, float(loss[0])
+
+    def train(self, X: np.ndarray, T: np.ndarray, epochs: int = 40, batch: int = 4096,
+              lr: float = 2e-3, seed: int = 0) -> np.ndarray:
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        hist = np.zeros(max(epochs, 1), dtype=np.float32)
+        self._ck(self.lib.kls_mlp_train(self.h, self._f(X), self._f(T), X.shape[0], epochs, batch,
+                                        lr, seed, self._f(hist)))
+        return hist[:epochs]
+
+
+# ---------------------------------------------------------------------------
+# training data from batched scans of random models
+# ---------------------------------------------------------------------------
+@dataclasses.dataclass
+class ModelSpec:
+    n_zang: int
+    q1: float
+    m: int
+
+
+def random_models(n: int, seed: int) -> List[ModelSpec]:
+    """n_zang in {2..6}, q1 ~ U[4, 12] (real), m in {2, 3}."""
+    rng = np.random.default_rng(seed)
+    return [ModelSpec(int(rng.integers(2, 7)), float(rng.uniform(4.0, 12.0)), int(rng.integers(2, 4)))
+            for _ in range(n)]
+
+
+def model_config(base: KalnajsConfig, spec: ModelSpec) -> KalnajsConfig:
+    c = copy_config(base)
+    c.model.n_zang, c.model.q1, c.physics.m = spec.n_zang, spec.q1, spec.m
+    return c
+
+
+def scan_samples(base: KalnajsConfig, specs: Sequence[ModelSpec], n_Op: int, n_gamma: int,
+                 Op_range=(0.2, 0.8), g_range=(0.01, 0.30), mixed: bool = True,
+                 device: int = 0):
+    """Batched scans: features and targets of every (model, omega) grid point."""
+    from . import api
+    Op = np.linspace(*Op_range, n_Op)
+    gm = np.linspace(*g_range, n_gamma)
+    OP, GM = np.meshgrid(Op, gm, indexing="xy")
+    Xs, Ts = [], []
+    for spec in specs:
+        cfg = model_config(base, spec)
+        pc = api.precompute_all(cfg, device=device)
+        dev = api.to_device(pc, api.GPUType.NVIDIA, "Float32" if mixed else "Float64")
+        om = spec.m * OP.ravel() + 1j * GM.ravel()
+        d, la = api.compute_determinant_batched(om, pc, dev, batch_size=64, log_abs=True)
+        pc.close()
+        ok = np.isfinite(la) & np.isfinite(d)
+        Xs.append(features(spec.n_zang, spec.q1, spec.m, OP.ravel()[ok], GM.ravel()[ok]))
+        Ts.append(targets(d[ok], la[ok]))
+    return np.concatenate(Xs), np.concatenate(Ts)
+
+
+def propose(mlp: MLP, spec: ModelSpec, n_Op: int = 256, n_gamma: int = 128,
+            Op_range=(0.2, 0.8), g_range=(0.01, 0.30)) -> Tuple[float, float]:
+    """Newton start: grid point of minimal predicted log|det|."""
+    Op = np.linspace(*Op_range, n_Op)
+    gm = np.linspace(*g_range, n_gamma)
+    OP, GM = np.meshgrid(Op, gm, indexing="xy")
+    y = mlp.forward(features(spec.n_zang, spec.q1, spec.m, OP.ravel(), GM.ravel()))
+    i = int(np.argmin(y[:, 0]))
+    return float(OP.ravel()[i]), float(GM.ravel()[i])
