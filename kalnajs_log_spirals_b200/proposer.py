@@ -157,12 +157,33 @@ def scan_samples(base: KalnajsConfig, specs: Sequence[ModelSpec], n_Op: int, n_g
     return np.concatenate(Xs), np.concatenate(Ts)
 
 
-def propose(mlp: MLP, spec: ModelSpec, n_Op: int = 256, n_gamma: int = 128,
-            Op_range=(0.2, 0.8), g_range=(0.01, 0.30)) -> Tuple[float, float]:
-    """Newton start: grid point of minimal predicted log|det|."""
+def shortlist(mlp: MLP, spec: ModelSpec, k: int = 48, n_Op: int = 41, n_gamma: int = 20,
+              Op_range=(0.2, 0.6), g_range=(0.01, 0.2)):
+    """The k points of the scan grid with the lowest predicted log|det|.
+
+    The grid is the reference scan's (ScanConfig defaults,
+    Configuration.jl:72-79); returns (Omega_p, gamma, column-major index)
+    arrays sorted by that index.
+    """
     Op = np.linspace(*Op_range, n_Op)
     gm = np.linspace(*g_range, n_gamma)
-    OP, GM = np.meshgrid(Op, gm, indexing="xy")
-    y = mlp.forward(features(spec.n_zang, spec.q1, spec.m, OP.ravel(), GM.ravel()))
-    i = int(np.argmin(y[:, 0]))
-    return float(OP.ravel()[i]), float(GM.ravel()[i])
+    OP, GM = np.meshgrid(Op, gm, indexing="xy")           # [n_gamma, n_Op]
+    y = mlp.forward(features(spec.n_zang, spec.q1, spec.m, OP.ravel(order="F"),
+                             GM.ravel(order="F")))
+    idx = np.sort(np.argsort(y[:, 0], kind="stable")[:k])   # column-major grid indices
+    return OP.ravel(order="F")[idx], GM.ravel(order="F")[idx], idx
+
+
+def propose(mlp: MLP, spec: ModelSpec, det_fn, k: int = 48, **grid) -> Tuple[float, float, int]:
+    """Newton start in place of grid_scan + find_minimum (GridScan.jl:25-88, 234-246).
+
+    ``det_fn(omegas) -> dets`` evaluates the true determinant at the k
+    shortlisted grid points (one batch); the start is the shortlisted point of
+    minimal |det|, first in column-major order as find_minimum takes it.  When
+    the scan's own argmin is on the shortlist this is exactly the scan's start.
+    Returns (Omega_p, gamma, determinant evaluations used).
+    """
+    Op, gm, _ = shortlist(mlp, spec, k=k, **grid)
+    d = np.asarray(det_fn(spec.m * Op + 1j * gm))
+    i = int(np.argmin(np.abs(d)))
+    return float(Op[i]), float(gm[i]), len(Op)
