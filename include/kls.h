@@ -224,6 +224,61 @@ int kls_mlp_grad(kls_mlp* mlp, const float* X, const float* T, int n, float* gra
 int kls_mlp_train(kls_mlp* mlp, const float* X, const float* T, int n, int epochs, int batch,
                   float lr, uint64_t seed, float* loss_hist);
 
+/* ---- uneven batch over models --------------------------------------------- *
+ * The reference scans one model at a time (grid_scan, GridScan.jl:25-88; its
+ * multi-GPU form GridScan.jl:125-197 splits one model's omega columns over
+ * devices).  A kls_multi evaluates `batch` omegas for each of n_models
+ * precomputed contexts (any mix of NR, Ne, N_alpha and l range, one device)
+ * per pass: the contraction of every model is one persistent launch, and the
+ * whole pass (omega upload, weights, contraction, split reduction, LU,
+ * result download) is one CUDA graph replay.  Each model keeps its
+ * context's K split count (tune with kls_autotune before creating the
+ * batch), so every determinant is bitwise what kls_det_batch returns for
+ * that context.  The contexts must outlive the batch and are not modified;
+ * a batch is not re-entrant.  Errors: kls_multi_last_error (NULL handle:
+ * errors of kls_multi_create).                                              */
+typedef struct kls_multi kls_multi;
+typedef struct kls_multi_info {
+    int32_t n_models, batch, mode;
+    int32_t n_items;              /* work items of the persistent contraction */
+    int32_t grid;                 /* CTAs of the persistent contraction       */
+    int32_t graph;                /* 1: passes replay a captured CUDA graph    */
+    int32_t launches_per_replay;  /* kernels in one pass                      */
+    int64_t replays;              /* passes so far                            */
+    double  last_ms;              /* device time of the last pass (ms)        */
+} kls_multi_info;
+int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, kls_multi** out);
+int kls_multi_destroy(kls_multi* mm);
+const char* kls_multi_last_error(const kls_multi* mm);
+/* omega_ri [n_models][n] interleaved; det_ri [n_models][n] interleaved;
+ * log_abs [n_models][n] (may be NULL).                                      */
+int kls_multi_det(kls_multi* mm, const double* omega_ri, int n, double* det_ri, double* log_abs);
+/* grid_scan of every model over one (Omega_p, gamma) grid, omega =
+ * m_model * Omega_p + i gamma; per model a [n_gamma, n_Op] column-major
+ * block of det_grid_ri / log_abs_grid and the column-major argmin
+ * (Omega_p0[i], gamma0[i]) as in GridScan.jl:234-246.  sc->mode and
+ * sc->batch are ignored (the batch's own).                                  */
+int kls_scan_multi(kls_multi* mm, const kls_scan_cfg* sc, double* det_grid_ri,
+                   double* log_abs_grid, double* Omega_p0, double* gamma0);
+int kls_multi_get_info(const kls_multi* mm, kls_multi_info* out);
+
+/* ---- autotuner (no reference counterpart) ---------------------------------- *
+ * Times the contraction of `mode` for the context at `batch` omegas per call
+ * with each candidate K split count (the occupancy-derived default, half,
+ * twice and three times it) and keeps the fastest for the context.  Results
+ * are cached per (device name, mode, N_alpha_pad, K_pad, batch) for the
+ * process, and in the text file named by the environment variable
+ * KLS_TUNE_CACHE when it is set.                                            */
+typedef struct kls_tune_result {
+    int32_t mode;
+    int32_t splits;               /* chosen K splits                          */
+    int32_t default_splits;       /* the untuned choice                       */
+    int32_t candidates;           /* candidates timed (0: from the cache)     */
+    double  ms_per_omega;         /* contraction time of the choice           */
+    double  default_ms_per_omega; /* and of the untuned choice (0: cached)    */
+} kls_tune_result;
+int kls_autotune(kls_ctx* ctx, int mode, int batch, kls_tune_result* out);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Per-stage device time (ms) of the last det batch when timing is enabled:
  * [0] weights, [1] contraction, [2] reduce/epilogue, [3] LU.               */

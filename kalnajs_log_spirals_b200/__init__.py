@@ -9,7 +9,7 @@ from .config import (CPUConfig, GPUConfig, GridConfig, IOConfig, KalnajsConfig, 
                      get_float_type, get_n_l, get_NPh, load_config, load_model, precision_cpu,
                      precision_gpu, save_config)
 from .api import (DevicePrecomputed, GPUType, NewtonResult, OrbitData, PrecomputedData,
-                  ToomreZangModel, build_M_matrix, compute_determinant,
+                  ModelBatch, ToomreZangModel, TuneResult, autotune, build_M_matrix, compute_determinant,
                   compute_determinant_batched, create_toomre_zang_model, detect_gpu_type,
                   find_minimum, grid_scan, newton_search, precompute_all, to_device)
 from ._lib import KLS_MODE_FP64, KLS_MODE_MIXED, KlsError
@@ -22,5 +22,5 @@ __all__ = [
     "create_toomre_zang_model", "PrecomputedData", "OrbitData", "precompute_all",
     "DevicePrecomputed", "to_device", "compute_determinant", "compute_determinant_batched",
     "build_M_matrix", "grid_scan", "find_minimum", "newton_search", "NewtonResult", "KlsError",
-    "KLS_MODE_FP64", "KLS_MODE_MIXED",
+    "KLS_MODE_FP64", "KLS_MODE_MIXED", "ModelBatch", "autotune", "TuneResult",
 ]

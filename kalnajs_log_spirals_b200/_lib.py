@@ -71,6 +71,19 @@ class kls_scan_cfg(C.Structure):
                 ("gamma_max", C.c_double), ("mode", C.c_int32), ("batch", C.c_int32)]
 
 
+class kls_multi_info(C.Structure):
+    _fields_ = [("n_models", C.c_int32), ("batch", C.c_int32), ("mode", C.c_int32),
+                ("n_items", C.c_int32), ("grid", C.c_int32), ("graph", C.c_int32),
+                ("launches_per_replay", C.c_int32), ("replays", C.c_int64),
+                ("last_ms", C.c_double)]
+
+
+class kls_tune_result(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("splits", C.c_int32), ("default_splits", C.c_int32),
+                ("candidates", C.c_int32), ("ms_per_omega", C.c_double),
+                ("default_ms_per_omega", C.c_double)]
+
+
 _P = C.c_void_p
 _D = C.POINTER(C.c_double)
 
@@ -109,6 +122,13 @@ SIGNATURES = {
                                C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "kls_mlp_train": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int,
                                 C.c_int, C.c_int, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "kls_multi_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_int, C.c_int, C.POINTER(_P)]),
+    "kls_multi_destroy": (C.c_int, [_P]),
+    "kls_multi_last_error": (C.c_char_p, [_P]),
+    "kls_multi_det": (C.c_int, [_P, _D, C.c_int, _D, _D]),
+    "kls_scan_multi": (C.c_int, [_P, C.POINTER(kls_scan_cfg), _D, _D, _D, _D]),
+    "kls_multi_get_info": (C.c_int, [_P, C.POINTER(kls_multi_info)]),
+    "kls_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(kls_tune_result)]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_launch_count": (C.c_int64, [_P]),

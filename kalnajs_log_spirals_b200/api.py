@@ -13,6 +13,7 @@ BasisFunctions.jl:381-437      DevicePrecomputed, to_device
 MatrixBuilder.jl:197-244       compute_determinant, compute_determinant_batched,
                                build_M_matrix
 GridScan.jl:25-88, 234-246     grid_scan, find_minimum
+GridScan.jl:125-197            ModelBatch (many models per launch), autotune
 NewtonSolver.jl:19-172         NewtonResult, newton_search
 GPUBackend.jl:27-31, 50-72     GPUType, detect_gpu_type
 =============================  ==============================================
@@ -529,3 +530,97 @@ def newton_search_hybrid(config: KalnajsConfig, precomputed: PrecomputedData,
                      hist[:min(res.iterations, int(n.max_iter))].copy(), int(res.det_evals))
     r.mixed_evals, r.fp64_evals = int(ev[0]), int(ev[1])
     return r
+
+
+# ---------------------------------------------------------------------------
+# Uneven batch over models and the autotuner (no reference counterpart)
+# ---------------------------------------------------------------------------
+@dataclass
+class TuneResult:
+    mode: int
+    splits: int
+    default_splits: int
+    candidates: int
+    ms_per_omega: float
+    default_ms_per_omega: float
+
+
+def autotune(precomputed: PrecomputedData, Tgpu="Float64", batch: int = 2) -> TuneResult:
+    """Choose the context's K split count for `Tgpu` by timing (kls_autotune)."""
+    r = _lib.kls_tune_result()
+    precomputed.ctx.call("kls_autotune", _mode_for(Tgpu), int(batch), C.byref(r))
+    return TuneResult(r.mode, r.splits, r.default_splits, r.candidates, r.ms_per_omega,
+                      r.default_ms_per_omega)
+
+
+class ModelBatch:
+    """Many precomputed models of any sizes evaluated together (kls_multi).
+
+    Each pass evaluates `batch` omegas per model: one persistent contraction
+    launch for all models, replayed from a captured CUDA graph.  Results are
+    bitwise those of compute_determinant_batched on each model's own context.
+    """
+
+    def __init__(self, precomputed: Sequence[PrecomputedData], Tgpu="Float64", batch: int = 16):
+        self.lib = _lib.load()
+        self.models = list(precomputed)
+        self.mode = _mode_for(Tgpu)
+        if self.mode == KLS_MODE_MIXED:
+            for pc in self.models:
+                pc.ctx.call("kls_prepare_mixed")
+        arr = (C.c_void_p * len(self.models))(*[pc.ctx.h for pc in self.models])
+        h = C.c_void_p()
+        code = self.lib.kls_multi_create(arr, len(self.models), self.mode, int(batch), C.byref(h))
+        if code:
+            raise _lib.KlsError(code, self.lib.kls_multi_last_error(None).decode())
+        self.h = h
+        self.batch = int(batch)
+
+    def _ck(self, code):
+        if code:
+            raise _lib.KlsError(code, self.lib.kls_multi_last_error(self.h).decode())
+
+    def det(self, omegas) -> Tuple[np.ndarray, np.ndarray]:
+        """omegas [n_models, n] complex -> (det [n_models, n], log|det| [n_models, n])."""
+        om = np.ascontiguousarray(np.asarray(omegas, dtype=np.complex128))
+        assert om.ndim == 2 and om.shape[0] == len(self.models)
+        n = om.shape[1]
+        d = np.empty_like(om)
+        la = np.empty(om.shape)
+        self._ck(self.lib.kls_multi_det(self.h, dptr(om.view(np.float64)), n,
+                                        dptr(d.view(np.float64)), dptr(la)))
+        return d, la
+
+    def scan(self, n_Op: int = 41, n_gamma: int = 20, Omega_p_range=(0.2, 0.6),
+             gamma_range=(0.01, 0.2)):
+        """Every model's grid_scan on one grid: (det [n_models, n_gamma, n_Op],
+        log|det| likewise, Omega_p0 [n_models], gamma0 [n_models])."""
+        sc = _lib.kls_scan_cfg(int(n_Op), int(n_gamma), float(Omega_p_range[0]),
+                               float(Omega_p_range[1]), float(gamma_range[0]),
+                               float(gamma_range[1]), self.mode, self.batch)
+        nm, n = len(self.models), n_Op * n_gamma
+        d = np.empty(nm * n, dtype=np.complex128)
+        la = np.empty(nm * n)
+        Op0 = np.empty(nm)
+        g0 = np.empty(nm)
+        self._ck(self.lib.kls_scan_multi(self.h, C.byref(sc), dptr(d.view(np.float64)), dptr(la),
+                                         dptr(Op0), dptr(g0)))
+        # per model a column-major [n_gamma, n_Op] block
+        return (d.reshape(nm, n_Op, n_gamma).transpose(0, 2, 1),
+                la.reshape(nm, n_Op, n_gamma).transpose(0, 2, 1), Op0, g0)
+
+    def info(self) -> dict:
+        i = _lib.kls_multi_info()
+        self._ck(self.lib.kls_multi_get_info(self.h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in i._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.kls_multi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

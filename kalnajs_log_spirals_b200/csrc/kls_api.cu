@@ -10,7 +10,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -630,6 +635,146 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
   res->converged = converged ? 1 : 0;
   res->det_evals = n_mixed + n_fp64;
   if (evals) { evals[0] = n_mixed; evals[1] = n_fp64; }
+  return KLS_OK;
+}
+
+// ---- autotuner ------------------------------------------------------------------
+namespace {
+
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;
+bool g_tune_loaded = false;
+
+std::string tune_key(const kls_ctx* c, int mode, int batch) {
+  cudaDeviceProp p;
+  std::string dev = "gpu";
+  if (cudaGetDeviceProperties(&p, c->device) == cudaSuccess) dev = p.name;
+  for (char& ch : dev)
+    if (ch == ' ') ch = '_';
+  std::ostringstream o;
+  o << dev << "|" << mode << "|" << c->Na_pad << "|" << c->K_pad << "|" << batch;
+  return o.str();
+}
+
+void tune_load_file() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  const char* path = std::getenv("KLS_TUNE_CACHE");
+  if (!path || !*path) return;
+  std::ifstream f(path);
+  std::string key;
+  int s;
+  while (f >> key >> s)
+    if (s > 0) g_tune[key] = s;
+}
+
+void tune_store(const std::string& key, int s) {
+  g_tune[key] = s;
+  const char* path = std::getenv("KLS_TUNE_CACHE");
+  if (!path || !*path) return;
+  std::ofstream f(path, std::ios::app);
+  f << key << " " << s << "\n";
+}
+
+int apply_splits(kls_ctx* c, int mode, int s) {
+  if (mode == KLS_MODE_FP64) {
+    if (c->splits != s) {
+      c->splits = s;
+      c->ws_omega = 0;            // the next batch reallocates the partials
+    }
+    return KLS_OK;
+  }
+  return kls_mixed_set_splits(c, s);
+}
+
+// contraction time per omega (ms) at the context's current split count
+int time_contraction(kls_ctx* c, int mode, int n, double* ms) {
+  int r;
+  if ((r = ensure_ws(c, n))) return r;
+  std::vector<double> om(2 * (size_t)n);
+  for (int z = 0; z < n; ++z) {
+    om[2 * z] = c->cfg.m * (0.3 + 0.3 * z / std::max(1, n));
+    om[2 * z + 1] = 0.02 + 0.2 * z / std::max(1, n);
+  }
+  KLS_CK(c, cudaMemcpyAsync(c->d_omega, om.data(), om.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, c->stream));
+  if ((r = kls_run_weights(c, n))) return r;
+  auto once = [&]() -> int {
+    return mode == KLS_MODE_FP64 ? kls_run_contract_f64(c, n, c->splits)
+                                 : kls_mixed_contract(c, n, 0);
+  };
+  if ((r = once())) return r;               // warm-up (and workspace growth)
+  cudaEvent_t e0, e1;
+  KLS_CK(c, cudaEventCreate(&e0));
+  KLS_CK(c, cudaEventCreate(&e1));
+  const int reps = 3;
+  cudaEventRecord(e0, c->stream);
+  for (int i = 0; i < reps && !r; ++i) r = once();
+  cudaEventRecord(e1, c->stream);
+  cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r) return r;
+  if (e != cudaSuccess) return kls_cuda_fail(c, e, "autotune timing");
+  if (mode == KLS_MODE_MIXED && (r = kls_mixed_check(c))) return r;
+  *ms = t / reps / n;
+  return KLS_OK;
+}
+
+}  // namespace
+
+int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (mode != KLS_MODE_FP64 && mode != KLS_MODE_MIXED)
+    return kls_fail(c, KLS_ERR_CONFIG, "unknown precision mode");
+  if (batch < 1 || batch > WS_CHUNK) return kls_fail(c, KLS_ERR_CONFIG, "bad autotune batch");
+  if (mode == KLS_MODE_MIXED && !c->mixed && (r = kls_mixed_prepare(c))) return r;
+  const int def = mode == KLS_MODE_FP64 ? kls_choose_splits(c) : kls_mixed_default_splits(c);
+  const int max_s = mode == KLS_MODE_FP64 ? (int)std::max<int64_t>(1, c->K_pad / (16 * 8))
+                                          : (int)std::max<int64_t>(1, c->K_pad / 64);
+  kls_tune_result res{};
+  res.mode = mode;
+  res.default_splits = def;
+  const std::string key = tune_key(c, mode, batch);
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    tune_load_file();
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      res.splits = std::min(it->second, max_s);
+      if ((r = apply_splits(c, mode, res.splits))) return r;
+      if (out) *out = res;
+      return KLS_OK;
+    }
+  }
+  std::vector<int> cand = {std::max(1, def / 2), def, 2 * def, 3 * def};
+  for (int& s : cand) s = std::max(1, std::min(s, max_s));
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  double best_ms = INFINITY;
+  int best = def;
+  for (int s : cand) {
+    if ((r = apply_splits(c, mode, s))) return r;
+    double ms = 0.0;
+    if ((r = time_contraction(c, mode, batch, &ms))) return r;
+    if (s == def) res.default_ms_per_omega = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = s;
+    }
+    res.candidates++;
+  }
+  if ((r = apply_splits(c, mode, best))) return r;
+  res.splits = best;
+  res.ms_per_omega = best_ms;
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    tune_store(key, best);
+  }
+  if (out) *out = res;
   return KLS_OK;
 }
 

@@ -57,18 +57,32 @@ __device__ __forceinline__ double2 real_over_complex(double a, double c, double 
   return make_double2(a * p, a * q);
 }
 
-__global__ void weights_kernel(int64_t K_pad, const double* __restrict__ omega,
-                               const double* __restrict__ Gk, const double* __restrict__ Ok,
-                               double2* __restrict__ wt) {
-  const int z = blockIdx.y;
-  const double wr = omega[2 * z], wi = omega[2 * z + 1];
-  double2* out = wt + (size_t)z * K_pad;
+__device__ __forceinline__ void weights_body(int64_t K_pad, double wr, double wi,
+                                             const double* __restrict__ Gk,
+                                             const double* __restrict__ Ok,
+                                             double2* __restrict__ out) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K_pad;
        k += (int64_t)gridDim.x * blockDim.x) {
     double dr = wr - Ok[k], di = wi;
     if (hypot(dr, di) < 1e-12) { dr = 1e-12; di = 1e-12; }
     out[k] = real_over_complex(Gk[k], dr, di);
   }
+}
+
+__global__ void weights_kernel(int64_t K_pad, const double* __restrict__ omega,
+                               const double* __restrict__ Gk, const double* __restrict__ Ok,
+                               double2* __restrict__ wt) {
+  const int z = blockIdx.y;
+  weights_body(K_pad, omega[2 * z], omega[2 * z + 1], Gk, Ok, wt + (size_t)z * K_pad);
+}
+
+// one (model, omega) pair per grid row
+__global__ void multi_weights_kernel(const kls_mdesc* __restrict__ md,
+                                     const int2* __restrict__ pairs) {
+  const int2 pz = pairs[blockIdx.y];
+  const kls_mdesc& d = md[pz.x];
+  const double* om = d.omega + 2 * pz.y;
+  weights_body(d.K_pad, om[0], om[1], d.Gk, d.Ok, d.wt + (size_t)pz.y * d.K_pad);
 }
 
 // ---- contraction -----------------------------------------------------------
@@ -85,11 +99,14 @@ struct ContractParams {
   int64_t K_pad, k_per_split;
 };
 
-__global__ void __launch_bounds__(CT_THREADS, 2)
-contract_kernel(ContractParams P, const double* __restrict__ Wre, const double* __restrict__ Wim,
-                const double2* __restrict__ wt, double2* __restrict__ part) {
-  extern __shared__ __align__(16) double smem[];
-  const int tile = blockIdx.x, split = blockIdx.y, z = blockIdx.z;
+// One 64 x 64 output tile of one K split for one omega: the partial tile goes
+// to part[(z * splits + split)][b][a].
+__device__ __forceinline__ void contract_tile(const ContractParams& P,
+                                              const double* __restrict__ Wre,
+                                              const double* __restrict__ Wim,
+                                              const double2* __restrict__ wt,
+                                              double2* __restrict__ part, double* smem, int tile,
+                                              int split, int z) {
   const int tm = tile / P.tiles_1d, tn = tile % P.tiles_1d;
   const int b0 = tm * KLS_TILE, a0 = tn * KLS_TILE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -160,9 +177,10 @@ contract_kernel(ContractParams P, const double* __restrict__ Wre, const double* 
       for (int j = 0; j < 4; ++j) {
         int off = kr * CT_S + wn * 32 + j * 8 + (lane >> 2);
         double xr = sBr[off], xi = sBi[off];
-        // w * conj(W) = (dr xr + di xi) + i (di xr - dr xi)
-        br[j] = dr * xr + di * xi;
-        bi[j] = di * xr - dr * xi;
+        // w * conj(W) = (dr xr + di xi) + i (di xr - dr xi); roundings
+        // pinned so every kernel that inlines this body gives the same bits
+        br[j] = __fma_rn(dr, xr, __dmul_rn(di, xi));
+        bi[j] = __fma_rn(di, xr, -__dmul_rn(dr, xi));
       }
       // two passes of 32 independent DMMAs: each accumulator's second
       // update issues 32 instructions after its first
@@ -198,15 +216,51 @@ contract_kernel(ContractParams P, const double* __restrict__ Wre, const double* 
   }
 }
 
+__global__ void __launch_bounds__(CT_THREADS, 2)
+contract_kernel(ContractParams P, const double* __restrict__ Wre, const double* __restrict__ Wim,
+                const double2* __restrict__ wt, double2* __restrict__ part) {
+  extern __shared__ __align__(16) double smem[];
+  contract_tile(P, Wre, Wim, wt, part, smem, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Persistent form over an uneven batch: every CTA takes work items
+// (model, omega, tile, split) from an atomic counter until the list is
+// exhausted.  Items are listed longest first, so the tail of the launch is
+// made of the short items of the small models.  Each item computes exactly
+// what contract_kernel computes for the same (tile, split, omega), so a
+// determinant is bitwise the same in either form.
+__global__ void __launch_bounds__(CT_THREADS, 2)
+multi_contract_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict__ items,
+                      int n_items, int* __restrict__ counter) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int i = s_item;
+    if (i >= n_items) break;
+    const kls_item it = items[i];
+    const kls_mdesc& d = md[it.model];
+    ContractParams P;
+    P.Na_pad = d.Na_pad;
+    P.tiles_1d = d.Na_pad / KLS_TILE;
+    P.splits = d.splits;
+    P.K_pad = d.K_pad;
+    P.k_per_split = d.k_per_split;
+    contract_tile(P, d.Wre, d.Wim, d.wt, d.part, smem, it.tile, it.split, it.z);
+    __syncthreads();          // shared stages and s_item are reused by the next item
+  }
+}
+
 // ---- split reduction + epilogue ------------------------------------------------
-__global__ void reduce_kernel(int Na, int Na_pad, int splits, double G,
-                              const double* __restrict__ Nk, const double2* __restrict__ part,
-                              double2* __restrict__ A, double2* __restrict__ Mout) {
-  const int z = blockIdx.y;
+__device__ __forceinline__ void reduce_body(int Na, int Na_pad, int splits, double G,
+                                            const double* __restrict__ Nk,
+                                            const double2* __restrict__ part,
+                                            double2* __restrict__ A, double2* __restrict__ Mout) {
   const size_t plane = (size_t)Na_pad * Na_pad;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
     int b = e / Na, a = e % Na;
-    const double2* src = part + (size_t)z * splits * plane + (size_t)b * Na_pad + a;
+    const double2* src = part + (size_t)b * Na_pad + a;
     double sr = 0.0, si = 0.0;
     for (int s = 0; s < splits; ++s) {
       double2 v = src[(size_t)s * plane];
@@ -214,10 +268,29 @@ __global__ void reduce_kernel(int Na, int Na_pad, int splits, double G,
       si += v.y;
     }
     double n = Nk[a];
-    double mr = (sr * G) * n, mi = (si * G) * n;
-    A[(size_t)z * Na * Na + e] = make_double2((a == b ? 1.0 : 0.0) - mr, -mi);
-    if (Mout && z == 0) Mout[e] = make_double2(mr, mi);
+    // unfused products: 1 - mr must not become an FMA in one kernel only
+    double mr = __dmul_rn(__dmul_rn(sr, G), n), mi = __dmul_rn(__dmul_rn(si, G), n);
+    A[e] = make_double2((a == b ? 1.0 : 0.0) - mr, -mi);
+    if (Mout) Mout[e] = make_double2(mr, mi);
   }
+}
+
+__global__ void reduce_kernel(int Na, int Na_pad, int splits, double G,
+                              const double* __restrict__ Nk, const double2* __restrict__ part,
+                              double2* __restrict__ A, double2* __restrict__ Mout) {
+  const int z = blockIdx.y;
+  const size_t plane = (size_t)Na_pad * Na_pad;
+  reduce_body(Na, Na_pad, splits, G, Nk, part + (size_t)z * splits * plane,
+              A + (size_t)z * Na * Na, z == 0 ? Mout : nullptr);
+}
+
+__global__ void multi_reduce_kernel(const kls_mdesc* __restrict__ md,
+                                    const int2* __restrict__ pairs) {
+  const int2 pz = pairs[blockIdx.y];
+  const kls_mdesc& d = md[pz.x];
+  const size_t plane = (size_t)d.Na_pad * d.Na_pad;
+  reduce_body(d.Na, d.Na_pad, d.splits, d.G, d.Nk, d.part + (size_t)pz.y * d.splits * plane,
+              d.A + (size_t)pz.y * d.Na * d.Na, nullptr);
 }
 
 }  // namespace
@@ -261,8 +334,7 @@ int kls_run_contract_f64(kls_ctx* c, int n, int splits) {
   P.tiles_1d = c->Na_pad / KLS_TILE;
   P.splits = splits;
   P.K_pad = c->K_pad;
-  int64_t slabs = c->K_pad / CT_BK;
-  P.k_per_split = ((slabs + splits - 1) / splits) * CT_BK;
+  P.k_per_split = kls_f64_k_per_split(c->K_pad, splits);
   dim3 grid(P.tiles_1d * P.tiles_1d, splits, n);
   contract_kernel<<<grid, CT_THREADS, CT_SMEM, c->stream>>>(P, c->d_Wre, c->d_Wim, c->d_wt,
                                                             c->d_part);
@@ -277,4 +349,45 @@ int kls_run_reduce(kls_ctx* c, int n, int splits, bool export_M) {
                                                         export_M ? c->d_M : nullptr);
   KLS_LAUNCHED(c);
   return KLS_OK;
+}
+
+// ---- uneven batch over models (kls_multi.cu) ------------------------------------
+int kls_multi_launch_f64(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs, int n_pairs,
+                         const kls_item* d_items, int n_items, int* d_counter, int grid,
+                         int64_t max_K_pad) {
+  int wblocks = (int)std::min<int64_t>((max_K_pad + 255) / 256, 1024);
+  multi_weights_kernel<<<dim3(wblocks, n_pairs), 256, 0, st>>>(d_md, d_pairs);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  if ((e = cudaFuncSetAttribute(multi_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)CT_SMEM)) != cudaSuccess)
+    return (int)e;
+  if ((e = cudaMemsetAsync(d_counter, 0, sizeof(int), st)) != cudaSuccess) return (int)e;
+  multi_contract_kernel<<<grid, CT_THREADS, CT_SMEM, st>>>(d_md, d_items, n_items, d_counter);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  multi_reduce_kernel<<<dim3(256, n_pairs), 256, 0, st>>>(d_md, d_pairs);
+  return (int)cudaGetLastError();
+}
+
+int kls_multi_launch_f64_weights(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs,
+                                 int n_pairs, int64_t max_K_pad) {
+  int wblocks = (int)std::min<int64_t>((max_K_pad + 255) / 256, 1024);
+  multi_weights_kernel<<<dim3(wblocks, n_pairs), 256, 0, st>>>(d_md, d_pairs);
+  return (int)cudaGetLastError();
+}
+
+int kls_multi_contract_slots(int device) {
+  int sms = 148, per_sm = 2;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaFuncSetAttribute(multi_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)CT_SMEM);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_contract_kernel, CT_THREADS,
+                                                    CT_SMEM) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return sms * per_sm;
+}
+
+int64_t kls_f64_k_per_split(int64_t K_pad, int splits) {
+  int64_t slabs = K_pad / CT_BK;
+  return ((slabs + splits - 1) / splits) * CT_BK;
 }

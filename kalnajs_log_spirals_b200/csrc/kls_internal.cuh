@@ -22,6 +22,42 @@ enum OrbitField {
 
 struct kls_mixed;   // split-BF16 tables (kls_mixed.cu)
 
+// One model of an uneven batch (device-resident descriptor, kls_multi.cu).
+// The tables are the model context's own; the per-omega buffers belong to
+// the batch.
+struct kls_mdesc {
+  const double* Wre;          // [K_pad][Na_pad]
+  const double* Wim;
+  const double* Gk;           // [K_pad]
+  const double* Ok;           // [K_pad]
+  const double* Nk;           // [Na]
+  const double* omega;        // [batch][2]
+  double2* wt;                // [batch][K_pad]
+  double2* part;              // FP64 form: [batch][splits][Na_pad][Na_pad]
+  double2* A;                 // [batch][Na][Na]
+  double2* det;               // [batch]
+  double* logabs;             // [batch]
+  double G;
+  int64_t K_pad, k_per_split;
+  int Na, Na_pad, splits, model;
+  // mixed form
+  const void* Xh;             // [2 Na_pad][K_pad] BF16 hi / lo
+  const void* Xl;
+  const void* tmap_h;         // device copies of the TMA descriptors (64-byte aligned)
+  const void* tmap_l;
+  void* wt32;                 // [batch][K_pad] float2, permuted per 64-block
+  double* mpart;              // [batch][msplits][2 Na_pad][2 Na_pad] column-major planes
+  int msplits, kb_per_split, nkb_total, om_per_item;
+};
+
+// One work item of the persistent contraction: FP64 form (model, omega z,
+// 64 x 64 tile, K split); mixed form (model, first omega z, 128-row x
+// 64-alpha tile, K split, n_om omegas from z, k-blocks [kb0, kb0 + nkb)).
+struct kls_item {
+  int model, z, tile, split;
+  int n_om, kb0, nkb, pad;
+};
+
 struct kls_ctx {
   kls_config cfg{};
   int device = 0;
@@ -114,3 +150,22 @@ int kls_mixed_contract(kls_ctx* c, int n, int splits);
 int kls_mixed_reduce(kls_ctx* c, int n, bool export_M);
 int kls_mixed_check(kls_ctx* c);     // pipeline timeout flag of the last launches
 void kls_mixed_free(kls_ctx* c);
+// uneven batch over models (kls_multi.cu drives these)
+int kls_multi_launch_f64(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs, int n_pairs,
+                         const kls_item* d_items, int n_items, int* d_counter, int grid,
+                         int64_t max_K_pad);
+int kls_multi_launch_lu(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs, int n_pairs,
+                        int max_Na);
+int kls_multi_launch_f64_weights(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs,
+                                 int n_pairs, int64_t max_K_pad);
+int kls_multi_contract_slots(int device);
+int64_t kls_f64_k_per_split(int64_t K_pad, int splits);
+int kls_multi_launch_mixed(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs,
+                           int n_pairs, const kls_item* d_items, const int* d_starts, int grid,
+                           int64_t max_K_pad, int* d_err);
+int kls_mixed_slots(int device);
+int kls_mixed_splits_of(const kls_ctx* c);
+int kls_mixed_default_splits(const kls_ctx* c);
+int kls_mixed_set_splits(kls_ctx* c, int splits);
+const void* kls_mixed_tables(const kls_ctx* c, const void** Xl, const void** tmap_h,
+                             const void** tmap_l);

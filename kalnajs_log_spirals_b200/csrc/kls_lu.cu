@@ -24,21 +24,24 @@ __device__ __forceinline__ double2 cinv(double c, double d) {
   return make_double2(r * t, -t);
 }
 
+// roundings pinned (no compiler choice of which product joins an FMA), so
+// every kernel that inlines the LU body gives the same bits
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return make_double2(__fma_rn(a.x, b.x, -__dmul_rn(a.y, b.y)),
+                      __fma_rn(a.x, b.y, __dmul_rn(a.y, b.x)));
 }
 
-__global__ void __launch_bounds__(LU_THREADS)
-lu_det_kernel(int n, double2* __restrict__ Aall, double2* __restrict__ det_out,
-              double* __restrict__ logabs_out) {
-  extern __shared__ double2 sh[];        // prow[n], lcol[n]
+// LU of one n x n row-major matrix A by the whole CTA; writes *det_out and,
+// if given, *logabs_out.  sh holds 2 n complex values.
+__device__ __forceinline__ void lu_det_body(int n, double2* __restrict__ A, double2* sh,
+                                            double2* __restrict__ det_out,
+                                            double* __restrict__ logabs_out) {
   double2* prow = sh;
   double2* lcol = sh + n;
   __shared__ double red_v[32];
   __shared__ int red_i[32];
   __shared__ int s_piv;
   __shared__ double2 s_u;
-  double2* A = Aall + (size_t)blockIdx.x * n * n;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
 
@@ -98,8 +101,8 @@ lu_det_kernel(int n, double2* __restrict__ Aall, double2* __restrict__ det_out,
       for (int c = j + 1 + lane; c < n; c += 32) {
         double2 p = prow[c];
         double2 a = row[c];
-        a.x -= l.x * p.x - l.y * p.y;
-        a.y -= l.x * p.y + l.y * p.x;
+        a.x = __dsub_rn(a.x, __fma_rn(l.x, p.x, -__dmul_rn(l.y, p.y)));
+        a.y = __dsub_rn(a.y, __fma_rn(l.x, p.y, __dmul_rn(l.y, p.x)));
         row[c] = a;
       }
     }
@@ -132,9 +135,26 @@ lu_det_kernel(int n, double2* __restrict__ Aall, double2* __restrict__ det_out,
       d = make_double2(scalbn(mant.x, (int)e), scalbn(mant.y, (int)e));
       la = log(hypot(mant.x, mant.y)) + (double)expo * 0.69314718055994530942;
     }
-    det_out[blockIdx.x] = d;
-    if (logabs_out) logabs_out[blockIdx.x] = la;
+    *det_out = d;
+    if (logabs_out) *logabs_out = la;
   }
+}
+
+__global__ void __launch_bounds__(LU_THREADS)
+lu_det_kernel(int n, double2* __restrict__ Aall, double2* __restrict__ det_out,
+              double* __restrict__ logabs_out) {
+  extern __shared__ double2 sh[];        // prow[n], lcol[n]
+  lu_det_body(n, Aall + (size_t)blockIdx.x * n * n, sh, det_out + blockIdx.x,
+              logabs_out ? logabs_out + blockIdx.x : nullptr);
+}
+
+// one (model, omega) pair per CTA, matrices of different sizes
+__global__ void __launch_bounds__(LU_THREADS)
+multi_lu_kernel(const kls_mdesc* __restrict__ md, const int2* __restrict__ pairs) {
+  extern __shared__ double2 sh[];
+  const int2 pz = pairs[blockIdx.x];
+  const kls_mdesc& d = md[pz.x];
+  lu_det_body(d.Na, d.A + (size_t)pz.y * d.Na * d.Na, sh, d.det + pz.y, d.logabs + pz.y);
 }
 
 }  // namespace
@@ -147,4 +167,16 @@ int kls_run_lu(kls_ctx* c, int n) {
   lu_det_kernel<<<n, LU_THREADS, sm, c->stream>>>(c->Na, c->d_A, c->d_det, c->d_logabs);
   KLS_LAUNCHED(c);
   return KLS_OK;
+}
+
+int kls_multi_launch_lu(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs, int n_pairs,
+                        int max_Na) {
+  size_t sm = 2 * (size_t)max_Na * sizeof(double2);
+  cudaError_t e;
+  if (sm > 48 * 1024 &&
+      (e = cudaFuncSetAttribute(multi_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm)) != cudaSuccess)
+    return (int)e;
+  multi_lu_kernel<<<n_pairs, LU_THREADS, sm, st>>>(d_md, d_pairs);
+  return (int)cudaGetLastError();
 }

@@ -452,11 +452,14 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
           uint32_t rh[4], rl[4], ih[4], il[4];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            // w conj(W) = (dr Wr + di Wi) + i (di Wr - dr Wi)
-            const float ur0 = w[q].x * wr[u][2 * q] + w[q].y * wi[u][2 * q];
-            const float ui0 = w[q].y * wr[u][2 * q] - w[q].x * wi[u][2 * q];
-            const float ur1 = w[q].z * wr[u][2 * q + 1] + w[q].w * wi[u][2 * q + 1];
-            const float ui1 = w[q].w * wr[u][2 * q + 1] - w[q].z * wi[u][2 * q + 1];
+            // w conj(W) = (dr Wr + di Wi) + i (di Wr - dr Wi), roundings pinned
+            // so both contraction kernels give the same bits
+            const float ur0 = __fmaf_rn(w[q].x, wr[u][2 * q], __fmul_rn(w[q].y, wi[u][2 * q]));
+            const float ui0 = __fmaf_rn(w[q].y, wr[u][2 * q], -__fmul_rn(w[q].x, wi[u][2 * q]));
+            const float ur1 =
+                __fmaf_rn(w[q].z, wr[u][2 * q + 1], __fmul_rn(w[q].w, wi[u][2 * q + 1]));
+            const float ui1 =
+                __fmaf_rn(w[q].w, wr[u][2 * q + 1], -__fmul_rn(w[q].z, wi[u][2 * q + 1]));
             rh[q] = pack_split(ur0, ur1, rl[q]);
             ih[q] = pack_split(ui0, ui1, il[q]);
           }
@@ -534,17 +537,18 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
 }
 
 // ---- reduction of the FP64 partial tiles -----------------------------------------
-__global__ void mixed_reduce_kernel(int Na, int Npad, int splits, double G,
-                                    const double* __restrict__ Nk, const double* __restrict__ part,
-                                    double2* __restrict__ A, double2* __restrict__ Mout) {
-  const int z = blockIdx.y;
+__device__ __forceinline__ void mixed_reduce_body(int Na, int Npad, int splits, double G,
+                                                  const double* __restrict__ Nk,
+                                                  const double* __restrict__ part,
+                                                  double2* __restrict__ A,
+                                                  double2* __restrict__ Mout) {
   const size_t R = 2 * (size_t)Npad;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
     const int b = e % Na, a = e / Na;          // consecutive threads: consecutive rows b
     double mr = 0.0, mi = 0.0;
     for (int s = 0; s < splits; ++s) {
       // plane of (omega, split), element (row c, column n) at n * R + c
-      const double* P = part + ((size_t)z * splits + s) * R * R;
+      const double* P = part + (size_t)s * R * R;
       const double pr_r = P[(size_t)(2 * a) * R + b], pr_i = P[(size_t)(2 * a + 1) * R + b];
       const double pi_r = P[(size_t)(2 * a) * R + Npad + b];
       const double pi_i = P[(size_t)(2 * a + 1) * R + Npad + b];
@@ -552,9 +556,378 @@ __global__ void mixed_reduce_kernel(int Na, int Npad, int splits, double G,
       mi += pr_i + pi_r;
     }
     const double n = Nk[a];
-    const double Mr = (mr * G) * n, Mi = (mi * G) * n;
-    A[(size_t)z * Na * Na + (size_t)b * Na + a] = make_double2((a == b ? 1.0 : 0.0) - Mr, -Mi);
-    if (Mout && z == 0) Mout[(size_t)b * Na + a] = make_double2(Mr, Mi);
+    // unfused products: 1 - Mr must not become an FMA in one kernel only
+    const double Mr = __dmul_rn(__dmul_rn(mr, G), n), Mi = __dmul_rn(__dmul_rn(mi, G), n);
+    A[(size_t)b * Na + a] = make_double2((a == b ? 1.0 : 0.0) - Mr, -Mi);
+    if (Mout) Mout[(size_t)b * Na + a] = make_double2(Mr, Mi);
+  }
+}
+
+__global__ void mixed_reduce_kernel(int Na, int Npad, int splits, double G,
+                                    const double* __restrict__ Nk, const double* __restrict__ part,
+                                    double2* __restrict__ A, double2* __restrict__ Mout) {
+  const int z = blockIdx.y;
+  const size_t R = 2 * (size_t)Npad;
+  mixed_reduce_body(Na, Npad, splits, G, Nk, part + (size_t)z * splits * R * R,
+                    A + (size_t)z * Na * Na, z == 0 ? Mout : nullptr);
+}
+
+// ---- uneven batch over models -------------------------------------------------
+__global__ void multi_weights32_kernel(const kls_mdesc* __restrict__ md,
+                                       const int2* __restrict__ pairs) {
+  const int2 pz = pairs[blockIdx.y];
+  const kls_mdesc& d = md[pz.x];
+  const double2* wt = d.wt + (size_t)pz.y * d.K_pad;
+  float2* w32 = reinterpret_cast<float2*>(d.wt32) + (size_t)pz.y * d.K_pad;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.K_pad;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = wt[i];
+    const int k = (int)(i & (MX_BK - 1));
+    const int c = k >> 3, q = (k >> 1) & 3, h = k & 1;
+    w32[(i & ~(int64_t)(MX_BK - 1)) + 2 * (8 * q + c) + h] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+__global__ void multi_mixed_reduce_kernel(const kls_mdesc* __restrict__ md,
+                                          const int2* __restrict__ pairs) {
+  const int2 pz = pairs[blockIdx.y];
+  const kls_mdesc& d = md[pz.x];
+  const size_t R = 2 * (size_t)d.Na_pad;
+  mixed_reduce_body(d.Na, d.Na_pad, d.msplits, d.G, d.Nk,
+                    d.mpart + (size_t)pz.y * d.msplits * R * R, d.A + (size_t)pz.y * d.Na * d.Na,
+                    nullptr);
+}
+
+__device__ __forceinline__ void tensormap_acquire(const void* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((uint64_t)map)
+               : "memory");
+}
+
+// Persistent form of mixed_contract_kernel over an uneven batch of models.
+// CTA b takes items [starts[b], starts[b+1]) of a list the host balanced
+// across CTAs (longest item first onto the least-loaded CTA); every role
+// walks the same items, and the stage, weights-slot and
+// accumulator phases run on counters that continue across items, so the
+// pipeline never drains between items.  An item computes exactly what the
+// one-model kernel computes for the same (tile, split, omegas): the same
+// k-blocks, chunks and FP64 flush order, hence the same bits.
+__global__ void __launch_bounds__(MX_THREADS, 1)
+mixed_multi_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict__ items,
+                   const int* __restrict__ starts, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_full_x[MX_STAGES], bar_full_y[MX_STAGES],
+      bar_empty[MX_STAGES], bar_w_full[MX_WSTAGES], bar_w_empty[MX_WSTAGES], bar_acc_full[2],
+      bar_acc_empty[2], bar_done;
+  __shared__ uint32_t s_tmem;
+  __shared__ volatile int s_abort;
+
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int t_beg = starts[blockIdx.x], t_end = starts[blockIdx.x + 1];
+  const bool any = t_end > t_beg;
+
+  auto xh_s = [&](int s) { return smem + (size_t)s * MX_STAGE_BYTES; };
+  auto xl_s = [&](int s) { return smem + (size_t)s * MX_STAGE_BYTES + MX_TILE_X; };
+  auto yh_s = [&](int s, int j) {
+    return smem + (size_t)s * MX_STAGE_BYTES + 2 * MX_TILE_X + (size_t)j * MX_TILE_Y;
+  };
+  auto yl_s = [&](int s, int j) {
+    return smem + (size_t)s * MX_STAGE_BYTES + 2 * MX_TILE_X + (size_t)(MX_OMEGA + j) * MX_TILE_Y;
+  };
+  auto w_s = [&](int ws, int j) {
+    return reinterpret_cast<float2*>(smem + (size_t)MX_STAGES * MX_STAGE_BYTES +
+                                     (size_t)ws * MX_OMEGA * MX_W_BYTES) + j * MX_BK;
+  };
+
+  if (tid == 0) {
+    s_abort = 0;
+    for (int s = 0; s < MX_STAGES; ++s) {
+      mbar_init(smem_u32(&bar_full_x[s]), 1);
+      mbar_init(smem_u32(&bar_full_y[s]), MX_PRODUCERS);
+      mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    for (int s = 0; s < MX_WSTAGES; ++s) {
+      mbar_init(smem_u32(&bar_w_full[s]), 1);
+      mbar_init(smem_u32(&bar_w_empty[s]), MX_PRODUCERS);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&bar_acc_full[b]), 1);
+      mbar_init(smem_u32(&bar_acc_empty[b]), 128);
+    }
+    mbar_init(smem_u32(&bar_done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2 && any) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(MX_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  if (warp == 0) {
+    // ---------------- TMA: X tiles
+    if (lane == 0 && any) {
+      uint32_t g = 0;
+      bool ok = true;
+      for (int t = t_beg; t < t_end && ok; ++t) {
+        const kls_item it = items[t];
+        const kls_mdesc& d = md[it.model];
+        const CUtensorMap* mh = reinterpret_cast<const CUtensorMap*>(d.tmap_h);
+        const CUtensorMap* ml = reinterpret_cast<const CUtensorMap*>(d.tmap_l);
+        tensormap_acquire(mh);
+        tensormap_acquire(ml);
+        const int m0 = (it.tile / (d.Na_pad / MX_AB)) * MX_BM;
+        for (int i = 0; i < it.nkb; ++i) {
+          const int s = g % MX_STAGES, r = g / MX_STAGES;
+          if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 1)) {
+            ok = false;
+            break;
+          }
+          const int64_t kx = (int64_t)(it.kb0 + i) * MX_BK;
+          const uint32_t fb = smem_u32(&bar_full_x[s]);
+          mbar_arrive_tx(fb, 2 * MX_TILE_X);
+          tma_load_2d(smem_u32(xh_s(s)), mh, (int)kx, m0, fb);
+          tma_load_2d(smem_u32(xl_s(s)), ml, (int)kx, m0, fb);
+          ++g;
+        }
+      }
+      for (uint32_t i = g > MX_STAGES ? g - MX_STAGES : 0; i < g; ++i)
+        mbar_wait(smem_u32(&bar_full_x[i % MX_STAGES]), (i / MX_STAGES) & 1, nullptr, err, 6);
+    }
+  } else if (warp == 3) {
+    // ---------------- weights ring
+    if (lane == 0 && any) {
+      uint32_t g = 0;
+      bool ok = true;
+      for (int t = t_beg; t < t_end && ok; ++t) {
+        const kls_item it = items[t];
+        const kls_mdesc& d = md[it.model];
+        const float2* wt32 = reinterpret_cast<const float2*>(d.wt32);
+        for (int i = 0; i < it.nkb; ++i) {
+          const int ws = g % MX_WSTAGES, r = g / MX_WSTAGES;
+          if (!mbar_wait(smem_u32(&bar_w_empty[ws]), (r & 1) ^ 1, &s_abort, err, 10)) {
+            ok = false;
+            break;
+          }
+          const int64_t kx = (int64_t)(it.kb0 + i) * MX_BK;
+          const uint32_t wb = smem_u32(&bar_w_full[ws]);
+          mbar_arrive_tx(wb, it.n_om * MX_W_BYTES);
+          for (int j = 0; j < it.n_om; ++j)
+            bulk_load(smem_u32(w_s(ws, j)), wt32 + (size_t)(it.z + j) * d.K_pad + kx, MX_W_BYTES,
+                      wb);
+          ++g;
+        }
+      }
+      for (uint32_t i = g > MX_WSTAGES ? g - MX_WSTAGES : 0; i < g; ++i)
+        mbar_wait(smem_u32(&bar_w_full[i % MX_WSTAGES]), (i / MX_WSTAGES) & 1, nullptr, err, 6);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0 && any) {
+      uint32_t g = 0, gch = 0;
+      bool ok = true;
+      for (int t = t_beg; t < t_end && ok; ++t) {
+        const kls_item it = items[t];
+        const uint32_t idesc = idesc_bf16(MX_BM, MX_BN * it.n_om);
+        for (int i = 0; i < it.nkb; ++i) {
+          const int s = g % MX_STAGES, r = g / MX_STAGES;
+          const uint32_t ch = gch + (uint32_t)(i / MX_CHUNK_KB), b = ch & 1;
+          const bool first = (i % MX_CHUNK_KB) == 0;
+          const bool last = (i % MX_CHUNK_KB) == MX_CHUNK_KB - 1 || i == it.nkb - 1;
+          if (first &&
+              !mbar_wait(smem_u32(&bar_acc_empty[b]), ((ch >> 1) & 1) ^ 1, &s_abort, err, 7)) {
+            ok = false;
+            break;
+          }
+          if (!mbar_wait(smem_u32(&bar_full_x[s]), r & 1, &s_abort, err, 2) ||
+              !mbar_wait(smem_u32(&bar_full_y[s]), r & 1, &s_abort, err, 3)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint64_t dxh = sw128_desc(smem_u32(xh_s(s)));
+          const uint64_t dxl = sw128_desc(smem_u32(xl_s(s)));
+          const uint32_t d = tmem + (uint32_t)(b * MX_ACC_COLS);
+          const uint64_t dyh0 = sw128_desc(smem_u32(yh_s(s, 0)));
+          const uint64_t dyl0 = sw128_desc(smem_u32(yl_s(s, 0)));
+#pragma unroll
+          for (int kk = 0; kk < MX_BK / 16; ++kk) {
+            const uint64_t koff = (uint64_t)(kk * 32) >> 4;
+            umma(d, dxh + koff, dyh0 + koff, idesc, (first && kk == 0) ? 0u : 1u);
+            umma(d, dxh + koff, dyl0 + koff, idesc, 1u);
+            umma(d, dxl + koff, dyh0 + koff, idesc, 1u);
+          }
+          umma_commit(smem_u32(&bar_empty[s]));
+          if (last) umma_commit(smem_u32(&bar_acc_full[b]));
+          ++g;
+        }
+        gch += (uint32_t)((it.nkb + MX_CHUNK_KB - 1) / MX_CHUNK_KB);
+      }
+      umma_commit(smem_u32(&bar_done));
+    }
+  } else if (warp >= 4 && warp < MX_DRAIN0) {
+    // ---------------- producers
+    const int pt = tid - 128;
+    const int c = pt & 7;
+    uint32_t g = 0;
+    bool ok = true;
+    for (int t = t_beg; t < t_end && ok; ++t) {
+      const kls_item it = items[t];
+      const kls_mdesc& d = md[it.model];
+      const __nv_bfloat16* Xh = reinterpret_cast<const __nv_bfloat16*>(d.Xh);
+      const __nv_bfloat16* Xl = reinterpret_cast<const __nv_bfloat16*>(d.Xl);
+      const int a0 = (it.tile % (d.Na_pad / MX_AB)) * MX_AB;
+      const int n_om = it.n_om;
+      int al_u[2];
+      const __nv_bfloat16* rows_u[2][4];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        al_u[u] = (pt >> 3) + 32 * u;
+        const size_t a = (size_t)(a0 + al_u[u]);
+        rows_u[u][0] = Xh + a * d.K_pad;
+        rows_u[u][1] = Xl + a * d.K_pad;
+        rows_u[u][2] = Xh + (d.Na_pad + a) * d.K_pad;
+        rows_u[u][3] = Xl + (d.Na_pad + a) * d.K_pad;
+      }
+      uint4 pre[2][4];
+      auto prefetch = [&](int i) {
+        const int64_t kb = (int64_t)(it.kb0 + i) * MX_BK;
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            pre[u][q] = __ldg(reinterpret_cast<const uint4*>(rows_u[u][q] + kb + c * 8));
+      };
+      prefetch(0);
+      for (int i = 0; i < it.nkb; ++i) {
+        const int s = g % MX_STAGES, r = g / MX_STAGES;
+        if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)) {
+          ok = false;
+          break;
+        }
+        const int ws = g % MX_WSTAGES;
+        if (!mbar_wait(smem_u32(&bar_w_full[ws]), (g / MX_WSTAGES) & 1, &s_abort, err, 8)) {
+          ok = false;
+          break;
+        }
+        float wr[2][8], wi[2][8];
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t ah = (&pre[u][0].x)[q], al = (&pre[u][1].x)[q];
+            const uint32_t bh = (&pre[u][2].x)[q], bl = (&pre[u][3].x)[q];
+            wr[u][2 * q] = bf_lo(ah) + bf_lo(al);
+            wr[u][2 * q + 1] = bf_hi(ah) + bf_hi(al);
+            wi[u][2 * q] = bf_lo(bh) + bf_lo(bl);
+            wi[u][2 * q + 1] = bf_hi(bh) + bf_hi(bl);
+          }
+        float4 wq[MX_OMEGA][4];
+#pragma unroll
+        for (int j = 0; j < MX_OMEGA; ++j) {
+          const float4* wz = reinterpret_cast<const float4*>(w_s(ws, j)) + c;
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            wq[j][q] = j < n_om ? wz[8 * q] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int j = 0; j < MX_OMEGA; ++j) {
+          if (j >= n_om) break;
+          const float4* w = wq[j];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int a_l = al_u[u];
+            uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const float ur0 = __fmaf_rn(w[q].x, wr[u][2 * q], __fmul_rn(w[q].y, wi[u][2 * q]));
+              const float ui0 = __fmaf_rn(w[q].y, wr[u][2 * q], -__fmul_rn(w[q].x, wi[u][2 * q]));
+              const float ur1 =
+                  __fmaf_rn(w[q].z, wr[u][2 * q + 1], __fmul_rn(w[q].w, wi[u][2 * q + 1]));
+              const float ui1 =
+                  __fmaf_rn(w[q].w, wr[u][2 * q + 1], -__fmul_rn(w[q].z, wi[u][2 * q + 1]));
+              rh[q] = pack_split(ur0, ur1, rl[q]);
+              ih[q] = pack_split(ui0, ui1, il[q]);
+            }
+            const uint32_t offr = sw128_off(2 * a_l, c), offi = sw128_off(2 * a_l + 1, c);
+            *reinterpret_cast<uint4*>(yh_s(s, j) + offr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+            *reinterpret_cast<uint4*>(yl_s(s, j) + offr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+            *reinterpret_cast<uint4*>(yh_s(s, j) + offi) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+            *reinterpret_cast<uint4*>(yl_s(s, j) + offi) = make_uint4(il[0], il[1], il[2], il[3]);
+          }
+        }
+        mbar_arrive(smem_u32(&bar_w_empty[ws]));
+        fence_proxy_async();
+        mbar_arrive(smem_u32(&bar_full_y[s]));
+        ++g;
+        if (i + 1 < it.nkb) prefetch(i + 1);
+      }
+    }
+  } else if (warp >= MX_DRAIN0) {
+    // ---------------- drain
+    const int q = warp & 3;
+    uint32_t gch = 0;
+    bool ok = true;
+    for (int t = t_beg; t < t_end && ok; ++t) {
+      const kls_item it = items[t];
+      const kls_mdesc& d = md[it.model];
+      const size_t R = 2 * (size_t)d.Na_pad;
+      const int tiles_a = d.Na_pad / MX_AB;
+      const int row = (it.tile / tiles_a) * MX_BM + q * 32 + lane;
+      const int a0 = (it.tile % tiles_a) * MX_AB;
+      const int nch = (it.nkb + MX_CHUNK_KB - 1) / MX_CHUNK_KB;
+      for (int ch = 0; ch < nch; ++ch) {
+        const uint32_t G = gch + (uint32_t)ch, b = G & 1;
+        bool w = mbar_wait(smem_u32(&bar_acc_full[b]), (G >> 1) & 1, &s_abort, err, 9);
+        w = __all_sync(0xffffffffu, w);
+        if (!w) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        for (int j = 0; j < it.n_om; ++j) {
+          double* out = d.mpart + ((size_t)(it.z + j) * d.msplits + it.split) * R * R + row;
+          for (int cc = 0; cc < MX_BN / 32; ++cc) {
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) +
+                                   (uint32_t)(b * MX_ACC_COLS + j * MX_BN + cc * 32);
+            TMEM_LD32(taddr, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            double* o = out + (size_t)(2 * a0 + cc * 32) * R;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              double old[16];
+              if (ch > 0) {
+#pragma unroll
+                for (int t2 = 0; t2 < 16; ++t2) old[t2] = o[(size_t)(16 * h + t2) * R];
+              } else {
+#pragma unroll
+                for (int t2 = 0; t2 < 16; ++t2) old[t2] = 0.0;
+              }
+#pragma unroll
+              for (int t2 = 0; t2 < 16; ++t2)
+                o[(size_t)(16 * h + t2) * R] = old[t2] + (double)__uint_as_float(v[16 * h + t2]);
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(smem_u32(&bar_acc_empty[b]));
+      }
+      gch += (uint32_t)nch;
+    }
+  }
+  __syncwarp();
+  if (warp == 2 && any) mbar_wait(smem_u32(&bar_done), 0, nullptr, err, 5);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 2 && any) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(MX_TMEM_COLS));
   }
 }
 
@@ -704,4 +1077,52 @@ void kls_mixed_free(kls_ctx* c) {
   cudaFree(c->mixed->err);
   delete c->mixed;
   c->mixed = nullptr;
+}
+
+// ---- uneven batch hooks (kls_multi.cu) ----------------------------------------
+int kls_multi_launch_mixed(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs,
+                           int n_pairs, const kls_item* d_items, const int* d_starts, int grid,
+                           int64_t max_K_pad, int* d_err) {
+  cudaError_t e;
+  int wblocks = (int)std::min<int64_t>((max_K_pad + 255) / 256, 1024);
+  multi_weights32_kernel<<<dim3(wblocks, n_pairs), 256, 0, st>>>(d_md, d_pairs);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  if ((e = cudaFuncSetAttribute(mixed_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)MX_SMEM)) != cudaSuccess)
+    return (int)e;
+  mixed_multi_kernel<<<grid, MX_THREADS, MX_SMEM, st>>>(d_md, d_items, d_starts, d_err);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  multi_mixed_reduce_kernel<<<dim3(256, n_pairs), 256, 0, st>>>(d_md, d_pairs);
+  return (int)cudaGetLastError();
+}
+
+int kls_mixed_slots(int device) {
+  int sms = 148, per_sm = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaFuncSetAttribute(mixed_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)MX_SMEM);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_multi_kernel, MX_THREADS,
+                                                    MX_SMEM) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return sms * per_sm;
+}
+
+int kls_mixed_splits_of(const kls_ctx* c) { return c->mixed ? c->mixed->splits : 0; }
+
+int kls_mixed_default_splits(const kls_ctx* c) { return mixed_splits(c); }
+
+int kls_mixed_set_splits(kls_ctx* c, int splits) {
+  if (!c->mixed) return KLS_ERR_STATE;
+  const int nkb = (int)(c->K_pad / MX_BK);
+  c->mixed->splits = std::max(1, std::min(splits, nkb));
+  return KLS_OK;
+}
+
+const void* kls_mixed_tables(const kls_ctx* c, const void** Xl, const void** tmap_h,
+                             const void** tmap_l) {
+  if (!c->mixed) return nullptr;
+  *Xl = c->mixed->Xl;
+  *tmap_h = &c->mixed->tm_h;
+  *tmap_l = &c->mixed->tm_l;
+  return c->mixed->Xh;
 }

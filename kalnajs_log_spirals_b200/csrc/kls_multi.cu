@@ -1,0 +1,486 @@
+// Uneven batch: det(I - M(omega)) for many disk models of different sizes in
+// shared launches (no reference counterpart as one launch: the reference runs
+// grid_scan once per model, and its multi-GPU scan, GridScan.jl:125-197,
+// splits one model's omega columns over devices).
+//
+// Every model keeps its own context (tables on the device); a kls_multi adds
+// per-omega buffers for a fixed batch of omegas per model and device-resident
+// descriptors (kls_mdesc), and lists the contraction's work items over all
+// models.  One batch is
+//
+//   H2D omegas -> weights (all models) -> persistent contraction (all models)
+//   -> split reduction (all models) -> LU (all models) -> D2H dets
+//
+// captured once into a CUDA graph and replayed for every chunk of omegas.
+// The FP64 contraction takes items from an atomic counter, longest first; the
+// mixed one gets per-CTA item ranges balanced on the host (longest item onto
+// the least-loaded CTA).  Each model's K split count is its context's own
+// (kls_autotune chooses it), so a determinant from the batch is bitwise the
+// one kls_det_batch returns for the same context.
+#include "kls_internal.cuh"
+#include <cuda.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <numeric>
+#include <queue>
+#include <vector>
+
+struct kls_multi {
+  int device = 0, mode = 0, batch = 0, n_models = 0;
+  std::vector<kls_ctx*> ctx;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  std::vector<kls_mdesc> md;
+  std::vector<kls_item> items;
+  std::vector<int> starts;          // mixed: per-CTA item ranges
+  std::vector<int2> pairs;          // (model, omega) pairs
+  int grid = 0, max_Na = 0;
+  int64_t max_K_pad = 0;
+
+  kls_mdesc* d_md = nullptr;
+  kls_item* d_items = nullptr;
+  int* d_starts = nullptr;
+  int2* d_pairs = nullptr;
+  int* d_counter = nullptr;
+  int* d_err = nullptr;
+  uint8_t* d_tmaps = nullptr;       // 2 CUtensorMap per model
+  double* d_omega = nullptr;        // [n_models][batch][2]
+  double2* d_det = nullptr;         // [n_models][batch]
+  double* d_logabs = nullptr;
+  std::vector<void*> bufs;          // per-model buffers to free
+
+  double* h_omega = nullptr;        // pinned [n_models][batch][2]
+  double* h_det = nullptr;          // pinned [n_models][batch][2]
+  double* h_logabs = nullptr;       // pinned [n_models][batch]
+  int* h_err = nullptr;             // pinned
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int64_t replays = 0;
+  float last_ms = 0.f;
+};
+
+namespace {
+
+thread_local std::string g_multi_create_err;
+
+int mfail(kls_multi* m, int code, const std::string& msg) {
+  if (m) m->err = msg;
+  else g_multi_create_err = msg;
+  return code;
+}
+int mcuda(kls_multi* m, cudaError_t e, const char* what) {
+  return mfail(m, e == cudaErrorMemoryAllocation ? KLS_ERR_OOM : KLS_ERR_CUDA,
+               std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define KM_CK(m, call)                                          \
+  do {                                                          \
+    cudaError_t e_ = (call);                                    \
+    if (e_ != cudaSuccess) return mcuda((m), e_, #call);        \
+  } while (0)
+
+template <typename T>
+int malloc_buf(kls_multi* m, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return mcuda(m, e, "cudaMalloc (uneven batch buffers)");
+  }
+  m->bufs.push_back(*p);
+  return KLS_OK;
+}
+
+// mixed items: effective K splits so that every split owns >= 1 k-block
+constexpr int MIX_BK = 64, MIX_BM = 128, MIX_AB = 64;
+
+int build_items(kls_multi* m) {
+  m->items.clear();
+  m->pairs.clear();
+  for (int i = 0; i < m->n_models; ++i)
+    for (int z = 0; z < m->batch; ++z) m->pairs.push_back(make_int2(i, z));
+  if (m->mode == KLS_MODE_FP64) {
+    for (int i = 0; i < m->n_models; ++i) {
+      const kls_mdesc& d = m->md[i];
+      const int tiles = (d.Na_pad / KLS_TILE) * (d.Na_pad / KLS_TILE);
+      for (int z = 0; z < m->batch; ++z)
+        for (int t = 0; t < tiles; ++t)
+          for (int s = 0; s < d.splits; ++s) {
+            int64_t kb = (int64_t)s * d.k_per_split;
+            int64_t ke = std::min(d.K_pad, kb + d.k_per_split);
+            m->items.push_back(kls_item{i, z, t, s, 1, 0, (int)std::max<int64_t>(0, ke - kb), 0});
+          }
+    }
+    // longest first; ties keep (model, omega, tile, split) order
+    std::stable_sort(m->items.begin(), m->items.end(),
+                     [](const kls_item& a, const kls_item& b) { return a.nkb > b.nkb; });
+    m->grid = std::max(1, std::min((int)m->items.size(), kls_multi_contract_slots(m->device)));
+    return KLS_OK;
+  }
+  std::vector<int64_t> cost;
+  for (int i = 0; i < m->n_models; ++i) {
+    const kls_mdesc& d = m->md[i];
+    const int tiles = (2 * d.Na_pad / MIX_BM) * (d.Na_pad / MIX_AB);
+    for (int z = 0; z < m->batch; z += d.om_per_item) {
+      const int n_om = std::min(d.om_per_item, m->batch - z);
+      for (int t = 0; t < tiles; ++t)
+        for (int s = 0; s < d.msplits; ++s) {
+          const int kb0 = s * d.kb_per_split;
+          const int nkb = std::min(d.nkb_total, kb0 + d.kb_per_split) - kb0;
+          if (nkb <= 0) continue;
+          m->items.push_back(kls_item{i, z, t, s, n_om, kb0, nkb, 0});
+        }
+    }
+  }
+  const int n = (int)m->items.size();
+  const int grid = std::max(1, std::min(n, kls_mixed_slots(m->device)));
+  // greedy LPT: cost ~ k-blocks x (X tile + n_om Y tiles)
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  auto c_of = [&](int k) { return (int64_t)m->items[k].nkb * (2 + m->items[k].n_om); };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return c_of(a) > c_of(b); });
+  typedef std::pair<int64_t, int> Load;
+  std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+  for (int b = 0; b < grid; ++b) heap.push(Load(0, b));
+  std::vector<std::vector<int>> per(grid);
+  for (int k : order) {
+    Load l = heap.top();
+    heap.pop();
+    per[l.second].push_back(k);
+    heap.push(Load(l.first + c_of(k), l.second));
+  }
+  std::vector<kls_item> flat;
+  m->starts.assign(grid + 1, 0);
+  for (int b = 0; b < grid; ++b) {
+    m->starts[b] = (int)flat.size();
+    for (int k : per[b]) flat.push_back(m->items[k]);
+  }
+  m->starts[grid] = (int)flat.size();
+  m->items.swap(flat);
+  m->grid = grid;
+  return KLS_OK;
+}
+
+int launch_batch(kls_multi* m) {
+  int r;
+  const int np = (int)m->pairs.size();
+  if (m->mode == KLS_MODE_FP64) {
+    r = kls_multi_launch_f64(m->stream, m->d_md, m->d_pairs, np, m->d_items, (int)m->items.size(),
+                             m->d_counter, m->grid, m->max_K_pad);
+  } else {
+    // the mixed weights are converted from the FP64 weights of the same pass
+    r = kls_multi_launch_f64_weights(m->stream, m->d_md, m->d_pairs, np, m->max_K_pad);
+    if (!r)
+      r = kls_multi_launch_mixed(m->stream, m->d_md, m->d_pairs, np, m->d_items, m->d_starts,
+                                 m->grid, m->max_K_pad, m->d_err);
+  }
+  if (r) return mcuda(m, (cudaError_t)r, "uneven batch launch");
+  r = kls_multi_launch_lu(m->stream, m->d_md, m->d_pairs, np, m->max_Na);
+  if (r) return mcuda(m, (cudaError_t)r, "uneven batch LU launch");
+  return KLS_OK;
+}
+
+// H2D omegas, the batch, D2H results: recorded once into a graph
+int capture(kls_multi* m) {
+  const size_t nz = (size_t)m->n_models * m->batch;
+  // one eager pass first: kernel attributes are set outside the capture and
+  // the launch shapes are checked before they are recorded
+  for (int i = 0; i < m->n_models; ++i)
+    for (int z = 0; z < m->batch; ++z) {
+      m->h_omega[2 * ((size_t)i * m->batch + z)] = m->ctx[i]->cfg.m * 0.4;
+      m->h_omega[2 * ((size_t)i * m->batch + z) + 1] = 0.1;
+    }
+  KM_CK(m, cudaMemcpyAsync(m->d_omega, m->h_omega, nz * 2 * sizeof(double),
+                           cudaMemcpyHostToDevice, m->stream));
+  int r = launch_batch(m);
+  if (r) return r;
+  KM_CK(m, cudaMemcpyAsync(m->h_err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  KM_CK(m, cudaStreamSynchronize(m->stream));
+  if (*m->h_err)
+    return mfail(m, KLS_ERR_CUDA,
+                 "mixed contraction pipeline timed out (code " + std::to_string(*m->h_err) + ")");
+  KM_CK(m, cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemcpyAsync(m->d_omega, m->h_omega, nz * 2 * sizeof(double),
+                                  cudaMemcpyHostToDevice, m->stream);
+  if (e != cudaSuccess) r = mcuda(m, e, "cudaMemcpyAsync (omegas)");
+  if (!r) r = launch_batch(m);
+  if (!r && (e = cudaMemcpyAsync(m->h_det, m->d_det, nz * sizeof(double2), cudaMemcpyDeviceToHost,
+                                 m->stream)) != cudaSuccess)
+    r = mcuda(m, e, "cudaMemcpyAsync (dets)");
+  if (!r && (e = cudaMemcpyAsync(m->h_logabs, m->d_logabs, nz * sizeof(double),
+                                 cudaMemcpyDeviceToHost, m->stream)) != cudaSuccess)
+    r = mcuda(m, e, "cudaMemcpyAsync (log|det|)");
+  if (!r && (e = cudaMemcpyAsync(m->h_err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                                 m->stream)) != cudaSuccess)
+    r = mcuda(m, e, "cudaMemcpyAsync (error flag)");
+  cudaGraph_t g = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(m->stream, &g);
+  if (r) {
+    if (g) cudaGraphDestroy(g);
+    return r;
+  }
+  if (ee != cudaSuccess) return mcuda(m, ee, "cudaStreamEndCapture");
+  m->graph = g;
+  KM_CK(m, cudaGraphInstantiate(&m->exec, g, 0));
+  return KLS_OK;
+}
+
+int replay(kls_multi* m) {
+  KM_CK(m, cudaEventRecord(m->ev0, m->stream));
+  KM_CK(m, cudaGraphLaunch(m->exec, m->stream));
+  KM_CK(m, cudaEventRecord(m->ev1, m->stream));
+  KM_CK(m, cudaStreamSynchronize(m->stream));
+  KM_CK(m, cudaEventElapsedTime(&m->last_ms, m->ev0, m->ev1));
+  m->replays++;
+  if (*m->h_err) {
+    int code = *m->h_err;
+    *m->h_err = 0;
+    cudaMemsetAsync(m->d_err, 0, sizeof(int), m->stream);
+    cudaStreamSynchronize(m->stream);
+    return mfail(m, KLS_ERR_CUDA,
+                 "mixed contraction pipeline timed out (code " + std::to_string(code) + ")");
+  }
+  return KLS_OK;
+}
+
+// omegas for model i (n of them, interleaved) -> results, chunked by batch
+int run_omegas(kls_multi* m, const std::function<void(int, int, double*)>& fill, int n,
+               double* det_ri, double* log_abs) {
+  const int B = m->batch;
+  for (int b0 = 0; b0 < n; b0 += B) {
+    const int nb = std::min(B, n - b0);
+    for (int i = 0; i < m->n_models; ++i) {
+      double* o = m->h_omega + (size_t)i * B * 2;
+      for (int z = 0; z < B; ++z) fill(i, b0 + std::min(z, nb - 1), o + 2 * z);
+      for (int z = 0; z < 2 * B; ++z)
+        if (!std::isfinite(o[z])) return mfail(m, KLS_ERR_NONFINITE, "non-finite omega");
+    }
+    int r = replay(m);
+    if (r) return r;
+    for (int i = 0; i < m->n_models; ++i)
+      for (int z = 0; z < nb; ++z) {
+        const size_t src = (size_t)i * B + z, dst = (size_t)i * n + b0 + z;
+        det_ri[2 * dst] = m->h_det[2 * src];
+        det_ri[2 * dst + 1] = m->h_det[2 * src + 1];
+        if (log_abs) log_abs[dst] = m->h_logabs[src];
+      }
+  }
+  return KLS_OK;
+}
+
+void release(kls_multi* m) {
+  if (m->exec) cudaGraphExecDestroy(m->exec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  for (void* p : m->bufs) cudaFree(p);
+  m->bufs.clear();
+  if (m->h_omega) cudaFreeHost(m->h_omega);
+  if (m->h_det) cudaFreeHost(m->h_det);
+  if (m->h_logabs) cudaFreeHost(m->h_logabs);
+  if (m->h_err) cudaFreeHost(m->h_err);
+  if (m->ev0) cudaEventDestroy(m->ev0);
+  if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->stream) cudaStreamDestroy(m->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* kls_multi_last_error(const kls_multi* m) {
+  return m ? m->err.c_str() : g_multi_create_err.c_str();
+}
+
+int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, kls_multi** out) {
+  if (!out) return mfail(nullptr, KLS_ERR_CONFIG, "null output handle");
+  *out = nullptr;
+  if (!models || n_models < 1 || batch < 1 || batch > 4096)
+    return mfail(nullptr, KLS_ERR_CONFIG, "need >= 1 model and 1 <= batch <= 4096");
+  if (mode != KLS_MODE_FP64 && mode != KLS_MODE_MIXED)
+    return mfail(nullptr, KLS_ERR_CONFIG, "unknown precision mode");
+  for (int i = 0; i < n_models; ++i) {
+    if (!models[i] || !models[i]->precomputed)
+      return mfail(nullptr, KLS_ERR_STATE, "model " + std::to_string(i) + " is not precomputed");
+    if (models[i]->device != models[0]->device)
+      return mfail(nullptr, KLS_ERR_CONFIG, "all models of a batch must be on one device");
+  }
+  kls_multi* m = new kls_multi();
+  m->device = models[0]->device;
+  m->mode = mode;
+  m->batch = batch;
+  m->n_models = n_models;
+  m->ctx.assign(models, models + n_models);
+  int r = KLS_OK;
+  auto bail = [&](int code) {
+    g_multi_create_err = m->err;
+    release(m);
+    delete m;
+    return code;
+  };
+  if (cudaSetDevice(m->device) != cudaSuccess) return bail(mcuda(m, cudaGetLastError(), "cudaSetDevice"));
+  if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&m->ev0) != cudaSuccess || cudaEventCreate(&m->ev1) != cudaSuccess)
+    return bail(mcuda(m, cudaGetLastError(), "stream/event creation"));
+  const size_t nz = (size_t)n_models * batch;
+  if ((r = malloc_buf(m, &m->d_omega, 2 * nz)) || (r = malloc_buf(m, &m->d_det, nz)) ||
+      (r = malloc_buf(m, &m->d_logabs, nz)) || (r = malloc_buf(m, &m->d_counter, 1)) ||
+      (r = malloc_buf(m, &m->d_err, 1)) ||
+      (r = malloc_buf(m, &m->d_tmaps, (size_t)2 * n_models * sizeof(CUtensorMap))))
+    return bail(r);
+  if (cudaMallocHost(&m->h_omega, 2 * nz * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&m->h_det, 2 * nz * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&m->h_logabs, nz * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&m->h_err, sizeof(int)) != cudaSuccess)
+    return bail(mcuda(m, cudaErrorMemoryAllocation, "cudaMallocHost"));
+  *m->h_err = 0;
+  std::fill(m->h_omega, m->h_omega + 2 * nz, 0.0);
+  if (cudaMemset(m->d_err, 0, sizeof(int)) != cudaSuccess)
+    return bail(mcuda(m, cudaGetLastError(), "cudaMemset"));
+
+  m->md.resize(n_models);
+  for (int i = 0; i < n_models; ++i) {
+    kls_ctx* c = models[i];
+    kls_mdesc d{};
+    d.Wre = c->d_Wre;
+    d.Wim = c->d_Wim;
+    d.Gk = c->d_Gk;
+    d.Ok = c->d_Ok;
+    d.Nk = c->d_N;
+    d.omega = m->d_omega + (size_t)2 * i * batch;
+    d.det = m->d_det + (size_t)i * batch;
+    d.logabs = m->d_logabs + (size_t)i * batch;
+    d.G = c->cfg.G;
+    d.K_pad = c->K_pad;
+    d.Na = c->Na;
+    d.Na_pad = c->Na_pad;
+    d.model = i;
+    if ((r = malloc_buf(m, &d.wt, (size_t)batch * c->K_pad))) return bail(r);
+    if ((r = malloc_buf(m, &d.A, (size_t)batch * c->Na * c->Na))) return bail(r);
+    if (mode == KLS_MODE_FP64) {
+      d.splits = c->splits;
+      d.k_per_split = kls_f64_k_per_split(c->K_pad, c->splits);
+      if ((r = malloc_buf(m, &d.part, (size_t)batch * d.splits * c->Na_pad * c->Na_pad)))
+        return bail(r);
+    } else {
+      if (!c->mixed && (r = kls_mixed_prepare(c))) return bail(mfail(m, r, c->err));
+      const void *xl = nullptr, *th = nullptr, *tl = nullptr;
+      d.Xh = kls_mixed_tables(c, &xl, &th, &tl);
+      d.Xl = xl;
+      uint8_t* dm = m->d_tmaps + (size_t)2 * i * sizeof(CUtensorMap);
+      if (cudaMemcpy(dm, th, sizeof(CUtensorMap), cudaMemcpyHostToDevice) != cudaSuccess ||
+          cudaMemcpy(dm + sizeof(CUtensorMap), tl, sizeof(CUtensorMap),
+                     cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (tensor maps)"));
+      d.tmap_h = dm;
+      d.tmap_l = dm + sizeof(CUtensorMap);
+      d.nkb_total = (int)(c->K_pad / MIX_BK);
+      const int s = kls_mixed_splits_of(c);
+      d.kb_per_split = (d.nkb_total + s - 1) / s;
+      d.msplits = (d.nkb_total + d.kb_per_split - 1) / d.kb_per_split;   // non-empty splits
+      d.om_per_item = 2;
+      float2* w32 = nullptr;
+      double* mp = nullptr;
+      const size_t R = 2 * (size_t)c->Na_pad;
+      if ((r = malloc_buf(m, &w32, (size_t)batch * c->K_pad)) ||
+          (r = malloc_buf(m, &mp, (size_t)batch * d.msplits * R * R)))
+        return bail(r);
+      d.wt32 = w32;
+      d.mpart = mp;
+    }
+    m->md[i] = d;
+    m->max_Na = std::max(m->max_Na, c->Na);
+    m->max_K_pad = std::max(m->max_K_pad, c->K_pad);
+  }
+  if ((r = build_items(m))) return bail(r);
+  if ((r = malloc_buf(m, &m->d_md, m->md.size())) ||
+      (r = malloc_buf(m, &m->d_items, m->items.size())) ||
+      (r = malloc_buf(m, &m->d_pairs, m->pairs.size())) ||
+      (r = malloc_buf(m, &m->d_starts, std::max<size_t>(m->starts.size(), 1))))
+    return bail(r);
+  if (cudaMemcpy(m->d_md, m->md.data(), m->md.size() * sizeof(kls_mdesc), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(m->d_items, m->items.data(), m->items.size() * sizeof(kls_item),
+                 cudaMemcpyHostToDevice) ||
+      cudaMemcpy(m->d_pairs, m->pairs.data(), m->pairs.size() * sizeof(int2),
+                 cudaMemcpyHostToDevice) ||
+      (!m->starts.empty() && cudaMemcpy(m->d_starts, m->starts.data(),
+                                        m->starts.size() * sizeof(int), cudaMemcpyHostToDevice)))
+    return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (descriptors)"));
+  if ((r = capture(m))) return bail(r);
+  *out = m;
+  return KLS_OK;
+}
+
+int kls_multi_destroy(kls_multi* m) {
+  if (!m) return KLS_OK;
+  cudaSetDevice(m->device);
+  release(m);
+  delete m;
+  return KLS_OK;
+}
+
+int kls_multi_det(kls_multi* m, const double* omega_ri, int n, double* det_ri, double* log_abs) {
+  if (!m) return KLS_ERR_CONFIG;
+  if (n < 0 || (n > 0 && (!omega_ri || !det_ri)))
+    return mfail(m, KLS_ERR_CONFIG, "bad omega / output buffers");
+  KM_CK(m, cudaSetDevice(m->device));
+  auto fill = [&](int i, int k, double* o) {
+    o[0] = omega_ri[2 * ((size_t)i * n + k)];
+    o[1] = omega_ri[2 * ((size_t)i * n + k) + 1];
+  };
+  return run_omegas(m, fill, n, det_ri, log_abs);
+}
+
+int kls_scan_multi(kls_multi* m, const kls_scan_cfg* sc, double* det_grid, double* log_abs_grid,
+                   double* Op0, double* g0) {
+  if (!m) return KLS_ERR_CONFIG;
+  if (!sc || sc->n_Op < 1 || sc->n_gamma < 1 || !det_grid)
+    return mfail(m, KLS_ERR_CONFIG, "bad scan configuration");
+  KM_CK(m, cudaSetDevice(m->device));
+  const int nO = sc->n_Op, nG = sc->n_gamma, n = nO * nG;
+  // column-major grid per model, omega = m_model * Omega_p + i gamma (GridScan.jl:47, :101-104)
+  auto fill = [&](int i, int q, double* o) {
+    const int ig = q % nG, jo = q / nG;
+    o[0] = m->ctx[i]->cfg.m * kls_lin(sc->Omega_p_min, sc->Omega_p_max, nO, jo);
+    o[1] = kls_lin(sc->gamma_min, sc->gamma_max, nG, ig);
+  };
+  std::vector<double> la;
+  double* lap = log_abs_grid;
+  if (!lap) {
+    la.resize((size_t)m->n_models * n);
+    lap = la.data();
+  }
+  int r = run_omegas(m, fill, n, det_grid, lap);
+  if (r) return r;
+  for (int i = 0; i < m->n_models; ++i) {
+    const double* d = det_grid + (size_t)2 * i * n;
+    int best = 0;
+    double bv = INFINITY;
+    for (int q = 0; q < n; ++q) {
+      double v = std::hypot(d[2 * q], d[2 * q + 1]);
+      if (std::isnan(v)) { best = q; break; }
+      if (v < bv) { bv = v; best = q; }
+    }
+    if (Op0) Op0[i] = kls_lin(sc->Omega_p_min, sc->Omega_p_max, nO, best / nG);
+    if (g0) g0[i] = kls_lin(sc->gamma_min, sc->gamma_max, nG, best % nG);
+  }
+  return KLS_OK;
+}
+
+int kls_multi_get_info(const kls_multi* m, kls_multi_info* out) {
+  if (!m || !out) return KLS_ERR_CONFIG;
+  out->n_models = m->n_models;
+  out->batch = m->batch;
+  out->mode = m->mode;
+  out->n_items = (int32_t)m->items.size();
+  out->grid = m->grid;
+  out->graph = m->exec ? 1 : 0;
+  out->replays = m->replays;
+  out->last_ms = m->last_ms;
+  // kernels per replay: weights (+ FP32 copy), contraction, reduction, LU
+  out->launches_per_replay = m->mode == KLS_MODE_FP64 ? 4 : 5;
+  return KLS_OK;
+}
+
+}  // extern "C"

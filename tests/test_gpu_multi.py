@@ -1,0 +1,120 @@
+"""Uneven batch over models (kls_multi) and the autotuner on the GPU.
+
+* A batch of models of different NR, Ne, N_alpha, l range and m gives, in one
+  persistent launch per pass, bitwise the determinants each model's own
+  context gives (FP64 and split-BF16 forms), including a partial last pass.
+* kls_scan_multi returns each model's grid_scan grid and argmin.
+* The passes replay one captured CUDA graph.
+* kls_autotune picks one of its candidates, caches it, and the determinant
+  after tuning agrees with the untuned one to FP64 rounding (a different
+  split count only regroups the FP64 sum).
+"""
+import numpy as np
+import pytest
+
+import kalnajs_log_spirals_b200 as K
+from tests.test_gpu_parity import kconfig
+
+pytestmark = pytest.mark.gpu
+
+BASE = dict(G=1.0, L0=1.0, Rc_min=0.01, Rc_max=10.0, v_min=0.01, alpha_max=10.0, nw=2001,
+            nwa=101)
+# (m, n_zang, q1, NR, Ne, N_alpha, l_max): three sizes, both m
+MODELS = [(2, 4, 7.0, 41, 11, 41, 10), (3, 3, 9.5, 31, 9, 97, 6), (2, 6, 5.2, 61, 13, 63, 16),
+          (3, 5, 11.0, 21, 7, 33, 4)]
+
+
+def configs():
+    return [kconfig(**BASE, m=m, n_zang=nz, q1=q, NR=nr, Ne=ne, N_alpha=na, l_min=-lm, l_max=lm)
+            for m, nz, q, nr, ne, na, lm in MODELS]
+
+
+def omegas(n, seed):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(0.3, 0.6, n) * 2 + 1j * rng.uniform(0.02, 0.25, n)
+
+
+@pytest.fixture(scope="module")
+def pcs(lib_path):
+    p = [K.precompute_all(c) for c in configs()]
+    yield p
+    for x in p:
+        x.close()
+
+
+@pytest.mark.parametrize("Tgpu", ["Float64", "Float32"])
+def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu):
+    n = 7                                  # passes of 3: 3 + 3 + 1
+    om = np.stack([omegas(n, 10 + i) * (m / 2) for i, (m, *_) in enumerate(MODELS)])
+    singles = []
+    for pc, o in zip(pcs, om):
+        dev = K.to_device(pc, K.GPUType.NVIDIA, Tgpu)
+        singles.append(K.compute_determinant_batched(o, pc, dev, batch_size=16, log_abs=True))
+    mb = K.ModelBatch(pcs, Tgpu, batch=3)
+    d, la = mb.det(om)
+    info = mb.info()
+    mb.close()
+    for i, (ds, ls) in enumerate(singles):
+        assert np.array_equal(d[i], ds), (i, np.max(np.abs(d[i] - ds) / np.abs(ds)))
+        assert np.array_equal(la[i], ls), i
+    assert info["graph"] == 1 and info["replays"] == 3 and info["n_models"] == len(MODELS)
+    assert info["launches_per_replay"] >= 4 and info["n_items"] > info["grid"] > 0
+
+
+def test_mixed_batch_close_to_fp64_batch(pcs):
+    om = np.stack([omegas(4, 20 + i) * (m / 2) for i, (m, *_) in enumerate(MODELS)])
+    a = K.ModelBatch(pcs, "Float64", batch=4)
+    b = K.ModelBatch(pcs, "Float32", batch=4)
+    d64, _ = a.det(om)
+    d32, _ = b.det(om)
+    a.close()
+    b.close()
+    assert np.max(np.abs(d32 - d64) / np.abs(d64)) < 1e-3
+
+
+def test_scan_multi_matches_grid_scan(pcs):
+    mb = K.ModelBatch(pcs, "Float64", batch=16)
+    dg, la, Op0, g0 = mb.scan(n_Op=9, n_gamma=5, Omega_p_range=(0.2, 0.6), gamma_range=(0.01, 0.2))
+    mb.close()
+    for i, pc in enumerate(pcs):
+        cfg = pc.config
+        cfg.scan.n_Op, cfg.scan.n_gamma = 9, 5
+        cfg.scan.Omega_p_min, cfg.scan.Omega_p_max = 0.2, 0.6
+        cfg.scan.gamma_min, cfg.scan.gamma_max = 0.01, 0.2
+        ref, o0, gg0 = K.grid_scan(cfg, pc)
+        assert dg[i].shape == ref.shape
+        assert np.array_equal(dg[i], ref)
+        assert np.allclose(la[i], np.log(np.abs(ref)), rtol=0, atol=1e-12)
+        assert (Op0[i], g0[i]) == (o0, gg0)
+
+
+@pytest.mark.parametrize("Tgpu", ["Float64", "Float32"])
+def test_autotune(lib_path, Tgpu):
+    c = configs()[2]
+    pc = K.precompute_all(c)
+    dev = K.to_device(pc, K.GPUType.NVIDIA, Tgpu)
+    om = omegas(3, 5)
+    before = K.compute_determinant_batched(om, pc, dev)
+    t = K.autotune(pc, Tgpu, batch=2)
+    assert t.candidates >= 2 and t.splits >= 1 and t.default_splits >= 1
+    assert 0 < t.ms_per_omega <= t.default_ms_per_omega * 1.0001
+    after = K.compute_determinant_batched(om, pc, dev)
+    tol = 1e-12 if Tgpu == "Float64" else 1e-5
+    assert np.max(np.abs(after - before) / np.abs(before)) < tol
+    again = K.autotune(pc, Tgpu, batch=2)          # process cache
+    assert again.candidates == 0 and again.splits == t.splits
+    # a batch built after tuning keeps the tuned split count: still bitwise
+    mb = K.ModelBatch([pc], Tgpu, batch=3)
+    d, _ = mb.det(om[None, :])
+    mb.close()
+    assert np.array_equal(d[0], after)
+    pc.close()
+
+
+def test_multi_rejects_bad_input(pcs):
+    with pytest.raises(K.KlsError):
+        K.ModelBatch(pcs, "Float64", batch=0)
+    mb = K.ModelBatch(pcs[:1], "Float64", batch=2)
+    with pytest.raises(K.KlsError):
+        mb.det(np.array([[np.nan + 0j, 1.0 + 0.1j]]))
+    mb.close()
