@@ -56,6 +56,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--accuracy-points", type=int, default=200)
+    ap.add_argument("--no-proposer", action="store_true",
+                    help="skip the learned-proposal time-to-root block")
+    ap.add_argument("--full-scan", action="store_true",
+                    help="time the whole FP64 41x20 scan instead of two of its columns")
+    ap.add_argument("--no-uneven", action="store_true",
+                    help="skip the 16-model uneven batched scan block")
+    ap.add_argument("--uneven-passes", type=int, default=3)
+    ap.add_argument("--uneven-batch", type=int, default=4)
     return ap.parse_args()
 
 
@@ -213,6 +221,175 @@ def omegas_for_step(step: int, rank: int, m: int, Op: float, g: float, delta: fl
     Op_s = Op + 1e-4 * ((step * 7 + rank * 131) % 97) / 97.0
     g_s = g + 1e-4 * ((step * 13 + rank * 71) % 89) / 89.0
     return [complex(m * Op_s, g_s), complex(m * (Op_s + delta), g_s), complex(m * Op_s, g_s + delta)]
+
+
+# ---------------------------------------------------------------------------
+# time-to-root: the reference workflow (41 x 20 grid scan, argmin, Newton) in
+# plain FP64 against a learned proposal + mixed/FP64 hybrid Newton
+# ---------------------------------------------------------------------------
+def time_to_root(args, K, P, cfg, pc, local, sync):
+    import numpy as np
+    from kalnajs_log_spirals_b200.api import newton_search_hybrid
+    out = {}
+    # proposer: trained on 2^17 samples of one batched scan over 64 seeded
+    # random models (small size), by the library's own BF16 kernels
+    base = K.load_model(K.load_config(os.path.join(ROOT, "configs", "size_s.toml")), args.model)
+    t0 = time.perf_counter()
+    specs = P.random_models(64, seed=2024)
+    X, T = P.scan_samples(base, specs, n_Op=64, n_gamma=32, batch=16, device=local)
+    t_gen = time.perf_counter() - t0
+    mlp = P.MLP(256, 4, seed=0, device=local)
+    t0 = time.perf_counter()
+    hist = mlp.train(X, T, epochs=150, batch=1024, lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t0
+    out["proposer_training"] = {
+        "samples": int(X.shape[0]), "models": len(specs), "model_seed": 2024,
+        "sample_grid": "64 x 32 over Omega_p [0.2, 0.8], gamma [0.01, 0.30] per model",
+        "model_size": "NR=101 Ne=21 N_alpha=101 l=[-25,25]", "network": "5-256-256-256-3 GELU",
+        "epochs": 150, "sample_gen_s": t_gen, "train_s": t_train,
+        "loss_first_last": [float(hist[0]), float(hist[-1])]}
+    s = cfg.scan
+    Op_grid = np.linspace(s.Omega_p_min, s.Omega_p_max, s.n_Op)
+    g_grid = np.linspace(s.gamma_min, s.gamma_max, s.n_gamma)
+    m = cfg.physics.m
+    devmx = K.to_device(pc, K.GPUType.NVIDIA, "Float32")
+    spec = P.ModelSpec(int(cfg.model.n_zang), float(cfg.model.q1), int(m))
+
+    # learned proposal + hybrid Newton
+    sync()
+    t0 = time.perf_counter()
+    Op_p, g_p, used = P.propose(mlp, spec, lambda om: K.compute_determinant_batched(
+        om, pc, devmx, batch_size=16), k=48, n_Op=s.n_Op, n_gamma=s.n_gamma,
+        Op_range=(s.Omega_p_min, s.Omega_p_max), g_range=(s.gamma_min, s.gamma_max))
+    t_prop = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rh = newton_search_hybrid(cfg, pc, Op_p, g_p)
+    t_hyb = time.perf_counter() - t0
+    mlp.close()
+
+    # plain FP64 reference workflow
+    sync()
+    t0 = time.perf_counter()
+    dgm, Op_m, g_m = K.grid_scan(cfg, pc, devmx)
+    t_scan_mx = time.perf_counter() - t0
+    if args.full_scan:
+        t0 = time.perf_counter()
+        dg64, Op64, g64 = K.grid_scan(cfg, pc, None)
+        t_scan64 = time.perf_counter() - t0
+        scan_note = "measured: whole 41 x 20 FP64 scan"
+    else:
+        # two whole columns of the FP64 scan (the mixed argmin's and its
+        # neighbour), the same batches of 16 the scan launches; every point
+        # costs the same, so the scan time is the column time x n_Op / 2
+        j = int(np.argmin(np.abs(Op_grid - Op_m)))
+        cols = [j, j + 1 if j + 1 < s.n_Op else j - 1]
+        om = np.array([m * Op_grid[c] + 1j * g for c in cols for g in g_grid])
+        t0 = time.perf_counter()
+        d64 = K.compute_determinant_batched(om, pc, None, batch_size=16)
+        t_cols = time.perf_counter() - t0
+        t_scan64 = t_cols * s.n_Op / len(cols)
+        q = int(np.argmin(np.abs(d64)))
+        Op64, g64 = float(Op_grid[cols[q // s.n_gamma]]), float(g_grid[q % s.n_gamma])
+        scan_note = (f"extrapolated: columns {cols} of {s.n_Op} ({len(om)} FP64 dets in "
+                     f"{t_cols:.2f} s) x {s.n_Op}/{len(cols)}; FP64 argmin of those columns "
+                     f"{'equals' if (Op64, g64) == (Op_m, g_m) else 'differs from'} the mixed scan's")
+    sync()
+    t0 = time.perf_counter()
+    r64 = K.newton_search(cfg, pc, None, K.GPUType.NVIDIA, "Float64", Op64, g64)
+    t_n64 = time.perf_counter() - t0
+    dOp, dg = abs(rh.Omega_p - r64.Omega_p), abs(rh.gamma - r64.gamma)
+    plain_total = t_scan64 + t_n64
+    learned_total = t_prop + t_hyb
+    out.update({
+        "workflow": "grid_scan 41x20 -> argmin -> Newton (tol %g)" % cfg.newton.tol,
+        "plain_fp64": {"scan_s": t_scan64, "scan": scan_note, "newton_s": t_n64,
+                       "total_s": plain_total, "start": [Op64, g64],
+                       "Omega_p": r64.Omega_p, "gamma": r64.gamma, "converged": r64.converged,
+                       "det_evals": s.n_Op * s.n_gamma + r64.det_evals},
+        "mixed_scan_then_hybrid": {"scan_s": t_scan_mx, "start": [float(Op_m), float(g_m)],
+                                   "total_s": t_scan_mx + t_hyb,
+                                   "note": "hybrid Newton time of the proposal row (same start)"
+                                   if (Op_m, g_m) == (Op_p, g_p) else "start differs from proposal"},
+        "learned_proposal_then_hybrid": {
+            "propose_s": t_prop, "mixed_dets_for_proposal": used, "start": [Op_p, g_p],
+            "newton_s": t_hyb, "total_s": learned_total, "Omega_p": rh.Omega_p,
+            "gamma": rh.gamma, "converged": rh.converged, "mixed_evals": rh.mixed_evals,
+            "fp64_evals": rh.fp64_evals},
+        "abs_dOmega_p": dOp, "abs_dgamma": dg,
+        "same_root_within_1e-10": bool(rh.converged and r64.converged and dOp <= 1e-10
+                                       and dg <= 1e-10),
+        "speedup_learned_vs_plain": plain_total / learned_total,
+        "timing": "host wall clock around synchronous library calls"})
+    return out
+
+
+# ---------------------------------------------------------------------------
+# uneven batched scan: 16 seeded models of three sizes, one persistent launch
+# per pass, split-BF16 form, autotuned K splits
+# ---------------------------------------------------------------------------
+def uneven_batch(args, K, P, local, sync):
+    import numpy as np
+    base = K.load_model(K.load_config(args.config), args.model)
+    specs = P.random_models(16, seed=0, sizes=P.SIZES)
+    t0 = time.perf_counter()
+    pcs, tunes = [], []
+    for sp in specs:
+        pc = K.precompute_all(P.model_config(base, sp), device=local)
+        pc.ctx.call("kls_prepare_mixed")
+        tunes.append(K.autotune(pc, "Float32", batch=args.uneven_batch))
+        K.release_fp64(pc)
+        pcs.append(pc)
+    sync()
+    t_setup = time.perf_counter() - t0
+    B, npass = args.uneven_batch, args.uneven_passes
+    nO, nG = 256, 128
+    Op = np.linspace(0.2, 0.8, nO)
+    gm = np.linspace(0.01, 0.30, nG)
+    q = np.arange((npass + 1) * B)                  # first grid points, column-major
+    pts = Op[q // nG], gm[q % nG]
+    om = np.stack([sp.m * pts[0] + 1j * pts[1] for sp in specs])
+    mb = K.ModelBatch(pcs, "Float32", batch=B)
+    mb.det(om[:, :B])                                 # warm-up pass
+    sync()
+    t0 = time.perf_counter()
+    dev_ms = 0.0
+    for p in range(1, npass + 1):
+        mb.det(om[:, p * B:(p + 1) * B])
+        dev_ms += mb.info()["last_ms"]
+    t_wall = time.perf_counter() - t0
+    info = mb.info()
+    mb.close()
+    n_det = len(specs) * B * npass
+    # the same omegas model by model through each context's own batch call
+    sync()
+    t0 = time.perf_counter()
+    for pc, o in zip(pcs, om):
+        dev = K.to_device(pc, K.GPUType.NVIDIA, "Float32")
+        for p in range(1, npass + 1):
+            K.compute_determinant_batched(o[p * B:(p + 1) * B], pc, dev, batch_size=B)
+    t_seq = time.perf_counter() - t0
+    for pc in pcs:
+        pc.close()
+    rate = n_det / (dev_ms * 1e-3)
+    sizes = [sp.size for sp in specs]
+    return {
+        "models": len(specs), "model_seed": 0, "sizes": {str(sz): sizes.count(sz) for sz in P.SIZES},
+        "grid": "256 x 128 over Omega_p [0.2, 0.8], gamma [0.01, 0.30]",
+        "omegas_per_model_per_pass": B, "passes_timed": npass,
+        "det_evals_per_s": rate, "ms_per_pass_device": dev_ms / npass,
+        "wall_det_evals_per_s": n_det / t_wall,
+        "one_model_at_a_time_det_evals_per_s": n_det / t_seq,
+        "projected_full_grid_s": len(specs) * nO * nG / rate,
+        "batch_launch": {"items": info["n_items"], "ctas": info["grid"],
+                         "schedule": ["persistent round robin", "one CTA per item"][info["schedule"]],
+                         "schedule_pass_ms": info["schedule_ms"],
+                         "graph_replay": bool(info["graph"]),
+                         "kernels_per_pass": info["launches_per_replay"]},
+        "autotune": [{"splits": t.splits, "default": t.default_splits,
+                      "ms_per_omega": t.ms_per_omega,
+                      "default_ms_per_omega": t.default_ms_per_omega} for t in tunes],
+        "setup_s": t_setup,
+        "form": "split-BF16 (FP64 tables released after the split)"}
 
 
 def ours(args):
@@ -402,12 +579,23 @@ def ours(args):
                 "abs_dgamma_vs_plain": abs(rh.gamma - r.gamma)}
             newton["speedup_hybrid_vs_plain"] = t_plain / t_h
 
+    # the two workflow blocks run at N = 1 only (the scaling run times the
+    # headline step alone)
+    ttr = None
+    if world == 1 and not args.no_proposer and not args.no_mixed:
+        from kalnajs_log_spirals_b200 import proposer as P
+        ttr = time_to_root(args, K, P, cfg, pc, local, torch.cuda.synchronize)
+    pc.close()
+    uneven = None
+    if world == 1 and not args.no_uneven:
+        from kalnajs_log_spirals_b200 import proposer as P
+        uneven = uneven_batch(args, K, P, local, torch.cuda.synchronize)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         rate, threads, sample = cpu_det_rate(cfg)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
 
-    pc.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -439,6 +627,8 @@ def ours(args):
         "precompute_s": t_pre,
         "mixed": mixed,
         "newton": newton,
+        "time_to_root": ttr,
+        "uneven_batch": uneven,
     }
     print(json.dumps(line), flush=True)
     return 0

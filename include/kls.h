@@ -128,6 +128,12 @@ int kls_set_stream(kls_ctx* ctx, void* cuda_stream);
 int kls_precompute(kls_ctx* ctx);
 /* Build the split-BF16 copy of the W table used by KLS_MODE_MIXED.         */
 int kls_prepare_mixed(kls_ctx* ctx);
+/* Free the FP64 W table after building the split-BF16 copy (no reference
+ * counterpart): a mixed-only context, 13 GB instead of 40 GB at NR=501,
+ * Ne=51, N_alpha=301, l in [-100, 100], so that many default-size models fit
+ * one GPU.  Afterwards KLS_MODE_FP64 calls, kls_export_W and FP64 batches
+ * return KLS_ERR_STATE.                                                     */
+int kls_release_fp64(kls_ctx* ctx);
 
 /* ---- exports in reference layout (host, column-major) ------------------- *
  * Omega_1/Omega_2/jacobian/F0/FE/FL/DJ: [NR, Ne]; w1/ra/pha: [nwa, NR, Ne]
@@ -246,6 +252,10 @@ typedef struct kls_multi_info {
     int32_t launches_per_replay;  /* kernels in one pass                      */
     int64_t replays;              /* passes so far                            */
     double  last_ms;              /* device time of the last pass (ms)        */
+    int32_t schedule;             /* mixed form: 0 persistent round robin,
+                                     1 one CTA per item (the faster of the two
+                                     passes timed at creation)                */
+    double  schedule_ms[2];       /* those two passes (ms)                    */
 } kls_multi_info;
 int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, kls_multi** out);
 int kls_multi_destroy(kls_multi* mm);

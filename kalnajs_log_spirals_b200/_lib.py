@@ -75,7 +75,8 @@ class kls_multi_info(C.Structure):
     _fields_ = [("n_models", C.c_int32), ("batch", C.c_int32), ("mode", C.c_int32),
                 ("n_items", C.c_int32), ("grid", C.c_int32), ("graph", C.c_int32),
                 ("launches_per_replay", C.c_int32), ("replays", C.c_int64),
-                ("last_ms", C.c_double)]
+                ("last_ms", C.c_double), ("schedule", C.c_int32),
+                ("schedule_ms", C.c_double * 2)]
 
 
 class kls_tune_result(C.Structure):
@@ -97,6 +98,7 @@ SIGNATURES = {
     "kls_set_stream": (C.c_int, [_P, _P]),
     "kls_precompute": (C.c_int, [_P]),
     "kls_prepare_mixed": (C.c_int, [_P]),
+    "kls_release_fp64": (C.c_int, [_P]),
     "kls_export_orbits": (C.c_int, [_P] + [_D] * 10),
     "kls_export_grids": (C.c_int, [_P] + [_D] * 6),
     "kls_export_alpha": (C.c_int, [_P] + [_D] * 3),

@@ -311,6 +311,12 @@ def to_device(precomp: PrecomputedData, gpu_type: GPUType = GPUType.NVIDIA,
                              mode, precomp)
 
 
+def release_fp64(precomp: PrecomputedData) -> None:
+    """Keep only the split-BF16 table (kls_release_fp64): FP64 evaluations of
+    this precompute raise KlsError afterwards."""
+    precomp.ctx.call("kls_release_fp64")
+
+
 def _mode(devprecomp: Optional[DevicePrecomputed]) -> int:
     return KLS_MODE_FP64 if devprecomp is None else devprecomp.mode
 
@@ -612,7 +618,9 @@ class ModelBatch:
     def info(self) -> dict:
         i = _lib.kls_multi_info()
         self._ck(self.lib.kls_multi_get_info(self.h, C.byref(i)))
-        return {f: getattr(i, f) for f, _ in i._fields_}
+        d = {f: getattr(i, f) for f, _ in i._fields_}
+        d["schedule_ms"] = list(i.schedule_ms)
+        return d
 
     def close(self):
         if getattr(self, "h", None):

@@ -110,6 +110,7 @@ int run_batch(kls_ctx* c, int n, int mode, bool export_M) {
   if ((r = kls_run_weights(c, n))) return r;
   if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[1], c->stream));
   if (mode == KLS_MODE_FP64) {
+    if (!c->d_Wre) return kls_fail(c, KLS_ERR_STATE, "the FP64 table was released (kls_release_fp64)");
     if ((r = kls_run_contract_f64(c, n, splits))) return r;
   } else if (mode == KLS_MODE_MIXED) {
     if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
@@ -310,6 +311,20 @@ int kls_prepare_mixed(kls_ctx* c) {
   return kls_mixed_prepare(c);
 }
 
+int kls_release_fp64(kls_ctx* c) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
+  KLS_CK(c, cudaStreamSynchronize(c->stream));
+  if (c->d_Wre) {
+    cudaFree(c->d_Wre);
+    cudaFree(c->d_Wim);
+    c->d_Wre = c->d_Wim = nullptr;
+    c->device_bytes -= (int64_t)(2 * (size_t)c->K_pad * c->Na_pad * sizeof(double));
+  }
+  return KLS_OK;
+}
+
 int kls_export_orbits(kls_ctx* c, double* Om1, double* Om2, double* jac, double* F0,
                       double* FE, double* FL, double* DJ, double* w1, double* ra, double* pha) {
   int r = check_ready(c);
@@ -359,6 +374,8 @@ int kls_export_resonant(kls_ctx* c, double* F0l, double* Ores) {
 }
 
 int kls_export_W(kls_ctx* c, int il0, int nl, double* W) {
+  if (c->precomputed && !c->d_Wre)
+    return kls_fail(c, KLS_ERR_STATE, "the FP64 table was released (kls_release_fp64)");
   int r = check_ready(c);
   if (r) return r;
   if (il0 < 0 || nl < 0 || il0 + nl > c->n_l || !W)
@@ -731,6 +748,8 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
   if (mode != KLS_MODE_FP64 && mode != KLS_MODE_MIXED)
     return kls_fail(c, KLS_ERR_CONFIG, "unknown precision mode");
   if (batch < 1 || batch > WS_CHUNK) return kls_fail(c, KLS_ERR_CONFIG, "bad autotune batch");
+  if (mode == KLS_MODE_FP64 && !c->d_Wre)
+    return kls_fail(c, KLS_ERR_STATE, "the FP64 table was released (kls_release_fp64)");
   if (mode == KLS_MODE_MIXED && !c->mixed && (r = kls_mixed_prepare(c))) return r;
   const int def = mode == KLS_MODE_FP64 ? kls_choose_splits(c) : kls_mixed_default_splits(c);
   const int max_s = mode == KLS_MODE_FP64 ? (int)std::max<int64_t>(1, c->K_pad / (16 * 8))

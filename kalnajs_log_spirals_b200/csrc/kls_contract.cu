@@ -225,8 +225,9 @@ contract_kernel(ContractParams P, const double* __restrict__ Wre, const double* 
 
 // Persistent form over an uneven batch: every CTA takes work items
 // (model, omega, tile, split) from an atomic counter until the list is
-// exhausted.  Items are listed longest first, so the tail of the launch is
-// made of the short items of the small models.  Each item computes exactly
+// exhausted.  The list runs model by model, largest first, tile fastest, so
+// CTAs running together share a k-range of one table (L2 reuse) and the tail
+// of the launch is made of the small models' items.  Each item computes exactly
 // what contract_kernel computes for the same (tile, split, omega), so a
 // determinant is bitwise the same in either form.
 __global__ void __launch_bounds__(CT_THREADS, 2)

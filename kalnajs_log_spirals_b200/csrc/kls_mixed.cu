@@ -604,9 +604,9 @@ __device__ __forceinline__ void tensormap_acquire(const void* map) {
 }
 
 // Persistent form of mixed_contract_kernel over an uneven batch of models.
-// CTA b takes items [starts[b], starts[b+1]) of a list the host balanced
-// across CTAs (longest item first onto the least-loaded CTA); every role
-// walks the same items, and the stage, weights-slot and
+// CTA b takes items [starts[b], starts[b+1]) of a list the host ordered
+// (round robin over a model-major list, so CTAs running at the same time
+// share a k-range of one table); every role walks the same items, and the stage, weights-slot and
 // accumulator phases run on counters that continue across items, so the
 // pipeline never drains between items.  An item computes exactly what the
 // one-model kernel computes for the same (tile, split, omegas): the same

@@ -12,9 +12,9 @@
 //   -> split reduction (all models) -> LU (all models) -> D2H dets
 //
 // captured once into a CUDA graph and replayed for every chunk of omegas.
-// The FP64 contraction takes items from an atomic counter, longest first; the
-// mixed one gets per-CTA item ranges balanced on the host (longest item onto
-// the least-loaded CTA).  Each model's K split count is its context's own
+// The FP64 contraction takes items from an atomic counter in list order; for
+// the mixed one the batch times one pass with each of two schedules of the
+// same list (a persistent round robin, one CTA per item) and keeps the faster.  Each model's K split count is its context's own
 // (kls_autotune chooses it), so a determinant from the batch is bitwise the
 // one kls_det_batch returns for the same context.
 #include "kls_internal.cuh"
@@ -24,7 +24,6 @@
 #include <cstring>
 #include <functional>
 #include <numeric>
-#include <queue>
 #include <vector>
 
 struct kls_multi {
@@ -35,7 +34,10 @@ struct kls_multi {
 
   std::vector<kls_mdesc> md;
   std::vector<kls_item> items;
+  std::vector<kls_item> list;       // mixed: items in locality order
   std::vector<int> starts;          // mixed: per-CTA item ranges
+  int schedule = 0;                 // mixed: 0 persistent round robin, 1 one CTA per item
+  double schedule_ms[2] = {0, 0};   // mixed: eager-pass time of each schedule
   std::vector<int2> pairs;          // (model, omega) pairs
   int grid = 0, max_Na = 0;
   int64_t max_K_pad = 0;
@@ -97,70 +99,82 @@ int malloc_buf(kls_multi* m, T** p, size_t count) {
 // mixed items: effective K splits so that every split owns >= 1 k-block
 constexpr int MIX_BK = 64, MIX_BM = 128, MIX_AB = 64;
 
+// Item order follows the one-model grids (tile fastest, then split, then
+// omega), model after model with the largest models first: CTAs that run at
+// the same time then work on the same k-range of one table, so its X and Y
+// rows are read from DRAM once and reused from L2, as in the one-model launch.
 int build_items(kls_multi* m) {
   m->items.clear();
   m->pairs.clear();
   for (int i = 0; i < m->n_models; ++i)
     for (int z = 0; z < m->batch; ++z) m->pairs.push_back(make_int2(i, z));
+  std::vector<int> order(m->n_models);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const kls_mdesc &x = m->md[a], &y = m->md[b];
+    return (double)x.K_pad * x.Na_pad * x.Na_pad > (double)y.K_pad * y.Na_pad * y.Na_pad;
+  });
   if (m->mode == KLS_MODE_FP64) {
-    for (int i = 0; i < m->n_models; ++i) {
+    for (int i : order) {
       const kls_mdesc& d = m->md[i];
       const int tiles = (d.Na_pad / KLS_TILE) * (d.Na_pad / KLS_TILE);
       for (int z = 0; z < m->batch; ++z)
-        for (int t = 0; t < tiles; ++t)
-          for (int s = 0; s < d.splits; ++s) {
+        for (int s = 0; s < d.splits; ++s)
+          for (int t = 0; t < tiles; ++t) {
             int64_t kb = (int64_t)s * d.k_per_split;
             int64_t ke = std::min(d.K_pad, kb + d.k_per_split);
             m->items.push_back(kls_item{i, z, t, s, 1, 0, (int)std::max<int64_t>(0, ke - kb), 0});
           }
     }
-    // longest first; ties keep (model, omega, tile, split) order
-    std::stable_sort(m->items.begin(), m->items.end(),
-                     [](const kls_item& a, const kls_item& b) { return a.nkb > b.nkb; });
     m->grid = std::max(1, std::min((int)m->items.size(), kls_multi_contract_slots(m->device)));
     return KLS_OK;
   }
-  std::vector<int64_t> cost;
-  for (int i = 0; i < m->n_models; ++i) {
+  m->list.clear();
+  for (int i : order) {
     const kls_mdesc& d = m->md[i];
     const int tiles = (2 * d.Na_pad / MIX_BM) * (d.Na_pad / MIX_AB);
     for (int z = 0; z < m->batch; z += d.om_per_item) {
       const int n_om = std::min(d.om_per_item, m->batch - z);
-      for (int t = 0; t < tiles; ++t)
-        for (int s = 0; s < d.msplits; ++s) {
+      for (int s = 0; s < d.msplits; ++s)
+        for (int t = 0; t < tiles; ++t) {
           const int kb0 = s * d.kb_per_split;
           const int nkb = std::min(d.nkb_total, kb0 + d.kb_per_split) - kb0;
           if (nkb <= 0) continue;
-          m->items.push_back(kls_item{i, z, t, s, n_om, kb0, nkb, 0});
+          m->list.push_back(kls_item{i, z, t, s, n_om, kb0, nkb, 0});
         }
     }
   }
-  const int n = (int)m->items.size();
-  const int grid = std::max(1, std::min(n, kls_mixed_slots(m->device)));
-  // greedy LPT: cost ~ k-blocks x (X tile + n_om Y tiles)
-  std::vector<int> order(n);
-  std::iota(order.begin(), order.end(), 0);
-  auto c_of = [&](int k) { return (int64_t)m->items[k].nkb * (2 + m->items[k].n_om); };
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return c_of(a) > c_of(b); });
-  typedef std::pair<int64_t, int> Load;
-  std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-  for (int b = 0; b < grid; ++b) heap.push(Load(0, b));
-  std::vector<std::vector<int>> per(grid);
-  for (int k : order) {
-    Load l = heap.top();
-    heap.pop();
-    per[l.second].push_back(k);
-    heap.push(Load(l.first + c_of(k), l.second));
+  return KLS_OK;
+}
+
+// Mixed form: per-CTA item ranges of the ordered list.  Schedule 0: a
+// persistent grid of one CTA per SM, CTA b taking items b, b + grid, ...;
+// schedule 1: one CTA per item (the hardware block scheduler hands items to
+// SMs as they free up, in list order).
+int schedule_items(kls_multi* m, int policy) {
+  const int n = (int)m->list.size();
+  m->items.clear();
+  if (policy == 0) {
+    const int grid = std::max(1, std::min(n, kls_mixed_slots(m->device)));
+    m->starts.assign(grid + 1, 0);
+    for (int b = 0; b < grid; ++b) {
+      m->starts[b] = (int)m->items.size();
+      for (int k = b; k < n; k += grid) m->items.push_back(m->list[k]);
+    }
+    m->starts[grid] = (int)m->items.size();
+    m->grid = grid;
+  } else {
+    m->items = m->list;
+    m->starts.resize(n + 1);
+    std::iota(m->starts.begin(), m->starts.end(), 0);
+    m->grid = std::max(1, n);
   }
-  std::vector<kls_item> flat;
-  m->starts.assign(grid + 1, 0);
-  for (int b = 0; b < grid; ++b) {
-    m->starts[b] = (int)flat.size();
-    for (int k : per[b]) flat.push_back(m->items[k]);
-  }
-  m->starts[grid] = (int)flat.size();
-  m->items.swap(flat);
-  m->grid = grid;
+  m->schedule = policy;
+  if (cudaMemcpy(m->d_items, m->items.data(), m->items.size() * sizeof(kls_item),
+                 cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(m->d_starts, m->starts.data(), m->starts.size() * sizeof(int),
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    return mcuda(m, cudaGetLastError(), "cudaMemcpy (schedule)");
   return KLS_OK;
 }
 
@@ -183,11 +197,10 @@ int launch_batch(kls_multi* m) {
   return KLS_OK;
 }
 
-// H2D omegas, the batch, D2H results: recorded once into a graph
-int capture(kls_multi* m) {
+// One eager pass (kernel attributes are set outside any capture and the
+// launch shapes are checked); *ms = its device time.
+int eager_pass(kls_multi* m, float* ms) {
   const size_t nz = (size_t)m->n_models * m->batch;
-  // one eager pass first: kernel attributes are set outside the capture and
-  // the launch shapes are checked before they are recorded
   for (int i = 0; i < m->n_models; ++i)
     for (int z = 0; z < m->batch; ++z) {
       m->h_omega[2 * ((size_t)i * m->batch + z)] = m->ctx[i]->cfg.m * 0.4;
@@ -195,13 +208,23 @@ int capture(kls_multi* m) {
     }
   KM_CK(m, cudaMemcpyAsync(m->d_omega, m->h_omega, nz * 2 * sizeof(double),
                            cudaMemcpyHostToDevice, m->stream));
+  KM_CK(m, cudaEventRecord(m->ev0, m->stream));
   int r = launch_batch(m);
   if (r) return r;
+  KM_CK(m, cudaEventRecord(m->ev1, m->stream));
   KM_CK(m, cudaMemcpyAsync(m->h_err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
   KM_CK(m, cudaStreamSynchronize(m->stream));
   if (*m->h_err)
     return mfail(m, KLS_ERR_CUDA,
                  "mixed contraction pipeline timed out (code " + std::to_string(*m->h_err) + ")");
+  if (ms) KM_CK(m, cudaEventElapsedTime(ms, m->ev0, m->ev1));
+  return KLS_OK;
+}
+
+// H2D omegas, the batch, D2H results: recorded once into a graph
+int capture(kls_multi* m) {
+  const size_t nz = (size_t)m->n_models * m->batch;
+  int r = KLS_OK;
   KM_CK(m, cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaMemcpyAsync(m->d_omega, m->h_omega, nz * 2 * sizeof(double),
                                   cudaMemcpyHostToDevice, m->stream);
@@ -305,6 +328,9 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
       return mfail(nullptr, KLS_ERR_STATE, "model " + std::to_string(i) + " is not precomputed");
     if (models[i]->device != models[0]->device)
       return mfail(nullptr, KLS_ERR_CONFIG, "all models of a batch must be on one device");
+    if (mode == KLS_MODE_FP64 && !models[i]->d_Wre)
+      return mfail(nullptr, KLS_ERR_STATE,
+                   "model " + std::to_string(i) + ": the FP64 table was released");
   }
   kls_multi* m = new kls_multi();
   m->device = models[0]->device;
@@ -394,19 +420,30 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
     m->max_K_pad = std::max(m->max_K_pad, c->K_pad);
   }
   if ((r = build_items(m))) return bail(r);
-  if ((r = malloc_buf(m, &m->d_md, m->md.size())) ||
-      (r = malloc_buf(m, &m->d_items, m->items.size())) ||
+  const size_t n_it = std::max(m->items.size(), m->list.size());
+  if ((r = malloc_buf(m, &m->d_md, m->md.size())) || (r = malloc_buf(m, &m->d_items, n_it)) ||
       (r = malloc_buf(m, &m->d_pairs, m->pairs.size())) ||
-      (r = malloc_buf(m, &m->d_starts, std::max<size_t>(m->starts.size(), 1))))
+      (r = malloc_buf(m, &m->d_starts, n_it + 1)))
     return bail(r);
   if (cudaMemcpy(m->d_md, m->md.data(), m->md.size() * sizeof(kls_mdesc), cudaMemcpyHostToDevice) ||
-      cudaMemcpy(m->d_items, m->items.data(), m->items.size() * sizeof(kls_item),
-                 cudaMemcpyHostToDevice) ||
       cudaMemcpy(m->d_pairs, m->pairs.data(), m->pairs.size() * sizeof(int2),
-                 cudaMemcpyHostToDevice) ||
-      (!m->starts.empty() && cudaMemcpy(m->d_starts, m->starts.data(),
-                                        m->starts.size() * sizeof(int), cudaMemcpyHostToDevice)))
+                 cudaMemcpyHostToDevice))
     return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (descriptors)"));
+  if (mode == KLS_MODE_FP64) {
+    if (cudaMemcpy(m->d_items, m->items.data(), m->items.size() * sizeof(kls_item),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (items)"));
+    if ((r = eager_pass(m, nullptr))) return bail(r);
+  } else {
+    // schedule tuning: one warm-up pass, then one timed pass per schedule
+    if ((r = schedule_items(m, 0)) || (r = eager_pass(m, nullptr))) return bail(r);
+    for (int p = 0; p < 2; ++p) {
+      float ms = 0.f;
+      if ((r = schedule_items(m, p)) || (r = eager_pass(m, &ms))) return bail(r);
+      m->schedule_ms[p] = ms;
+    }
+    if ((r = schedule_items(m, m->schedule_ms[1] < m->schedule_ms[0] ? 1 : 0))) return bail(r);
+  }
   if ((r = capture(m))) return bail(r);
   *out = m;
   return KLS_OK;
@@ -480,6 +517,9 @@ int kls_multi_get_info(const kls_multi* m, kls_multi_info* out) {
   out->last_ms = m->last_ms;
   // kernels per replay: weights (+ FP32 copy), contraction, reduction, LU
   out->launches_per_replay = m->mode == KLS_MODE_FP64 ? 4 : 5;
+  out->schedule = m->schedule;
+  out->schedule_ms[0] = m->schedule_ms[0];
+  out->schedule_ms[1] = m->schedule_ms[1];
   return KLS_OK;
 }
 

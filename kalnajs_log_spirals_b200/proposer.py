@@ -120,40 +120,60 @@ class ModelSpec:
     n_zang: int
     q1: float
     m: int
+    size: Optional[Tuple[int, int, int, int]] = None    # (NR, Ne, N_alpha, l_max)
 
 
-def random_models(n: int, seed: int) -> List[ModelSpec]:
-    """n_zang in {2..6}, q1 ~ U[4, 12] (real), m in {2, 3}."""
+# the three disk-model sizes of the uneven batched scan
+SIZES = ((101, 21, 101, 25), (301, 31, 201, 60), (501, 51, 301, 100))
+
+
+def random_models(n: int, seed: int, sizes: Optional[Sequence[Tuple[int, int, int, int]]] = None
+                  ) -> List[ModelSpec]:
+    """n_zang in {2..6}, q1 ~ U[4, 12] (real), m in {2, 3}; size drawn from
+    `sizes` when given (else the base configuration's)."""
     rng = np.random.default_rng(seed)
-    return [ModelSpec(int(rng.integers(2, 7)), float(rng.uniform(4.0, 12.0)), int(rng.integers(2, 4)))
-            for _ in range(n)]
+    out = []
+    for _ in range(n):
+        nz, q1, m = int(rng.integers(2, 7)), float(rng.uniform(4.0, 12.0)), int(rng.integers(2, 4))
+        size = tuple(sizes[int(rng.integers(0, len(sizes)))]) if sizes else None
+        out.append(ModelSpec(nz, q1, m, size))
+    return out
 
 
 def model_config(base: KalnajsConfig, spec: ModelSpec) -> KalnajsConfig:
     c = copy_config(base)
     c.model.n_zang, c.model.q1, c.physics.m = spec.n_zang, spec.q1, spec.m
+    if spec.size is not None:
+        NR, Ne, Na, lmax = spec.size
+        c.grid.NR, c.grid.Ne, c.grid.N_alpha = NR, Ne, Na
+        c.grid.l_min, c.grid.l_max = -lmax, lmax
     return c
 
 
 def scan_samples(base: KalnajsConfig, specs: Sequence[ModelSpec], n_Op: int, n_gamma: int,
                  Op_range=(0.2, 0.8), g_range=(0.01, 0.30), mixed: bool = True,
-                 device: int = 0):
-    """Batched scans: features and targets of every (model, omega) grid point."""
+                 device: int = 0, batch: int = 16):
+    """Features and targets of every (model, omega) point of one batched scan
+    over all models (api.ModelBatch: every pass is one persistent launch over
+    the uneven batch)."""
     from . import api
+    pcs = [api.precompute_all(model_config(base, s), device=device) for s in specs]
+    try:
+        mb = api.ModelBatch(pcs, "Float32" if mixed else "Float64", batch=batch)
+        d, la, _, _ = mb.scan(n_Op, n_gamma, Op_range, g_range)   # [n_models, n_gamma, n_Op]
+        mb.close()
+    finally:
+        for pc in pcs:
+            pc.close()
     Op = np.linspace(*Op_range, n_Op)
     gm = np.linspace(*g_range, n_gamma)
-    OP, GM = np.meshgrid(Op, gm, indexing="xy")
+    OP, GM = np.meshgrid(Op, gm, indexing="xy")                   # [n_gamma, n_Op]
     Xs, Ts = [], []
-    for spec in specs:
-        cfg = model_config(base, spec)
-        pc = api.precompute_all(cfg, device=device)
-        dev = api.to_device(pc, api.GPUType.NVIDIA, "Float32" if mixed else "Float64")
-        om = spec.m * OP.ravel() + 1j * GM.ravel()
-        d, la = api.compute_determinant_batched(om, pc, dev, batch_size=64, log_abs=True)
-        pc.close()
-        ok = np.isfinite(la) & np.isfinite(d)
+    for i, spec in enumerate(specs):
+        di, li = d[i].ravel(), la[i].ravel()
+        ok = np.isfinite(li) & np.isfinite(di)
         Xs.append(features(spec.n_zang, spec.q1, spec.m, OP.ravel()[ok], GM.ravel()[ok]))
-        Ts.append(targets(d[ok], la[ok]))
+        Ts.append(targets(di[ok], li[ok]))
     return np.concatenate(Xs), np.concatenate(Ts)
 
 

@@ -58,7 +58,9 @@ def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu):
         assert np.array_equal(d[i], ds), (i, np.max(np.abs(d[i] - ds) / np.abs(ds)))
         assert np.array_equal(la[i], ls), i
     assert info["graph"] == 1 and info["replays"] == 3 and info["n_models"] == len(MODELS)
-    assert info["launches_per_replay"] >= 4 and info["n_items"] > info["grid"] > 0
+    assert info["launches_per_replay"] >= 4 and info["n_items"] >= info["grid"] > 0
+    if Tgpu == "Float32":
+        assert info["schedule"] in (0, 1) and min(info["schedule_ms"]) > 0
 
 
 def test_mixed_batch_close_to_fp64_batch(pcs):
@@ -118,3 +120,23 @@ def test_multi_rejects_bad_input(pcs):
     with pytest.raises(K.KlsError):
         mb.det(np.array([[np.nan + 0j, 1.0 + 0.1j]]))
     mb.close()
+
+
+def test_release_fp64_keeps_mixed(lib_path):
+    c = configs()[1]
+    pc = K.precompute_all(c)
+    dev = K.to_device(pc, K.GPUType.NVIDIA, "Float32")
+    om = omegas(3, 8) * 1.5
+    before = K.compute_determinant_batched(om, pc, dev)
+    K.release_fp64(pc)
+    after = K.compute_determinant_batched(om, pc, dev)
+    assert np.array_equal(before, after)
+    with pytest.raises(K.KlsError):
+        K.compute_determinant_batched(om, pc, None)
+    with pytest.raises(K.KlsError):
+        K.ModelBatch([pc], "Float64", batch=2)
+    mb = K.ModelBatch([pc], "Float32", batch=3)
+    d, _ = mb.det(om[None, :])
+    mb.close()
+    assert np.array_equal(d[0], after)
+    pc.close()
