@@ -11,7 +11,7 @@ from .config import (CPUConfig, GPUConfig, GridConfig, IOConfig, KalnajsConfig, 
 from .api import (DevicePrecomputed, GPUType, NewtonResult, OrbitData, PrecomputedData,
                   ModelBatch, ToomreZangModel, TuneResult, autotune, build_M_matrix, compute_determinant,
                   compute_determinant_batched, create_toomre_zang_model, detect_gpu_type,
-                  find_minimum, grid_scan, newton_search, precompute_all, release_fp64,
+                  find_minimum, grid_scan, grid_scan_distributed, newton_search, precompute_all, release_fp64,
                   to_device)
 from ._lib import KLS_MODE_FP64, KLS_MODE_MIXED, KlsError
 
@@ -23,5 +23,5 @@ __all__ = [
     "create_toomre_zang_model", "PrecomputedData", "OrbitData", "precompute_all",
     "DevicePrecomputed", "to_device", "compute_determinant", "compute_determinant_batched",
     "build_M_matrix", "grid_scan", "find_minimum", "newton_search", "NewtonResult", "KlsError",
-    "KLS_MODE_FP64", "KLS_MODE_MIXED", "ModelBatch", "autotune", "TuneResult", "release_fp64",
+    "KLS_MODE_FP64", "KLS_MODE_MIXED", "ModelBatch", "autotune", "TuneResult", "release_fp64", "grid_scan_distributed",
 ]

@@ -439,6 +439,48 @@ def grid_scan(config: KalnajsConfig, precomputed: PrecomputedData,
     return det_grid, Op0, g0
 
 
+def grid_scan_distributed(config: KalnajsConfig, precomputed: Optional[PrecomputedData] = None,
+                          devprecomp: Optional[DevicePrecomputed] = None, group=None,
+                          column_fn=None):
+    """grid_scan with one process per GPU (torch.distributed, e.g. under torchrun).
+
+    Rank r of W evaluates the Omega_p columns ``column_ranges(n_Op, W)[r]``
+    (the column split of scan_multi_gpu!, GridScan.jl:133-144) on its own
+    replica of the precompute; one all_gather of the det blocks (16 B per
+    determinant) gives every rank the same (det_grid, Omega_p_init,
+    gamma_init) that grid_scan returns.  ``column_fn(Op_cols, gamma_grid, m)``
+    evaluates one [n_gamma, n_cols] block; by default this rank's
+    ``precomputed`` on its GPU.
+    """
+    import torch
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    s = config.scan
+    m = int(config.physics.m)
+    Op_grid = _linspace(s.Omega_p_min, s.Omega_p_max, s.n_Op)
+    g_grid = _linspace(s.gamma_min, s.gamma_max, s.n_gamma)
+    ranges = column_ranges(s.n_Op, world)
+    cols = ranges[rank]
+    if column_fn is None:
+        mode = _mode(devprecomp)
+        column_fn = lambda Opc, gg, mm: _scan_columns(precomputed, mode, Opc, gg, mm)
+    block = np.asarray(column_fn(Op_grid[cols], g_grid, m), dtype=np.complex128)
+    width = max(r.stop - r.start for r in ranges)
+    dev = torch.device("cuda", torch.cuda.current_device()) \
+        if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    buf = torch.zeros((s.n_gamma, width, 2), dtype=torch.float64, device=dev)
+    if block.size:
+        buf[:, :block.shape[1]] = torch.view_as_real(torch.from_numpy(block)).to(dev)
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    det_grid = np.empty((s.n_gamma, s.n_Op), dtype=np.complex128)
+    for r, part in zip(ranges, parts):
+        p = part.cpu().numpy()
+        det_grid[:, r] = p[:, :r.stop - r.start, 0] + 1j * p[:, :r.stop - r.start, 1]
+    Op0, g0 = find_minimum(det_grid, Op_grid, g_grid)
+    return det_grid, Op0, g0
+
+
 def column_ranges(n_Op: int, n_gpus: int) -> List[slice]:
     """Contiguous column blocks, the first n_Op % n_gpus one wider (GridScan.jl:133-144)."""
     per, rem = divmod(n_Op, n_gpus)
