@@ -62,6 +62,8 @@ def parse():
                     help="time the whole FP64 41x20 scan instead of two of its columns")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the 16-model uneven batched scan block")
+    ap.add_argument("--no-refgpu", action="store_true",
+                    help="skip the reference GPU algorithm (cuBLAS ZGEMM per harmonic) arm")
     ap.add_argument("--uneven-passes", type=int, default=3)
     ap.add_argument("--uneven-batch", type=int, default=4)
     return ap.parse_args()
@@ -221,6 +223,47 @@ def omegas_for_step(step: int, rank: int, m: int, Op: float, g: float, delta: fl
     Op_s = Op + 1e-4 * ((step * 7 + rank * 131) % 97) / 97.0
     g_s = g + 1e-4 * ((step * 13 + rank * 71) % 89) / 89.0
     return [complex(m * Op_s, g_s), complex(m * (Op_s + delta), g_s), complex(m * Op_s, g_s + delta)]
+
+
+# ---------------------------------------------------------------------------
+# the reference's GPU algorithm on this B200 (NL_julia_direct_gpu.jl:277-288,
+# MatrixBuilder.jl:100-185): per harmonic l a weighted copy w .* conj(W_l) and
+# one ZGEMM W_l^T (.) (cuBLAS through torch), then M to the host and LAPACK det
+# ---------------------------------------------------------------------------
+def reference_algorithm_gpu(torch, NPh: int, Na: int, n_l: int, reps: int = 2):
+    import numpy as np
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    # synthetic table in the reference layout [n_l][NPh][N_alpha] (the cost
+    # does not depend on the values)
+    W = torch.empty((n_l, NPh, Na), dtype=torch.complex128, device="cuda")
+    for l in range(n_l):
+        W[l].real.normal_(generator=g)
+        W[l].imag.normal_(generator=g)
+    Ores = (torch.rand((n_l, NPh), dtype=torch.float64, device="cuda", generator=g) - 0.5) * 6
+    Gk = torch.randn((n_l, NPh), dtype=torch.float64, device="cuda", generator=g)
+    eye = np.eye(Na)
+
+    def one(omega):
+        M = torch.zeros((Na, Na), dtype=torch.complex128, device="cuda")
+        for l in range(n_l):
+            den = omega - Ores[l]
+            den = torch.where(den.abs() < 1e-12, torch.full_like(den, 1e-12 + 1e-12j), den)
+            M += W[l].transpose(0, 1) @ ((Gk[l] / den)[:, None] * W[l].conj())
+        return np.linalg.det(eye - M.cpu().numpy() * 1e-3)
+
+    one(0.88 + 0.12j)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in range(reps):
+        one(0.88 + 0.12j + 1e-3 * r)
+    t = (time.perf_counter() - t0) / reps
+    del W
+    torch.cuda.empty_cache()
+    return {"det_evals_per_s": 1.0 / t, "s_per_det": t,
+            "form": "per-harmonic weighted copy + cuBLAS ZGEMM (torch.matmul complex128), "
+                    "M to the host, numpy LAPACK det; synthetic table of the default size",
+            "reps": reps}
 
 
 # ---------------------------------------------------------------------------
@@ -579,6 +622,9 @@ def ours(args):
                 "abs_dgamma_vs_plain": abs(rh.gamma - r.gamma)}
             newton["speedup_hybrid_vs_plain"] = t_plain / t_h
 
+    refgpu = None
+    if world == 1 and not args.no_refgpu:
+        refgpu = reference_algorithm_gpu(torch, dims.NPh, dims.N_alpha, dims.n_l)
     # the two workflow blocks run at N = 1 only (the scaling run times the
     # headline step alone)
     ttr = None
@@ -627,6 +673,7 @@ def ours(args):
         "precompute_s": t_pre,
         "mixed": mixed,
         "newton": newton,
+        "reference_algorithm_gpu": refgpu,
         "time_to_root": ttr,
         "uneven_batch": uneven,
     }
