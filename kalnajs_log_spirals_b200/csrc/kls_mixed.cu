@@ -289,16 +289,16 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
     s_abort = 0;
     for (int s = 0; s < MX_STAGES; ++s) {
       mbar_init(smem_u32(&bar_full_x[s]), 1);
-      mbar_init(smem_u32(&bar_full_y[s]), MX_PRODUCERS);
+      mbar_init(smem_u32(&bar_full_y[s]), MX_PRODUCERS / 32);
       mbar_init(smem_u32(&bar_empty[s]), 1);
     }
     for (int s = 0; s < MX_WSTAGES; ++s) {
       mbar_init(smem_u32(&bar_w_full[s]), 1);
-      mbar_init(smem_u32(&bar_w_empty[s]), MX_PRODUCERS);
+      mbar_init(smem_u32(&bar_w_empty[s]), MX_PRODUCERS / 32);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&bar_acc_full[b]), 1);
-      mbar_init(smem_u32(&bar_acc_empty[b]), 128);
+      mbar_init(smem_u32(&bar_acc_empty[b]), 4);
     }
     mbar_init(smem_u32(&bar_done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -415,9 +415,14 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
     if (nkb > 0) prefetch(0);
     for (int i = 0; i < nkb; ++i) {
       const int s = i % MX_STAGES, r = i / MX_STAGES;
-      if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)) break;
+      // warp-uniform outcomes: a warp leaves the loop as a whole
+      if (!__all_sync(0xffffffffu,
+                      mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)))
+        break;
       const int ws = i % MX_WSTAGES;
-      if (!mbar_wait(smem_u32(&bar_w_full[ws]), (i / MX_WSTAGES) & 1, &s_abort, err, 8)) break;
+      if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&bar_w_full[ws]), (i / MX_WSTAGES) & 1,
+                                             &s_abort, err, 8)))
+        break;
       // W of both units in FP32 (hi + lo is exact in FP32)
       float wr[2][8], wi[2][8];
 #pragma unroll
@@ -470,9 +475,14 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
           *reinterpret_cast<uint4*>(yl_s(s, j) + offi) = make_uint4(il[0], il[1], il[2], il[3]);
         }
       }
-      mbar_arrive(smem_u32(&bar_w_empty[ws]));      // weights slot read
+      // one arrival per warp (weights slot read, Y tiles written): 256
+      // same-address arrivals per stage would serialise on the shared port
       fence_proxy_async();
-      mbar_arrive(smem_u32(&bar_full_y[s]));
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(smem_u32(&bar_w_empty[ws]));
+        mbar_arrive(smem_u32(&bar_full_y[s]));
+      }
       if (i + 1 < nkb) prefetch(i + 1);
     }
   } else if (warp >= MX_DRAIN0) {
@@ -519,7 +529,8 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
         }
       }
       tc_fence_before();
-      if (nkb > 0) mbar_arrive(smem_u32(&bar_acc_empty[b]));
+      __syncwarp();
+      if (nkb > 0 && lane == 0) mbar_arrive(smem_u32(&bar_acc_empty[b]));
     }
   }
   __syncwarp();
@@ -643,16 +654,16 @@ mixed_multi_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict_
     s_abort = 0;
     for (int s = 0; s < MX_STAGES; ++s) {
       mbar_init(smem_u32(&bar_full_x[s]), 1);
-      mbar_init(smem_u32(&bar_full_y[s]), MX_PRODUCERS);
+      mbar_init(smem_u32(&bar_full_y[s]), MX_PRODUCERS / 32);
       mbar_init(smem_u32(&bar_empty[s]), 1);
     }
     for (int s = 0; s < MX_WSTAGES; ++s) {
       mbar_init(smem_u32(&bar_w_full[s]), 1);
-      mbar_init(smem_u32(&bar_w_empty[s]), MX_PRODUCERS);
+      mbar_init(smem_u32(&bar_w_empty[s]), MX_PRODUCERS / 32);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(smem_u32(&bar_acc_full[b]), 1);
-      mbar_init(smem_u32(&bar_acc_empty[b]), 128);
+      mbar_init(smem_u32(&bar_acc_empty[b]), 4);
     }
     mbar_init(smem_u32(&bar_done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -805,12 +816,14 @@ mixed_multi_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict_
       prefetch(0);
       for (int i = 0; i < it.nkb; ++i) {
         const int s = g % MX_STAGES, r = g / MX_STAGES;
-        if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4)) {
+        if (!__all_sync(0xffffffffu,
+                        mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 4))) {
           ok = false;
           break;
         }
         const int ws = g % MX_WSTAGES;
-        if (!mbar_wait(smem_u32(&bar_w_full[ws]), (g / MX_WSTAGES) & 1, &s_abort, err, 8)) {
+        if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&bar_w_full[ws]), (g / MX_WSTAGES) & 1,
+                                               &s_abort, err, 8))) {
           ok = false;
           break;
         }
@@ -860,9 +873,12 @@ mixed_multi_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict_
             *reinterpret_cast<uint4*>(yl_s(s, j) + offi) = make_uint4(il[0], il[1], il[2], il[3]);
           }
         }
-        mbar_arrive(smem_u32(&bar_w_empty[ws]));
         fence_proxy_async();
-        mbar_arrive(smem_u32(&bar_full_y[s]));
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(smem_u32(&bar_w_empty[ws]));
+          mbar_arrive(smem_u32(&bar_full_y[s]));
+        }
         ++g;
         if (i + 1 < it.nkb) prefetch(i + 1);
       }
@@ -915,7 +931,8 @@ mixed_multi_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict_
           }
         }
         tc_fence_before();
-        mbar_arrive(smem_u32(&bar_acc_empty[b]));
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&bar_acc_empty[b]));
       }
       gch += (uint32_t)nch;
     }
