@@ -289,6 +289,19 @@ typedef struct kls_tune_result {
 } kls_tune_result;
 int kls_autotune(kls_ctx* ctx, int mode, int batch, kls_tune_result* out);
 
+/* ---- determinant stage form (no reference counterpart) -------------------- *
+ * KLS_LU_CLUSTER factors each I - M(omega) on one thread-block cluster of 8
+ * (or 16) CTAs with the matrix held in their shared memory (latency: one
+ * matrix per cluster); KLS_LU_CTA uses one CTA per matrix through L2
+ * (throughput for many matrices).  KLS_LU_AUTO (default) takes the cluster
+ * form when N_alpha >= 128 and the batch fits one wave of clusters.  Both
+ * forms return bitwise the same determinants.  KLS_LU_CLUSTER fails with
+ * KLS_ERR_UNSUPPORTED when N_alpha is too large for it.                      */
+#define KLS_LU_AUTO          0
+#define KLS_LU_CTA           1
+#define KLS_LU_CLUSTER       2
+int kls_set_lu_mode(kls_ctx* ctx, int mode);
+
 /* ---- instrumentation ----------------------------------------------------- */
 /* Per-stage device time (ms) of the last det batch when timing is enabled:
  * [0] weights, [1] contraction, [2] reduce/epilogue, [3] LU.               */

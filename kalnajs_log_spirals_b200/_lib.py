@@ -23,6 +23,10 @@ KLS_ERR_UNSUPPORTED = 7
 KLS_MODE_FP64 = 0
 KLS_MODE_MIXED = 1
 
+KLS_LU_AUTO = 0
+KLS_LU_CTA = 1
+KLS_LU_CLUSTER = 2
+
 STATUS_NAMES = {0: "KLS_OK", 1: "KLS_ERR_CONFIG", 2: "KLS_ERR_CUDA", 3: "KLS_ERR_OOM",
                 4: "KLS_ERR_STATE", 5: "KLS_ERR_NONFINITE", 6: "KLS_ERR_SINGULAR",
                 7: "KLS_ERR_UNSUPPORTED"}
@@ -131,6 +135,7 @@ SIGNATURES = {
     "kls_scan_multi": (C.c_int, [_P, C.POINTER(kls_scan_cfg), _D, _D, _D, _D]),
     "kls_multi_get_info": (C.c_int, [_P, C.POINTER(kls_multi_info)]),
     "kls_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(kls_tune_result)]),
+    "kls_set_lu_mode": (C.c_int, [_P, C.c_int]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_launch_count": (C.c_int64, [_P]),

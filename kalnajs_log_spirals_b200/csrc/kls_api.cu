@@ -797,6 +797,14 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
   return KLS_OK;
 }
 
+int kls_set_lu_mode(kls_ctx* c, int mode) {
+  if (!c) return KLS_ERR_CONFIG;
+  if (mode != KLS_LU_AUTO && mode != KLS_LU_CTA && mode != KLS_LU_CLUSTER)
+    return kls_fail(c, KLS_ERR_CONFIG, "unknown LU mode");
+  c->lu_mode = mode;
+  return KLS_OK;
+}
+
 int kls_enable_timing(kls_ctx* c, int on) {
   if (!c) return KLS_ERR_CONFIG;
   c->timing = on != 0;

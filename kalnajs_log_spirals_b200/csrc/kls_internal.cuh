@@ -105,6 +105,11 @@ struct kls_ctx {
 
   kls_mixed* mixed = nullptr;
 
+  // determinant stage: KLS_LU_* form and the cluster size it uses (-1: not
+  // chosen yet, 0: the cluster form does not fit)
+  int lu_mode = 0;
+  int lu_cluster = -1;
+
   // instrumentation
   int64_t launches = 0;
   bool timing = false;
