@@ -218,6 +218,35 @@ def read_traffic(name: str):
     return None
 
 
+def precompute_roofline(cfg, dims, pre_ms, peak64: float, peaks: dict):
+    """Orbit integration and W_l quadrature kernels against the FP64 and HBM
+    peaks (CUDA-event times of the precompute in this run)."""
+    NPh, Na, n_l, nwa, nw = dims.NPh, dims.N_alpha, dims.n_l, dims.nwa, cfg.grid.nw
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_note = "of measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else \
+        "of fallback (6.65 TB/s)"
+    t_orb, t_wl = pre_ms[0] * 1e-3, pre_ms[1] * 1e-3
+    out = {}
+    if t_orb > 0:
+        orb_bytes = 3.0 * nwa * NPh * 8 + 17.0 * NPh * 8 + 2.0 * nw * 8
+        out["orbit_kernel"] = {
+            "ms": pre_ms[0], "point_evaluations_per_s": 2.0 * nw * NPh / t_orb,
+            "algorithmic_bytes": orb_bytes, "hbm_gbs": orb_bytes / t_orb / 1e9,
+            "hbm_frac": orb_bytes / t_orb / 1e9 / hbm, "hbm_peak_note": hbm_note,
+            "bound": "FP64 + transcendentals (2 nw point evaluations per orbit)"}
+    if t_wl > 0:
+        wl_bytes = float(NPh) * Na * n_l * 16 + 3.0 * nwa * NPh * 8
+        wl_flops = 4.0 * n_l * nwa * Na * NPh
+        out["wl_kernel"] = {
+            "ms": pre_ms[1], "algorithmic_bytes": wl_bytes, "hbm_gbs": wl_bytes / t_wl / 1e9,
+            "hbm_frac": wl_bytes / t_wl / 1e9 / hbm, "hbm_peak_note": hbm_note,
+            "algorithmic_flops": wl_flops, "tflops": wl_flops / t_wl / 1e12,
+            "fp64_frac": wl_flops / t_wl / 1e12 / peak64,
+            "fp64_peak_note": "of measured: cuBLAS DGEMM in this run",
+            "bound": "FP64 tensor pipe (DMMA); output 16 B per table entry"}
+    return out
+
+
 def omegas_for_step(step: int, rank: int, m: int, Op: float, g: float, delta: float):
     # a Newton FD triple around a point that moves with the step (distinct omegas)
     Op_s = Op + 1e-4 * ((step * 7 + rank * 131) % 97) / 97.0
@@ -462,10 +491,15 @@ def ours(args):
         else "of fallback (1.59 PFLOP/s)"
 
     t0 = time.perf_counter()
-    pc = K.precompute_all(cfg, device=local)
+    pc = K.api.PrecomputedData(cfg, K.create_toomre_zang_model(cfg), local)
+    lib, h = pc.ctx.lib, pc.ctx.h
+    _lib.check(h, lib.kls_enable_timing(h, 1))
+    pc.ctx.call("kls_precompute")
+    _lib.check(h, lib.kls_enable_timing(h, 0))
     torch.cuda.synchronize()
     t_pre = time.perf_counter() - t0
-    lib, h = pc.ctx.lib, pc.ctx.h
+    pre_ms = (C.c_float * 2)()
+    _lib.check(h, lib.kls_get_precompute_ms(h, pre_ms))
     dims = pc.ctx.dims
     # a dedicated stream: the library launches on it and the events are
     # recorded on it (the legacy default stream has handle 0, which the
@@ -671,6 +705,7 @@ def ours(args):
         "gpu_launches": int(launches),
         "clocks": clk,
         "precompute_s": t_pre,
+        "precompute": precompute_roofline(cfg, dims, pre_ms, peak64, peaks),
         "mixed": mixed,
         "newton": newton,
         "reference_algorithm_gpu": refgpu,

@@ -307,6 +307,9 @@ int kls_set_lu_mode(kls_ctx* ctx, int mode);
  * [0] weights, [1] contraction, [2] reduce/epilogue, [3] LU.               */
 int kls_enable_timing(kls_ctx* ctx, int on);
 int kls_get_stage_ms(kls_ctx* ctx, float* ms4);
+/* Device time (ms) of the last kls_precompute's orbit_kernel [0] and
+ * wl_kernel [1] when timing was enabled before it.                         */
+int kls_get_precompute_ms(kls_ctx* ctx, float* ms2);
 /* Kernels launched by this context since creation (monotone counter).      */
 int64_t kls_launch_count(const kls_ctx* ctx);
 

@@ -138,6 +138,7 @@ SIGNATURES = {
     "kls_set_lu_mode": (C.c_int, [_P, C.c_int]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "kls_get_precompute_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_launch_count": (C.c_int64, [_P]),
 }
 

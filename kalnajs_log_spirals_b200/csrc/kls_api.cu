@@ -276,6 +276,7 @@ int kls_destroy(kls_ctx* c) {
                   c->d_det, c->d_logabs};
   for (void* p : ptrs) dfree(p);
   for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
+  for (auto& ev : c->pev) if (ev) cudaEventDestroy(ev);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
   return KLS_OK;
@@ -301,6 +302,10 @@ int kls_precompute(kls_ctx* c) {
   if ((r = kls_run_orbits(c))) return r;
   if ((r = kls_run_basis(c))) return r;
   KLS_CK(c, cudaStreamSynchronize(c->stream));
+  if (c->timing && c->pev[3]) {
+    KLS_CK(c, cudaEventElapsedTime(&c->pre_ms[0], c->pev[0], c->pev[1]));
+    KLS_CK(c, cudaEventElapsedTime(&c->pre_ms[1], c->pev[2], c->pev[3]));
+  }
   c->precomputed = true;
   return KLS_OK;
 }
@@ -808,6 +813,13 @@ int kls_set_lu_mode(kls_ctx* c, int mode) {
 int kls_enable_timing(kls_ctx* c, int on) {
   if (!c) return KLS_ERR_CONFIG;
   c->timing = on != 0;
+  return KLS_OK;
+}
+
+int kls_get_precompute_ms(kls_ctx* c, float* ms2) {
+  if (!c || !ms2) return KLS_ERR_CONFIG;
+  ms2[0] = c->pre_ms[0];
+  ms2[1] = c->pre_ms[1];
   return KLS_OK;
 }
 

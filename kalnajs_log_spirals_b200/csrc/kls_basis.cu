@@ -51,7 +51,12 @@ wl_kernel(WlParams P, const double* __restrict__ of, const int* __restrict__ val
   __shared__ double sC[WL_LB * WL_SC];
   __shared__ double sEr[WL_BK * WL_SE];
   __shared__ double sEi[WL_BK * WL_SE];
-  const int p = blockIdx.x, lb = blockIdx.y, ab = blockIdx.z;
+  // one orbit's (l block, alpha block) CTAs are consecutive in launch order,
+  // so its w1 / r / theta samples are read from DRAM once and then from L2
+  const int nlb = (P.n_l + WL_LB - 1) / WL_LB, nab = P.Na_pad / WL_AB;
+  const int p = (int)(blockIdx.x / (unsigned)(nlb * nab));
+  const int lb = (int)((blockIdx.x / (unsigned)nab) % (unsigned)nlb);
+  const int ab = (int)(blockIdx.x % (unsigned)nab);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int NPh = P.NPh, nwa = P.nwa;
   const double* w1 = w1g + (size_t)p * nwa;
@@ -255,9 +260,11 @@ int kls_run_basis(kls_ctx* c) {
   P.NPh = c->NPh; P.nwa = c->nwa; P.Na = c->Na; P.Na_pad = c->Na_pad; P.n_l = c->n_l;
   P.l_min = k.l_min; P.m = k.m;
   P.astep = c->Na > 1 ? (2.0 * k.alpha_max) / (double)(c->Na - 1) : 0.0;
-  dim3 grid(c->NPh, (c->n_l + WL_LB - 1) / WL_LB, c->Na_pad / WL_AB);
+  dim3 grid((unsigned)c->NPh * ((c->n_l + WL_LB - 1) / WL_LB) * (c->Na_pad / WL_AB));
+  kls_pre_mark(c, 2);
   wl_kernel<<<grid, WL_THREADS, 0, c->stream>>>(P, c->d_of, c->d_valid, c->d_w1, c->d_ra,
                                                 c->d_pha, c->d_alpha, c->d_Wre, c->d_Wim);
   KLS_LAUNCHED(c);
+  kls_pre_mark(c, 3);
   return KLS_OK;
 }

@@ -115,7 +115,17 @@ struct kls_ctx {
   bool timing = false;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   float stage_ms[4] = {0, 0, 0, 0};
+  // precompute kernels when timing is on: orbit_kernel, wl_kernel
+  cudaEvent_t pev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float pre_ms[2] = {0, 0};
 };
+
+// event pair around one precompute kernel (no-op unless c->timing)
+inline void kls_pre_mark(kls_ctx* c, int i) {
+  if (!c->timing) return;
+  if (!c->pev[i]) cudaEventCreate(&c->pev[i]);
+  cudaEventRecord(c->pev[i], c->stream);
+}
 
 // ---- helpers -------------------------------------------------------------
 int kls_fail(kls_ctx* c, int code, const std::string& msg);

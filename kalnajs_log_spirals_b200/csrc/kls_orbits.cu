@@ -318,10 +318,12 @@ int kls_run_orbits(kls_ctx* c) {
                             c->stream));
   KLS_CK(c, cudaMemcpyAsync(c->d_SRC, src.data(), c->NR * sizeof(double), cudaMemcpyHostToDevice,
                             c->stream));
+  kls_pre_mark(c, 0);
   orbit_kernel<<<c->NPh, ORB_THREADS, 0, c->stream>>>(P, c->d_cosw, c->d_sinw, c->d_rc, c->d_SRC,
                                                       c->d_of, c->NPh, c->d_valid, c->d_w1,
                                                       c->d_ra, c->d_pha);
   KLS_LAUNCHED(c);
+  kls_pre_mark(c, 1);
   // the host vectors must outlive the asynchronous copies
   KLS_CK(c, cudaStreamSynchronize(c->stream));
   return KLS_OK;
