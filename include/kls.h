@@ -63,7 +63,16 @@ typedef struct kls_config {
     int32_t l_min, l_max;  /* radial harmonics                              */
     int32_t nw;         /* orbit integration points                          */
     int32_t nwa;        /* stored (subsampled) orbit points                  */
+    /* Quadrature rules of the alpha, ln Rc and v grids (KLS_QUAD_*), the
+     * --quad=alpha-Rc-v option of NL_julia_boole.jl:14-16, 221-249.  0 keeps
+     * the package's rules (trapezoid, trapezoid, Simpson).                  */
+    int32_t quad_alpha, quad_rc, quad_v;
 } kls_config;
+
+#define KLS_QUAD_DEFAULT     0
+#define KLS_QUAD_TRAPEZOID   1
+#define KLS_QUAD_SIMPSON     2  /* falls back to the trapezoid rule for even n */
+#define KLS_QUAD_BOOLE       3  /* n = 4k + 1 points, else the Simpson rule   */
 
 /* Dimensions derived from a config (and device padding). */
 typedef struct kls_dims {

@@ -23,6 +23,12 @@ KLS_ERR_UNSUPPORTED = 7
 KLS_MODE_FP64 = 0
 KLS_MODE_MIXED = 1
 
+KLS_QUAD_DEFAULT = 0
+KLS_QUAD_TRAPEZOID = 1
+KLS_QUAD_SIMPSON = 2
+KLS_QUAD_BOOLE = 3
+QUAD_CODES = {"t": KLS_QUAD_TRAPEZOID, "s": KLS_QUAD_SIMPSON, "b": KLS_QUAD_BOOLE}
+
 KLS_LU_AUTO = 0
 KLS_LU_CTA = 1
 KLS_LU_CLUSTER = 2
@@ -43,7 +49,8 @@ class kls_config(C.Structure):
                 ("q1", C.c_double), ("NR", C.c_int32), ("Ne", C.c_int32),
                 ("Rc_min", C.c_double), ("Rc_max", C.c_double), ("v_min", C.c_double),
                 ("N_alpha", C.c_int32), ("alpha_max", C.c_double), ("l_min", C.c_int32),
-                ("l_max", C.c_int32), ("nw", C.c_int32), ("nwa", C.c_int32)]
+                ("l_max", C.c_int32), ("nw", C.c_int32), ("nwa", C.c_int32),
+                ("quad_alpha", C.c_int32), ("quad_rc", C.c_int32), ("quad_v", C.c_int32)]
 
 
 class kls_dims(C.Structure):

@@ -44,7 +44,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import KLS_MODE_FP64, KLS_MODE_MIXED, KlsError, check, dptr
-from .config import KalnajsConfig, copy_config
+from .config import check_quadrature, KalnajsConfig, copy_config
 
 
 # ---------------------------------------------------------------------------
@@ -104,6 +104,9 @@ def _kls_config(config: KalnajsConfig, model: Optional[ToomreZangModel]) -> _lib
     k.N_alpha, k.alpha_max = int(g.N_alpha), float(g.alpha_max)
     k.l_min, k.l_max = int(g.l_min), int(g.l_max)
     k.nw, k.nwa = int(g.nw), int(g.nwa)
+    q = getattr(g, "quadrature", "tts")
+    check_quadrature(q)
+    k.quad_alpha, k.quad_rc, k.quad_v = (_lib.QUAD_CODES[ch] for ch in q)
     return k
 
 

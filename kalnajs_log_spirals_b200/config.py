@@ -45,6 +45,9 @@ class GridConfig:
     l_max: int = 25
     nw: int = 10001
     nwa: int = 201
+    # alpha, ln Rc and v quadrature rules, t / s / b each (the --quad option
+    # of NL_julia_boole.jl:14-16); "tts" is the package's choice
+    quadrature: str = "tts"
 
 
 @dataclass
@@ -108,6 +111,12 @@ class KalnajsConfig:
     reference: ReferenceConfig = field(default_factory=ReferenceConfig)
 
 
+def check_quadrature(q: str) -> None:
+    """Three rule letters (alpha, ln Rc, v), each t / s / b."""
+    if not (isinstance(q, str) and len(q) == 3 and all(ch in "tsb" for ch in q)):
+        raise ValueError(f"grid.quadrature must be 3 letters of t/s/b (alpha, Rc, v), got {q!r}")
+
+
 def _apply(obj: Any, data: Dict[str, Any], keys) -> None:
     for k in keys:
         if k in data:
@@ -127,7 +136,8 @@ def load_config(filepath: str) -> KalnajsConfig:
         _apply(c.model, data["model"], ("L0", "n_zang", "q1"))
     if "grid" in data:
         _apply(c.grid, data["grid"], ("NR", "Ne", "Rc_min", "Rc_max", "v_min", "N_alpha",
-                                      "alpha_max", "l_min", "l_max", "nw", "nwa"))
+                                      "alpha_max", "l_min", "l_max", "nw", "nwa", "quadrature"))
+        check_quadrature(c.grid.quadrature)
     if "scan" in data:
         _apply(c.scan, data["scan"], ("n_Op", "n_gamma", "Omega_p_min", "Omega_p_max",
                                       "gamma_min", "gamma_max"))
@@ -190,7 +200,7 @@ def save_config(config: KalnajsConfig, filepath: str) -> None:
         ("physics", config.physics, ("m", "G")),
         ("model", config.model, ("L0", "n_zang", "q1")),
         ("grid", config.grid, ("NR", "Ne", "Rc_min", "Rc_max", "v_min", "N_alpha", "alpha_max",
-                               "l_min", "l_max", "nw", "nwa")),
+                               "l_min", "l_max", "nw", "nwa", "quadrature")),
         ("scan", config.scan, ("n_Op", "n_gamma", "Omega_p_min", "Omega_p_max", "gamma_min",
                                "gamma_max")),
         ("newton", config.newton, ("max_iter", "tol", "delta", "use_line_search",

@@ -62,6 +62,8 @@ int validate(const kls_config* k, std::string& msg) {
   if (np * (k->l_max - k->l_min + 1) > 4.0e9) return bad("NPh * n_l too large");
   if (!std::isfinite(k->G) || !std::isfinite(k->L0) || !std::isfinite(k->v_min))
     return bad("non-finite G, L0 or v_min");
+  for (int q : {k->quad_alpha, k->quad_rc, k->quad_v})
+    if (q < KLS_QUAD_DEFAULT || q > KLS_QUAD_BOOLE) return bad("unknown quadrature rule");
   return KLS_OK;
 }
 

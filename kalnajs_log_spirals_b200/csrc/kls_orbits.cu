@@ -29,6 +29,7 @@ struct OrbitParams {
   double L0, q1, qz, sigma_r0, DF_const;
   int n_zang;
   double dw;
+  int quad_v;          // KLS_QUAD_* rule of the v grid (never DEFAULT here)
 };
 
 // trapezoid weight of point i of a sequence (OrbitIntegration.jl:63-74)
@@ -39,18 +40,36 @@ __host__ __device__ double trap_w(double xm, double x0, double xp, int i, int n)
   return (xp - xm) / 2;
 }
 
-// Simpson weight of v point ie (OrbitIntegration.jl:79-95): falls back to
-// the trapezoid rule for n < 3 or even n
-__device__ double simpson_w(const OrbitParams& P, int ie) {
-  int n = P.Ne;
-  auto v = [&](int i) { return kls_lin(P.v_min, 1.0, n, i); };
-  if (n < 3 || (n % 2) == 0) {
-    double xm = ie > 0 ? v(ie - 1) : 0.0, xp = ie < n - 1 ? v(ie + 1) : 0.0;
-    return trap_w(xm, v(ie), xp, ie, n);
+// Weight of point i of an n-point uniform grid x(.) under `rule`:
+// KLS_QUAD_TRAPEZOID (OrbitIntegration.jl:63-74), KLS_QUAD_SIMPSON
+// (OrbitIntegration.jl:79-95: the trapezoid rule for n < 3 or even n) or
+// KLS_QUAD_BOOLE (2h/45 (7, 32, 12, 32, 14, ..., 7) for n = 4k + 1 >= 5,
+// else the Simpson rule; NL_julia_boole.jl:186-217).
+template <typename X>
+__host__ __device__ double quad_w(int rule, const X& x, int i, int n) {
+  auto trap = [&]() {
+    double xm = i > 0 ? x(i - 1) : 0.0, xp = i < n - 1 ? x(i + 1) : 0.0;
+    return trap_w(xm, x(i), xp, i, n);
+  };
+  if (rule == KLS_QUAD_TRAPEZOID) return trap();
+  if (rule == KLS_QUAD_BOOLE && n >= 5 && (n - 1) % 4 == 0) {
+    double dx = x(1) - x(0);
+    double f = 2 * dx / 45;
+    if (i == 0 || i == n - 1) return 7 * f;
+    int r = i % 4;
+    return r == 0 ? 14 * f : (r == 2 ? 12 * f : 32 * f);
   }
-  double dx = v(1) - v(0);
-  if (ie == 0 || ie == n - 1) return dx / 3;
-  return (ie % 2 == 1) ? 4 * dx / 3 : 2 * dx / 3;
+  if (n < 3 || (n % 2) == 0) return trap();
+  double dx = x(1) - x(0);
+  if (i == 0 || i == n - 1) return dx / 3;
+  return (i % 2 == 1) ? 4 * dx / 3 : 2 * dx / 3;
+}
+
+// S_e weight of v point ie (OrbitIntegration.jl:119-123; Simpson unless the
+// configuration selects another rule)
+__device__ double v_weight(const OrbitParams& P, int ie) {
+  auto v = [&](int i) { return kls_lin(P.v_min, 1.0, P.Ne, i); };
+  return quad_w(P.quad_v, v, ie, P.Ne);
 }
 
 __device__ double taper(const OrbitParams& P, double L) {
@@ -266,7 +285,7 @@ orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __res
     if (!isfinite(FL)) FL = 0.0;
     // S_e quadrature weight (OrbitIntegration.jl:119-123); S_RC from the host
     double src = SRC[iR];
-    double se = simpson_w(P, ie);
+    double se = v_weight(P, ie);
     double vals[OF_COUNT] = {Rc, ecc, v, R1, R2, E, L, L2, sg, se,
                              Om1, Om2, jac, F0, FE, FL, src * se * jac};
     for (int f = 0; f < OF_COUNT; ++f) of[(size_t)f * NPh + p] = vals[f];
@@ -288,6 +307,7 @@ int kls_run_orbits(kls_ctx* c) {
   // DF normalisation (Models.jl:53-54), Gamma of a real argument
   P.DF_const = 1.0 / (2.0 * KLS_PI * std::pow(2.0, P.qz / 2.0) * std::sqrt(KLS_PI) *
                       std::tgamma((P.qz + 1.0) / 2.0) * std::pow(P.sigma_r0, P.qz + 2.0));
+  P.quad_v = k.quad_v == KLS_QUAD_DEFAULT ? KLS_QUAD_SIMPSON : k.quad_v;
   double w0 = kls_lin(1e-8, KLS_PI - 1e-8, c->nw, 0);
   double w1 = kls_lin(1e-8, KLS_PI - 1e-8, c->nw, 1);
   P.dw = w1 - w0;
@@ -305,10 +325,13 @@ int kls_run_orbits(kls_ctx* c) {
   }
   const double la = std::log10(k.Rc_min), lb = std::log10(k.Rc_max);
   for (int i = 0; i < c->NR; ++i) rc[i] = std::pow(10.0, kls_lin(la, lb, c->NR, i));
-  for (int i = 0; i < c->NR; ++i) {
-    double um = i > 0 ? std::log(rc[i - 1]) : 0.0;
-    double up = i < c->NR - 1 ? std::log(rc[i + 1]) : 0.0;
-    src[i] = rc[i] * trap_w(um, std::log(rc[i]), up, i, c->NR);
+  {
+    // S_RC = Rc * (weights on ln Rc): trapezoid unless configured
+    std::vector<double> u(c->NR);
+    for (int i = 0; i < c->NR; ++i) u[i] = std::log(rc[i]);
+    const int rule = k.quad_rc == KLS_QUAD_DEFAULT ? KLS_QUAD_TRAPEZOID : k.quad_rc;
+    auto x = [&](int i) { return u[i]; };
+    for (int i = 0; i < c->NR; ++i) src[i] = rc[i] * quad_w(rule, x, i, c->NR);
   }
   KLS_CK(c, cudaMemcpyAsync(c->d_cosw, cw.data(), c->nw * sizeof(double), cudaMemcpyHostToDevice,
                             c->stream));
@@ -330,11 +353,14 @@ int kls_run_orbits(kls_ctx* c) {
 }
 
 int kls_upload_alpha(kls_ctx* c) {
-  // alpha grid and its trapezoid weights (BasisFunctions.jl:106-107)
+  // alpha grid and its weights (BasisFunctions.jl:106-107: trapezoid unless
+  // configured)
   std::vector<double> a(c->Na), d(c->Na);
   for (int i = 0; i < c->Na; ++i) a[i] = kls_lin(-c->cfg.alpha_max, c->cfg.alpha_max, c->Na, i);
-  for (int i = 0; i < c->Na; ++i)
-    d[i] = trap_w(i > 0 ? a[i - 1] : 0.0, a[i], i < c->Na - 1 ? a[i + 1] : 0.0, i, c->Na);
+  const int rule =
+      c->cfg.quad_alpha == KLS_QUAD_DEFAULT ? KLS_QUAD_TRAPEZOID : c->cfg.quad_alpha;
+  auto x = [&](int i) { return a[i]; };
+  for (int i = 0; i < c->Na; ++i) d[i] = quad_w(rule, x, i, c->Na);
   KLS_CK(c, cudaMemcpy(c->d_alpha, a.data(), c->Na * sizeof(double), cudaMemcpyHostToDevice));
   KLS_CK(c, cudaMemcpy(c->d_dalpha, d.data(), c->Na * sizeof(double), cudaMemcpyHostToDevice));
   return KLS_OK;

@@ -18,6 +18,7 @@ struct KlsConfig
     NR::Int32; Ne::Int32; Rc_min::Float64; Rc_max::Float64; v_min::Float64
     N_alpha::Int32; alpha_max::Float64; l_min::Int32; l_max::Int32
     nw::Int32; nwa::Int32
+    quad_alpha::Int32; quad_rc::Int32; quad_v::Int32   # 0: the package's rules
 end
 
 struct KlsNewtonCfg
@@ -62,7 +63,7 @@ function kls_config(config, model)
     g = config.grid
     KlsConfig(config.physics.m, config.physics.G, config.model.L0, config.model.n_zang,
               Float64(config.model.q1), g.NR, g.Ne, g.Rc_min, g.Rc_max, g.v_min, g.N_alpha,
-              g.alpha_max, g.l_min, g.l_max, g.nw, g.nwa)
+              g.alpha_max, g.l_min, g.l_max, g.nw, g.nwa, 0, 0, 0)
 end
 
 "precompute_all (BasisFunctions.jl:73): grids, orbits, W_l, N_m on the GPU."

@@ -71,6 +71,9 @@ class OracleConfig:
     l_max: int = 25
     nw: int = 10001
     nwa: int = 201
+    # quadrature rules of the alpha, ln Rc and v grids, one of t / s / b each
+    # (NL_julia_boole.jl:14-16, 221-249); "tts" is the package's choice
+    quad: str = "tts"
 
     @property
     def n_l(self) -> int:
@@ -195,6 +198,29 @@ def simpson_coef(x: np.ndarray) -> np.ndarray:
     return S
 
 
+def boole_coef(x: np.ndarray) -> np.ndarray:
+    """Composite Boole weights 2h/45 (7, 32, 12, 32, 14, ..., 7) for n = 4k + 1
+    points, else the Simpson rule (NL_julia_boole.jl:186-217; n < 5 also
+    falls back, where the script has no defined result)."""
+    n = len(x)
+    if n < 5 or (n - 1) % 4 != 0:
+        return simpson_coef(x)
+    dx = x[1] - x[0]
+    f = 2 * dx / 45
+    S = np.empty(n)
+    for i in range(n):
+        r = i % 4
+        S[i] = 14 * f if r == 0 else (12 * f if r == 2 else 32 * f)
+    S[0] = 7 * f
+    S[-1] = 7 * f
+    return S
+
+
+def quad_coef(x: np.ndarray, rule: str) -> np.ndarray:
+    """GetCoefs (NL_julia_boole.jl:221-232): t trapezoid, s Simpson, b Boole."""
+    return {"t": trapezoid_coef, "s": simpson_coef, "b": boole_coef}[rule](x)
+
+
 # --------------------------------------------------------------------------
 # OrbitIntegration.jl:102-170
 # --------------------------------------------------------------------------
@@ -219,9 +245,9 @@ def compute_grids(c: OracleConfig, model: ToomreZang) -> Grids:
     Rc_1d = np.array([10.0 ** float(x) for x in linspace(math.log10(c.Rc_min),
                                                           math.log10(c.Rc_max), NR)])
     uRc = np.array([math.log(x) for x in Rc_1d])
-    S_RC = Rc_1d * trapezoid_coef(uRc)
+    S_RC = Rc_1d * quad_coef(uRc, c.quad[1])
     v_arr = linspace(c.v_min, 1.0, Ne)
-    S_e = np.tile(simpson_coef(v_arr), (NR, 1))
+    S_e = np.tile(quad_coef(v_arr, c.quad[2]), (NR, 1))
     v = np.tile(v_arr, (NR, 1))
     Rc = np.tile(Rc_1d[:, None], (1, Ne))
     v = np.where(np.abs(v) < 1e-14, 1e-12, v)
@@ -445,7 +471,7 @@ def precompute_all(c: OracleConfig, with_W: bool = True) -> Precomputed:
     g = compute_grids(c, model)
     o = compute_orbits(c, model, g)
     alpha = linspace(-c.alpha_max, c.alpha_max, c.N_alpha)
-    d_alpha = trapezoid_coef(alpha)
+    d_alpha = quad_coef(alpha, c.quad[0])
     l_arr = np.arange(c.l_min, c.l_max + 1)
     W = compute_W_l(c, o, alpha, l_arr) if with_W else None
     N = compute_N_kernel(c.m, alpha, d_alpha)

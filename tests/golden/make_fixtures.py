@@ -33,6 +33,10 @@ CASES = {
     # odd/even quadrature fallbacks, other m, n_zang, real q1
     "variants": dict(m=3, n_zang=2, q1=5.5, Ne=6, NR=7, N_alpha=8, l_min=-2, l_max=4,
                      alpha_max=5.0, nw=301, nwa=31),
+    # Boole rule on all three grids (n = 4k + 1), NL_julia_boole.jl --quad=bbb
+    "boole": dict(quad="bbb", NR=9, Ne=9, N_alpha=9),
+    # Simpson on alpha and ln Rc, Boole falling back to Simpson/trapezoid on v
+    "quad_mixed": dict(quad="ssb", NR=9, Ne=8, N_alpha=11),
 }
 
 OMEGAS = [0.88 + 0.12j, 0.6 + 0.05j, 1.2 + 0.3j]
@@ -86,8 +90,10 @@ def sensitivity(name: str, over: dict, base: dict) -> dict:
             for k, v in base.items() if k not in ("config", "omegas")}
 
 
-def main() -> None:
+def main(names=None) -> None:
     for name, over in CASES.items():
+        if names and name not in names:
+            continue
         d = make(name, over)
         d.update(sensitivity(name, over, d))
         path = os.path.join(HERE, f"{name}.npz")
@@ -96,4 +102,4 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

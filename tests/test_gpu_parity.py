@@ -34,6 +34,8 @@ def kconfig(**kw) -> K.KalnajsConfig:
               "l_max", "nw", "nwa"):
         if f in kw:
             setattr(c.grid, f, kw[f])
+    if "quad" in kw:
+        c.grid.quadrature = kw["quad"]
     return c
 
 

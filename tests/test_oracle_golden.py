@@ -100,3 +100,39 @@ def test_find_minimum_column_major_first():
     g = np.array([[3, 1, 5], [1, 4, 1]], dtype=complex)
     # minima |1| at (0,1), (1,0), (1,2); column-major first is (1,0)
     assert O.find_minimum(g, np.array([0.1, 0.2, 0.3]), np.array([0.01, 0.02])) == (0.1, 0.02)
+
+
+def test_boole_rule_is_exact_to_degree_five():
+    x = np.linspace(0.0, 2.0, 9)                 # n = 4k + 1
+    S = O.boole_coef(x)
+    for k in range(6):
+        exact = 2.0 ** (k + 1) / (k + 1)
+        assert abs(np.dot(S, x ** k) - exact) < 1e-13 * exact, k
+    assert abs(np.dot(S, x ** 6) - 2.0 ** 7 / 7) > 1e-6   # degree 6 is not exact
+
+
+def test_boole_falls_back_to_simpson_and_trapezoid():
+    for n in (6, 7, 8, 4, 3, 2):
+        x = np.linspace(-1.0, 3.0, n)
+        assert np.array_equal(O.boole_coef(x), O.simpson_coef(x)), n
+    for rule in "tsb":
+        for n in (5, 9, 13, 10):
+            x = np.linspace(-1.0, 3.0, n)
+            assert abs(O.quad_coef(x, rule).sum() - 4.0) < 1e-13, (rule, n)
+
+
+def test_quadrature_config_key(tmp_path):
+    import kalnajs_log_spirals_b200 as K
+    p = tmp_path / "c.toml"
+    p.write_text('[grid]\nNR = 9\nquadrature = "bbs"\n')
+    c = K.load_config(str(p))
+    assert c.grid.quadrature == "bbs"
+    K.save_config(c, str(tmp_path / "d.toml"))
+    assert K.load_config(str(tmp_path / "d.toml")).grid.quadrature == "bbs"
+    p.write_text('[grid]\nquadrature = "tx"\n')
+    with pytest.raises(ValueError):
+        K.load_config(str(p))
+    from kalnajs_log_spirals_b200 import api, _lib
+    k = api._kls_config(c, None)
+    assert (k.quad_alpha, k.quad_rc, k.quad_v) == (_lib.KLS_QUAD_BOOLE, _lib.KLS_QUAD_BOOLE,
+                                                   _lib.KLS_QUAD_SIMPSON)
