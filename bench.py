@@ -570,6 +570,9 @@ def ours(args):
         _lib.check(h, lib.kls_enable_timing(h, 0))
         return stage / reps
 
+    # K split counts chosen by the library's autotuner at this batch size
+    tunes = {"fp64": K.autotune(pc, "Float64", batch=nb)}
+
     # ---- plain FP64: device-resident timing (headline) ----------------------
     ms, launches, clk = time_device(_lib.KLS_MODE_FP64, sample_clocks=True)
     ms_per_step = ms / args.steps
@@ -602,6 +605,7 @@ def ours(args):
         t0 = time.perf_counter()
         _lib.check(h, lib.kls_prepare_mixed(h))
         t_split = time.perf_counter() - t0
+        tunes["mixed"] = K.autotune(pc, "Float32", batch=nb)
         ms_mx, launches_mx, _ = time_device(_lib.KLS_MODE_MIXED)
         stage_mx = stage_times(_lib.KLS_MODE_MIXED)
         ach_mx = nb * mixed_flops_per_det / (stage_mx[1] * 1e-3) / 1e12
@@ -704,6 +708,10 @@ def ours(args):
                 "d2h_bytes_per_step": nb * 24},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "autotune": {k: {"splits": t.splits, "default_splits": t.default_splits,
+                         "candidates": t.candidates, "ms_per_omega": t.ms_per_omega,
+                         "default_ms_per_omega": t.default_ms_per_omega}
+                     for k, t in tunes.items()},
         "precompute_s": t_pre,
         "precompute": precompute_roofline(cfg, dims, pre_ms, peak64, peaks),
         "mixed": mixed,

@@ -207,3 +207,39 @@ def propose(mlp: MLP, spec: ModelSpec, det_fn, k: int = 48, **grid) -> Tuple[flo
     d = np.asarray(det_fn(spec.m * Op + 1j * gm))
     i = int(np.argmin(np.abs(d)))
     return float(Op[i]), float(gm[i]), len(Op)
+
+
+@dataclasses.dataclass
+class RootResult:
+    """find_root outcome: the Newton result and how its start was found."""
+    newton: object                 # api.NewtonResult (hybrid Newton, FP64 finish)
+    start: Tuple[float, float]
+    source: str                    # "proposal" or "grid_scan"
+    proposal_dets: int             # determinants spent on the proposal
+    scan_dets: int                 # determinants spent on the fallback scan (0 if none)
+
+
+def find_root(mlp: MLP, config: KalnajsConfig, precomputed, k: int = 48,
+              min_gamma: float = 1e-4) -> RootResult:
+    """Newton root of det(I - M) with a learned start and the scan as fallback.
+
+    The proposal (``propose`` over the config's scan grid, split-BF16
+    determinants) starts ``newton_search_hybrid``, whose last steps and
+    stopping test are FP64; if that Newton does not converge to a growing
+    mode (gamma > min_gamma), the reference workflow runs instead: the full
+    grid scan (GridScan.jl:25-88) in the split-BF16 form and the hybrid
+    Newton from its argmin.
+    """
+    from . import api
+    s = config.scan
+    spec = ModelSpec(int(config.model.n_zang), float(config.model.q1), int(config.physics.m))
+    dev = api.to_device(precomputed, api.GPUType.NVIDIA, "Float32")
+    Op, g, used = propose(mlp, spec, lambda om: api.compute_determinant_batched(
+        om, precomputed, dev, batch_size=16), k=k, n_Op=s.n_Op, n_gamma=s.n_gamma,
+        Op_range=(s.Omega_p_min, s.Omega_p_max), g_range=(s.gamma_min, s.gamma_max))
+    r = api.newton_search_hybrid(config, precomputed, Op, g)
+    if r.converged and r.gamma > min_gamma:
+        return RootResult(r, (Op, g), "proposal", used, 0)
+    _, Op0, g0 = api.grid_scan(config, precomputed, dev)
+    r = api.newton_search_hybrid(config, precomputed, Op0, g0)
+    return RootResult(r, (Op0, g0), "grid_scan", used, s.n_Op * s.n_gamma)

@@ -101,3 +101,28 @@ def test_proposer_replaces_the_grid_scan(lib_path):
     assert tried >= 4
     assert agree >= 0.75 * tried, (agree, tried)
     assert prop_evals * 10 < scan_evals, (prop_evals, scan_evals)
+
+
+def test_find_root_falls_back_to_the_scan(lib_path):
+    """A proposal whose Newton root is not accepted (here: min_gamma above any
+    growth rate) falls back to the reference workflow, grid scan then Newton,
+    and returns the scan-started root; with the default acceptance the
+    (untrained) network's start still yields a converged root."""
+    cfg = kconfig(**TINY)
+    cfg.newton.tol = 1e-12
+    cfg.newton.max_iter = 40
+    pc = K.precompute_all(cfg)
+    mlp = P.MLP(256, 4, seed=123)                 # untrained
+    forced = P.find_root(mlp, cfg, pc, k=4, min_gamma=10.0)
+    free = P.find_root(mlp, cfg, pc, k=4)
+    _, Op0, g0 = K.grid_scan(cfg, pc)
+    ref = newton64(cfg, Op0, g0)
+    pc.close()
+    mlp.close()
+    assert forced.source == "grid_scan" and forced.proposal_dets == 4
+    assert forced.scan_dets == cfg.scan.n_Op * cfg.scan.n_gamma
+    assert forced.start == (Op0, g0)
+    assert ref.converged and forced.newton.converged
+    assert abs(forced.newton.Omega_p - ref.Omega_p) <= 1e-10
+    assert abs(forced.newton.gamma - ref.gamma) <= 1e-10
+    assert free.newton.converged and free.source in ("proposal", "grid_scan")
