@@ -284,7 +284,8 @@ int kls_multi_get_info(const kls_multi* mm, kls_multi_info* out);
 /* ---- autotuner (no reference counterpart) ---------------------------------- *
  * Times the contraction of `mode` for the context at `batch` omegas per call
  * with each candidate K split count (the occupancy-derived default, half,
- * twice and three times it) and keeps the fastest for the context.  Results
+ * twice and three times it) and, for the split-BF16 form, each kernel (one
+ * CTA or a CTA pair per tile), and keeps the fastest for the context.  Results
  * are cached per (device name, mode, N_alpha_pad, K_pad, batch) for the
  * process, and in the text file named by the environment variable
  * KLS_TUNE_CACHE when it is set.                                            */
@@ -295,8 +296,12 @@ typedef struct kls_tune_result {
     int32_t candidates;           /* candidates timed (0: from the cache)     */
     double  ms_per_omega;         /* contraction time of the choice           */
     double  default_ms_per_omega; /* and of the untuned choice (0: cached)    */
+    int32_t form;                 /* split-BF16 kernel chosen (KLS_MIXED_*)   */
 } kls_tune_result;
 int kls_autotune(kls_ctx* ctx, int mode, int batch, kls_tune_result* out);
+/* Set the K split count of `mode` by hand (clamped to what the table
+ * allows); determinants stay batch-independent for a fixed count.         */
+int kls_set_splits(kls_ctx* ctx, int mode, int splits);
 
 /* ---- determinant stage form (no reference counterpart) -------------------- *
  * KLS_LU_CLUSTER factors each I - M(omega) on one thread-block cluster of 8
@@ -310,6 +315,19 @@ int kls_autotune(kls_ctx* ctx, int mode, int batch, kls_tune_result* out);
 #define KLS_LU_CTA           1
 #define KLS_LU_CLUSTER       2
 int kls_set_lu_mode(kls_ctx* ctx, int mode);
+
+/* ---- split-BF16 contraction kernel (no reference counterpart) ------------- *
+ * KLS_MIXED_ONE_CTA: one CTA per 128-row x 64-alpha x 2-omega tile.
+ * KLS_MIXED_PAIR: a cluster of two CTAs per 256-row tile (tcgen05
+ * cta_group::2, M = 256): each SM forms half as much of the per-omega
+ * operand; it pays off when 2 N_alpha_pad is a multiple of 256 (otherwise
+ * the last pair's odd CTA has no rows).  Both return the same bits.
+ * KLS_MIXED_AUTO (the default) is the one-CTA form; kls_autotune times both.
+ * Calls kls_prepare_mixed first if needed.                                    */
+#define KLS_MIXED_AUTO       0
+#define KLS_MIXED_ONE_CTA    1
+#define KLS_MIXED_PAIR       2
+int kls_set_mixed_form(kls_ctx* ctx, int form);
 
 /* ---- instrumentation ----------------------------------------------------- */
 /* Per-stage device time (ms) of the last det batch when timing is enabled:

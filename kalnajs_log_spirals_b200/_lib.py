@@ -29,6 +29,10 @@ KLS_QUAD_SIMPSON = 2
 KLS_QUAD_BOOLE = 3
 QUAD_CODES = {"t": KLS_QUAD_TRAPEZOID, "s": KLS_QUAD_SIMPSON, "b": KLS_QUAD_BOOLE}
 
+KLS_MIXED_AUTO = 0
+KLS_MIXED_ONE_CTA = 1
+KLS_MIXED_PAIR = 2
+
 KLS_LU_AUTO = 0
 KLS_LU_CTA = 1
 KLS_LU_CLUSTER = 2
@@ -93,7 +97,7 @@ class kls_multi_info(C.Structure):
 class kls_tune_result(C.Structure):
     _fields_ = [("mode", C.c_int32), ("splits", C.c_int32), ("default_splits", C.c_int32),
                 ("candidates", C.c_int32), ("ms_per_omega", C.c_double),
-                ("default_ms_per_omega", C.c_double)]
+                ("default_ms_per_omega", C.c_double), ("form", C.c_int32)]
 
 
 _P = C.c_void_p
@@ -142,7 +146,9 @@ SIGNATURES = {
     "kls_scan_multi": (C.c_int, [_P, C.POINTER(kls_scan_cfg), _D, _D, _D, _D]),
     "kls_multi_get_info": (C.c_int, [_P, C.POINTER(kls_multi_info)]),
     "kls_autotune": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(kls_tune_result)]),
+    "kls_set_splits": (C.c_int, [_P, C.c_int, C.c_int]),
     "kls_set_lu_mode": (C.c_int, [_P, C.c_int]),
+    "kls_set_mixed_form": (C.c_int, [_P, C.c_int]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_get_precompute_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),

@@ -594,6 +594,7 @@ class TuneResult:
     candidates: int
     ms_per_omega: float
     default_ms_per_omega: float
+    form: int = 0
 
 
 def autotune(precomputed: PrecomputedData, Tgpu="Float64", batch: int = 2) -> TuneResult:
@@ -601,7 +602,7 @@ def autotune(precomputed: PrecomputedData, Tgpu="Float64", batch: int = 2) -> Tu
     r = _lib.kls_tune_result()
     precomputed.ctx.call("kls_autotune", _mode_for(Tgpu), int(batch), C.byref(r))
     return TuneResult(r.mode, r.splits, r.default_splits, r.candidates, r.ms_per_omega,
-                      r.default_ms_per_omega)
+                      r.default_ms_per_omega, r.form)
 
 
 class ModelBatch:

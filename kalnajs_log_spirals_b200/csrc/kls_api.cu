@@ -666,7 +666,7 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
 namespace {
 
 std::mutex g_tune_mu;
-std::map<std::string, int> g_tune;
+std::map<std::string, std::pair<int, int>> g_tune;   // key -> (splits, mixed form)
 bool g_tune_loaded = false;
 
 std::string tune_key(const kls_ctx* c, int mode, int batch) {
@@ -680,24 +680,31 @@ std::string tune_key(const kls_ctx* c, int mode, int batch) {
   return o.str();
 }
 
+// cache file lines: "<key> <splits> <form>"
 void tune_load_file() {
   if (g_tune_loaded) return;
   g_tune_loaded = true;
   const char* path = std::getenv("KLS_TUNE_CACHE");
   if (!path || !*path) return;
   std::ifstream f(path);
-  std::string key;
-  int s;
-  while (f >> key >> s)
-    if (s > 0) g_tune[key] = s;
+  std::string line;
+  while (std::getline(f, line)) {
+    std::istringstream in(line);
+    std::string key;
+    int s = 0, form = 0;
+    if (in >> key >> s && s > 0) {
+      if (!(in >> form)) form = 0;
+      g_tune[key] = std::make_pair(s, form);
+    }
+  }
 }
 
-void tune_store(const std::string& key, int s) {
-  g_tune[key] = s;
+void tune_store(const std::string& key, int s, int form) {
+  g_tune[key] = std::make_pair(s, form);
   const char* path = std::getenv("KLS_TUNE_CACHE");
   if (!path || !*path) return;
   std::ofstream f(path, std::ios::app);
-  f << key << " " << s << "\n";
+  f << key << " " << s << " " << form << "\n";
 }
 
 int apply_splits(kls_ctx* c, int mode, int s) {
@@ -758,9 +765,15 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
   if (mode == KLS_MODE_FP64 && !c->d_Wre)
     return kls_fail(c, KLS_ERR_STATE, "the FP64 table was released (kls_release_fp64)");
   if (mode == KLS_MODE_MIXED && !c->mixed && (r = kls_mixed_prepare(c))) return r;
-  const int def = mode == KLS_MODE_FP64 ? kls_choose_splits(c) : kls_mixed_default_splits(c);
-  const int max_s = mode == KLS_MODE_FP64 ? (int)std::max<int64_t>(1, c->K_pad / (16 * 8))
-                                          : (int)std::max<int64_t>(1, c->K_pad / 64);
+  const bool mixed = mode == KLS_MODE_MIXED;
+  const int def = mixed ? kls_mixed_default_splits(c) : kls_choose_splits(c);
+  const int def_form = mixed ? kls_mixed_form_of(c) : 0;
+  const int max_s = mixed ? (int)std::max<int64_t>(1, c->K_pad / 64)
+                          : (int)std::max<int64_t>(1, c->K_pad / (16 * 8));
+  auto apply = [&](int s, int form) -> int {
+    if (mixed && (r = kls_mixed_set_form(c, form))) return r;
+    return apply_splits(c, mode, s);
+  };
   kls_tune_result res{};
   res.mode = mode;
   res.default_splits = def;
@@ -770,8 +783,9 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
     tune_load_file();
     auto it = g_tune.find(key);
     if (it != g_tune.end()) {
-      res.splits = std::min(it->second, max_s);
-      if ((r = apply_splits(c, mode, res.splits))) return r;
+      res.splits = std::min(it->second.first, max_s);
+      res.form = mixed ? (it->second.second ? it->second.second : def_form) : 0;
+      if ((r = apply(res.splits, res.form))) return r;
       if (out) *out = res;
       return KLS_OK;
     }
@@ -780,28 +794,56 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
   for (int& s : cand) s = std::max(1, std::min(s, max_s));
   std::sort(cand.begin(), cand.end());
   cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  // the split-BF16 form also chooses its tile: one CTA or a CTA pair
+  std::vector<int> forms = mixed ? std::vector<int>{KLS_MIXED_ONE_CTA, KLS_MIXED_PAIR}
+                                 : std::vector<int>{0};
   double best_ms = INFINITY;
-  int best = def;
-  for (int s : cand) {
-    if ((r = apply_splits(c, mode, s))) return r;
-    double ms = 0.0;
-    if ((r = time_contraction(c, mode, batch, &ms))) return r;
-    if (s == def) res.default_ms_per_omega = ms;
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = s;
+  int best = def, best_form = def_form;
+  for (int form : forms)
+    for (int s : cand) {
+      if ((r = apply(s, form))) return r;
+      double ms = 0.0;
+      if ((r = time_contraction(c, mode, batch, &ms))) return r;
+      if (s == def && form == def_form) res.default_ms_per_omega = ms;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = s;
+        best_form = form;
+      }
+      res.candidates++;
     }
-    res.candidates++;
-  }
-  if ((r = apply_splits(c, mode, best))) return r;
+  if ((r = apply(best, best_form))) return r;
   res.splits = best;
+  res.form = best_form;
   res.ms_per_omega = best_ms;
   {
     std::lock_guard<std::mutex> g(g_tune_mu);
-    tune_store(key, best);
+    tune_store(key, best, best_form);
   }
   if (out) *out = res;
   return KLS_OK;
+}
+
+int kls_set_splits(kls_ctx* c, int mode, int splits) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (splits < 1) return kls_fail(c, KLS_ERR_CONFIG, "splits must be >= 1");
+  if (mode == KLS_MODE_FP64) {
+    const int max_s = (int)std::max<int64_t>(1, c->K_pad / (16 * 8));
+    return apply_splits(c, mode, std::min(splits, max_s));
+  }
+  if (mode != KLS_MODE_MIXED) return kls_fail(c, KLS_ERR_CONFIG, "unknown precision mode");
+  if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
+  return apply_splits(c, mode, splits);
+}
+
+int kls_set_mixed_form(kls_ctx* c, int form) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (form != KLS_MIXED_AUTO && form != KLS_MIXED_ONE_CTA && form != KLS_MIXED_PAIR)
+    return kls_fail(c, KLS_ERR_CONFIG, "unknown mixed contraction form");
+  if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
+  return kls_mixed_set_form(c, form == KLS_MIXED_AUTO ? KLS_MIXED_ONE_CTA : form);
 }
 
 int kls_set_lu_mode(kls_ctx* c, int mode) {

@@ -181,6 +181,8 @@ int kls_multi_launch_mixed(cudaStream_t st, const kls_mdesc* d_md, const int2* d
 int kls_mixed_slots(int device);
 int kls_mixed_splits_of(const kls_ctx* c);
 int kls_mixed_default_splits(const kls_ctx* c);
+int kls_mixed_set_form(kls_ctx* c, int form);
+int kls_mixed_form_of(const kls_ctx* c);
 int kls_mixed_set_splits(kls_ctx* c, int splits);
 const void* kls_mixed_tables(const kls_ctx* c, const void** Xl, const void** tmap_h,
                              const void** tmap_l);

@@ -547,6 +547,375 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
   }
 }
 
+// ---- CTA-pair form (tcgen05 cta_group::2) ------------------------------------
+// Two CTAs of a cluster compute a 256-row x 2-omega tile with M = 256,
+// N = 128 x omegas MMAs issued by the even CTA ("leader"):
+//   A (X rows): CTA c holds rows m0_c = (2 tp + c) 128 .. +127 (its own TMA);
+//   B (Y rows): CTA c produces the Y rows of alphas a0 + 32c .. +31 for both
+//               omegas (row omega 64 + 2 alpha + part), so each SM forms half
+//               as much of Y per output as the one-CTA kernel;
+//   D: CTA c's TMEM holds its 128 rows; column j < N/2 comes from the
+//      leader's Y tile, j >= N/2 from the peer's.
+// The peer's TMA completes on the leader's full barrier (cta_group::2 form),
+// its producer and drain warps arrive on the leader's barriers through
+// shared::cluster addresses, and the leader's commits multicast to both CTAs.
+// A final cluster barrier keeps both CTAs resident until the last remote
+// access.  When 2 Npad is not a multiple of 256 the last pair's odd CTA has
+// no X rows: it loads nothing, still produces its half of Y, and its drain
+// writes nothing.  Same k-blocks, chunks, flush order and U arithmetic as
+// mixed_contract_kernel.
+constexpr int MP_STAGES = 3;
+constexpr int MP_AH = MX_AB / 2;                               // alphas per CTA
+constexpr int MP_TILE_Y = MX_OMEGA * 2 * MP_AH * MX_BK * 2;    // 16 KB per part
+constexpr int MP_STAGE_BYTES = 2 * MX_TILE_X + 2 * MP_TILE_Y;  // 64 KB
+constexpr size_t MP_SMEM = (size_t)MP_STAGES * MP_STAGE_BYTES + MX_WRING_BYTES + 1024;
+
+struct PairParams {
+  int Npad, rows;
+  int64_t K_pad;
+  int nkb_total, kb_per_split, splits, n_omega, tiles_a;
+};
+
+__device__ __forceinline__ uint32_t mapa_u32(uint32_t a, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_cl(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait, cluster-scope acquire (barriers that the peer CTA completes)
+__device__ __forceinline__ bool mbar_wait_cl(uint32_t a, uint32_t parity, volatile int* abort,
+                                             int* err, int code) {
+  unsigned long long t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    if (mbar_try_cl(a, parity)) return true;
+    if (abort && *abort) return false;
+    if ((it & 63) == 0) {
+      unsigned long long t = globaltimer();
+      if (t0 == 0) t0 = t;
+      else if (t - t0 > MX_WAIT_NS) {
+        if (abort) *abort = 1;
+        atomicCAS(err, 0, code);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                          uint32_t acc) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+// commit of the leader's MMAs to the barrier at this offset in both CTAs
+__device__ __forceinline__ void umma_pair_commit(uint32_t mbar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(mbar),
+      "h"((unsigned short)3)
+      : "memory");
+}
+// TMA into this CTA's shared memory, completing on the leader's barrier
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                                 uint32_t mbar_cluster) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(mbar_cluster)
+      : "memory");
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MX_THREADS, 1)
+mixed_pair_kernel(const __grid_constant__ CUtensorMap tm_h, const __grid_constant__ CUtensorMap tm_l,
+                  PairParams P, const __nv_bfloat16* __restrict__ Xh,
+                  const __nv_bfloat16* __restrict__ Xl, const float2* __restrict__ wt32,
+                  double* __restrict__ part, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_full_x[MP_STAGES], bar_full_y[MP_STAGES],
+      bar_empty[MP_STAGES], bar_w_full[MX_WSTAGES], bar_w_empty[MX_WSTAGES], bar_acc_full[2],
+      bar_acc_empty[2], bar_done;
+  __shared__ uint32_t s_tmem;
+  __shared__ volatile int s_abort;
+
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint32_t crank;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(crank));
+  const bool leader = crank == 0;
+  const int pair_tile = blockIdx.x >> 1;
+  const int tp = pair_tile / P.tiles_a, ta = pair_tile % P.tiles_a;
+  const int R = P.rows;
+  const int m0 = (2 * tp + (int)crank) * MX_BM;       // this CTA's first X row
+  const bool has_rows = m0 < R;
+  const bool peer_rows = (2 * tp + 1) * MX_BM < R;      // the odd CTA of the pair has rows
+  const int a0 = ta * MX_AB;
+  const int ah0 = a0 + MP_AH * (int)crank;               // this CTA's alphas
+  const int split = blockIdx.y, grp = blockIdx.z;
+  const int om0 = grp * MX_OMEGA;
+  const int n_om = min(MX_OMEGA, P.n_omega - om0);
+  const int kb0 = split * P.kb_per_split;
+  const int nkb = max(0, min(P.nkb_total, kb0 + P.kb_per_split) - kb0);
+  const int nch = (nkb + MX_CHUNK_KB - 1) / MX_CHUNK_KB;
+  const int NB = MX_BN * n_om;                            // MMA N
+  const int half = NB / 2;                                // columns per CTA
+
+  auto xh_s = [&](int s) { return smem + (size_t)s * MP_STAGE_BYTES; };
+  auto xl_s = [&](int s) { return smem + (size_t)s * MP_STAGE_BYTES + MX_TILE_X; };
+  auto yh_s = [&](int s) { return smem + (size_t)s * MP_STAGE_BYTES + 2 * MX_TILE_X; };
+  auto yl_s = [&](int s) {
+    return smem + (size_t)s * MP_STAGE_BYTES + 2 * MX_TILE_X + MP_TILE_Y;
+  };
+  auto w_s = [&](int ws, int j) {
+    return reinterpret_cast<float2*>(smem + (size_t)MP_STAGES * MP_STAGE_BYTES +
+                                     (size_t)ws * MX_OMEGA * MX_W_BYTES) + j * MX_BK;
+  };
+
+  if (tid == 0) {
+    s_abort = 0;
+    for (int s = 0; s < MP_STAGES; ++s) {
+      mbar_init(smem_u32(&bar_full_x[s]), 1);
+      mbar_init(smem_u32(&bar_full_y[s]), 2 * (MX_PRODUCERS / 32));
+      mbar_init(smem_u32(&bar_empty[s]), 1);
+    }
+    for (int s = 0; s < MX_WSTAGES; ++s) {
+      mbar_init(smem_u32(&bar_w_full[s]), 1);
+      mbar_init(smem_u32(&bar_w_empty[s]), MX_PRODUCERS / 32);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&bar_acc_full[b]), 1);
+      mbar_init(smem_u32(&bar_acc_empty[b]), 2 * 4);
+    }
+    mbar_init(smem_u32(&bar_done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2 && nkb > 0) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(MX_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();            // both CTAs' barriers initialised, TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  if (warp == 0) {
+    // ---------------- TMA: this CTA's X tile, completing on the leader's barrier
+    if (lane == 0 && nkb > 0) {
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % MP_STAGES, r = i / MP_STAGES;
+        if (!mbar_wait_cl(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 1)) break;
+        const uint32_t fb = mapa_u32(smem_u32(&bar_full_x[s]), 0);
+        if (leader) mbar_arrive_tx(smem_u32(&bar_full_x[s]), (peer_rows ? 2 : 1) * 2 * MX_TILE_X);
+        if (has_rows) {
+          const int64_t kx = (int64_t)(kb0 + i) * MX_BK;
+          tma_load_2d_pair(smem_u32(xh_s(s)), &tm_h, (int)kx, m0, fb);
+          tma_load_2d_pair(smem_u32(xl_s(s)), &tm_l, (int)kx, m0, fb);
+        }
+      }
+    }
+  } else if (warp == 3) {
+    // ---------------- weights ring (this CTA's producers)
+    if (lane == 0 && nkb > 0) {
+      int issued = 0;
+      for (int i = 0; i < nkb; ++i) {
+        const int ws = i % MX_WSTAGES, r = i / MX_WSTAGES;
+        if (!mbar_wait(smem_u32(&bar_w_empty[ws]), (r & 1) ^ 1, &s_abort, err, 10)) break;
+        const int64_t kx = (int64_t)(kb0 + i) * MX_BK;
+        const uint32_t wb = smem_u32(&bar_w_full[ws]);
+        mbar_arrive_tx(wb, n_om * MX_W_BYTES);
+        for (int j = 0; j < n_om; ++j)
+          bulk_load(smem_u32(w_s(ws, j)), wt32 + (size_t)(om0 + j) * P.K_pad + kx, MX_W_BYTES, wb);
+        issued = i + 1;
+      }
+      for (int i = max(0, issued - MX_WSTAGES); i < issued; ++i)
+        mbar_wait(smem_u32(&bar_w_full[i % MX_WSTAGES]), (i / MX_WSTAGES) & 1, nullptr, err, 6);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (leader only)
+    if (leader && lane == 0 && nkb > 0) {
+      const uint32_t idesc = idesc_bf16(2 * MX_BM, NB);
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % MP_STAGES, r = i / MP_STAGES;
+        const int ch = i / MX_CHUNK_KB, b = ch & 1;
+        const bool first = (i % MX_CHUNK_KB) == 0;
+        const bool last = (i % MX_CHUNK_KB) == MX_CHUNK_KB - 1 || i == nkb - 1;
+        if (first &&
+            !mbar_wait_cl(smem_u32(&bar_acc_empty[b]), ((ch >> 1) & 1) ^ 1, &s_abort, err, 7))
+          break;
+        if (!mbar_wait_cl(smem_u32(&bar_full_x[s]), r & 1, &s_abort, err, 2)) break;
+        if (!mbar_wait_cl(smem_u32(&bar_full_y[s]), r & 1, &s_abort, err, 3)) break;
+        tc_fence_after();
+        const uint64_t dxh = sw128_desc(smem_u32(xh_s(s)));
+        const uint64_t dxl = sw128_desc(smem_u32(xl_s(s)));
+        const uint64_t dyh = sw128_desc(smem_u32(yh_s(s)));
+        const uint64_t dyl = sw128_desc(smem_u32(yl_s(s)));
+        const uint32_t d = tmem + (uint32_t)(b * MX_ACC_COLS);
+#pragma unroll
+        for (int kk = 0; kk < MX_BK / 16; ++kk) {
+          const uint64_t koff = (uint64_t)(kk * 32) >> 4;
+          umma_pair(d, dxh + koff, dyh + koff, idesc, (first && kk == 0) ? 0u : 1u);
+          umma_pair(d, dxh + koff, dyl + koff, idesc, 1u);
+          umma_pair(d, dxl + koff, dyh + koff, idesc, 1u);
+        }
+        umma_pair_commit(smem_u32(&bar_empty[s]));
+        if (last) umma_pair_commit(smem_u32(&bar_acc_full[b]));
+      }
+      umma_pair_commit(smem_u32(&bar_done));
+    }
+  } else if (warp >= 4 && warp < MX_DRAIN0) {
+    // ---------------- producers: this CTA's 32 alphas x 8 k-chunks, both omegas
+    const int pt = tid - 128;
+    const int al = pt >> 3, c = pt & 7;
+    const size_t a = (size_t)(ah0 + al);
+    const __nv_bfloat16* rows_u[4] = {Xh + a * P.K_pad, Xl + a * P.K_pad,
+                                      Xh + (P.Npad + a) * P.K_pad, Xl + (P.Npad + a) * P.K_pad};
+    uint4 pre[4];
+    auto prefetch = [&](int i) {
+      const int64_t kb = (int64_t)(kb0 + i) * MX_BK;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        pre[q] = __ldg(reinterpret_cast<const uint4*>(rows_u[q] + kb + c * 8));
+    };
+    const uint32_t offr = sw128_off(2 * al, c), offi = sw128_off(2 * al + 1, c);
+    if (nkb > 0) prefetch(0);
+    for (int i = 0; i < nkb; ++i) {
+      const int s = i % MP_STAGES, r = i / MP_STAGES;
+      if (!__all_sync(0xffffffffu, mbar_wait_cl(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort,
+                                                err, 4)))
+        break;
+      const int ws = i % MX_WSTAGES;
+      if (!__all_sync(0xffffffffu, mbar_wait(smem_u32(&bar_w_full[ws]), (i / MX_WSTAGES) & 1,
+                                             &s_abort, err, 8)))
+        break;
+      float wr[8], wi[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t ah = (&pre[0].x)[q], all = (&pre[1].x)[q];
+        const uint32_t bh = (&pre[2].x)[q], bl = (&pre[3].x)[q];
+        wr[2 * q] = bf_lo(ah) + bf_lo(all);
+        wr[2 * q + 1] = bf_hi(ah) + bf_hi(all);
+        wi[2 * q] = bf_lo(bh) + bf_lo(bl);
+        wi[2 * q + 1] = bf_hi(bh) + bf_hi(bl);
+      }
+#pragma unroll
+      for (int j = 0; j < MX_OMEGA; ++j) {
+        if (j >= n_om) break;
+        const float4* wz = reinterpret_cast<const float4*>(w_s(ws, j)) + c;
+        float4 w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[q] = wz[8 * q];
+        uint32_t rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float ur0 = __fmaf_rn(w[q].x, wr[2 * q], __fmul_rn(w[q].y, wi[2 * q]));
+          const float ui0 = __fmaf_rn(w[q].y, wr[2 * q], -__fmul_rn(w[q].x, wi[2 * q]));
+          const float ur1 = __fmaf_rn(w[q].z, wr[2 * q + 1], __fmul_rn(w[q].w, wi[2 * q + 1]));
+          const float ui1 = __fmaf_rn(w[q].w, wr[2 * q + 1], -__fmul_rn(w[q].z, wi[2 * q + 1]));
+          rh[q] = pack_split(ur0, ur1, rl[q]);
+          ih[q] = pack_split(ui0, ui1, il[q]);
+        }
+        // rows omega 64 + 2 alpha + part: omega j's block starts 8 swizzle atoms on
+        const uint32_t ob = (uint32_t)j * 8 * 1024;
+        *reinterpret_cast<uint4*>(yh_s(s) + ob + offr) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+        *reinterpret_cast<uint4*>(yl_s(s) + ob + offr) = make_uint4(rl[0], rl[1], rl[2], rl[3]);
+        *reinterpret_cast<uint4*>(yh_s(s) + ob + offi) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+        *reinterpret_cast<uint4*>(yl_s(s) + ob + offi) = make_uint4(il[0], il[1], il[2], il[3]);
+      }
+      fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(smem_u32(&bar_w_empty[ws]));
+        if (leader) mbar_arrive(smem_u32(&bar_full_y[s]));
+        else mbar_arrive_remote(mapa_u32(smem_u32(&bar_full_y[s]), 0));
+      }
+      if (i + 1 < nkb) prefetch(i + 1);
+    }
+  } else if (warp >= MX_DRAIN0) {
+    // ---------------- drain: this CTA's 128 rows x N columns -> FP64 partial
+    const int q = warp & 3;
+    const int row = m0 + q * 32 + lane;
+    const bool row_ok = row < R;
+    const size_t RR = (size_t)R;
+    for (int ch = 0; ch < max(nch, 1); ++ch) {
+      const int b = ch & 1;
+      bool ok = nkb > 0;
+      if (ok) ok = mbar_wait_cl(smem_u32(&bar_acc_full[b]), (ch >> 1) & 1, &s_abort, err, 9);
+      ok = __all_sync(0xffffffffu, ok);
+      if (nkb > 0 && !ok) break;
+      tc_fence_after();
+      for (int cc = 0; cc < NB / 32; ++cc) {
+        const int col0 = cc * 32;
+        const int h = col0 / half, n = col0 % half;
+        const int om = n / 64;
+        const int dcol = 2 * a0 + 64 * h + (n % 64);     // output column of TMEM column col0
+        uint32_t v[32];
+        if (nkb > 0) {
+          const uint32_t taddr =
+              tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * MX_ACC_COLS + col0);
+          TMEM_LD32(taddr, v);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        } else {
+#pragma unroll
+          for (int t = 0; t < 32; ++t) v[t] = 0u;
+        }
+        if (!row_ok) continue;
+        double* o = part + ((size_t)(om0 + om) * P.splits + split) * RR * RR + row +
+                    (size_t)dcol * RR;
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+          double old[16];
+          if (ch > 0) {
+#pragma unroll
+            for (int t = 0; t < 16; ++t) old[t] = o[(size_t)(16 * hh + t) * RR];
+          } else {
+#pragma unroll
+            for (int t = 0; t < 16; ++t) old[t] = 0.0;
+          }
+#pragma unroll
+          for (int t = 0; t < 16; ++t)
+            o[(size_t)(16 * hh + t) * RR] = old[t] + (double)__uint_as_float(v[16 * hh + t]);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (nkb > 0 && lane == 0) {
+        if (leader) mbar_arrive(smem_u32(&bar_acc_empty[b]));
+        else mbar_arrive_remote(mapa_u32(smem_u32(&bar_acc_empty[b]), 0));
+      }
+    }
+  }
+  __syncwarp();
+  // every MMA of the pair has completed (bounded; ignores abort)
+  if (warp == 2 && nkb > 0) mbar_wait_cl(smem_u32(&bar_done), 0, nullptr, err, 5);
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();            // no CTA leaves while its peer may still touch it
+  if (warp == 2 && nkb > 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(MX_TMEM_COLS));
+  }
+}
+
 // ---- reduction of the FP64 partial tiles -----------------------------------------
 __device__ __forceinline__ void mixed_reduce_body(int Na, int Npad, int splits, double G,
                                                   const double* __restrict__ Nk,
@@ -965,6 +1334,7 @@ struct kls_mixed {
   size_t wt32_elems = 0;
   int* err = nullptr;
   int splits = 1;
+  int form = KLS_MIXED_ONE_CTA;   // contraction kernel: one CTA or a CTA pair per tile
 };
 
 static int mixed_splits(const kls_ctx* c) {
@@ -1022,6 +1392,8 @@ int kls_mixed_prepare(kls_ctx* c) {
   m->splits = mixed_splits(c);
   KLS_CK(c, cudaFuncSetAttribute(mixed_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)MX_SMEM));
+  KLS_CK(c, cudaFuncSetAttribute(mixed_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)MP_SMEM));
   KLS_CK(c, cudaStreamSynchronize(c->stream));
   return KLS_OK;
 }
@@ -1048,6 +1420,23 @@ int kls_mixed_contract(kls_ctx* c, int n, int) {
   weights32_kernel<<<(unsigned)std::min<size_t>((nw + 255) / 256, 4096), 256, 0, c->stream>>>(
       (int64_t)nw, c->d_wt, m->wt32);
   KLS_LAUNCHED(c);
+  if (m->form == KLS_MIXED_PAIR) {
+    PairParams Q{};
+    Q.Npad = c->Na_pad;
+    Q.rows = (int)R;
+    Q.K_pad = c->K_pad;
+    Q.nkb_total = (int)(c->K_pad / MX_BK);
+    Q.splits = m->splits;
+    Q.kb_per_split = (Q.nkb_total + m->splits - 1) / m->splits;
+    Q.n_omega = n;
+    Q.tiles_a = c->Na_pad / MX_AB;
+    const int row_pairs = (int)((R + 2 * MX_BM - 1) / (2 * MX_BM));
+    dim3 grid((unsigned)(2 * row_pairs * Q.tiles_a), m->splits, (n + MX_OMEGA - 1) / MX_OMEGA);
+    mixed_pair_kernel<<<grid, MX_THREADS, MP_SMEM, c->stream>>>(m->tm_h, m->tm_l, Q, m->Xh, m->Xl,
+                                                                m->wt32, m->part, m->err);
+    KLS_LAUNCHED(c);
+    return KLS_OK;
+  }
   MixedParams P{};
   P.Npad = c->Na_pad;
   P.rows = (int)R;
@@ -1127,6 +1516,14 @@ int kls_mixed_slots(int device) {
 int kls_mixed_splits_of(const kls_ctx* c) { return c->mixed ? c->mixed->splits : 0; }
 
 int kls_mixed_default_splits(const kls_ctx* c) { return mixed_splits(c); }
+
+int kls_mixed_set_form(kls_ctx* c, int form) {
+  if (!c->mixed) return KLS_ERR_STATE;
+  c->mixed->form = form;
+  return KLS_OK;
+}
+
+int kls_mixed_form_of(const kls_ctx* c) { return c->mixed ? c->mixed->form : 0; }
 
 int kls_mixed_set_splits(kls_ctx* c, int splits) {
   if (!c->mixed) return KLS_ERR_STATE;
