@@ -11,7 +11,8 @@ from .config import (CPUConfig, GPUConfig, GridConfig, IOConfig, KalnajsConfig, 
 from .api import (DevicePrecomputed, GPUType, NewtonResult, OrbitData, PrecomputedData,
                   ModelBatch, ToomreZangModel, TuneResult, autotune, build_M_matrix, compute_determinant,
                   compute_determinant_batched, create_toomre_zang_model, detect_gpu_type,
-                  find_minimum, grid_scan, grid_scan_distributed, newton_search, precompute_all, release_fp64,
+                  compute_determinant_ksharded, find_minimum, grid_scan, grid_scan_distributed,
+                  harmonic_ranges, precompute_ksharded, newton_search, precompute_all, release_fp64,
                   to_device)
 from ._lib import KLS_MODE_FP64, KLS_MODE_MIXED, KlsError
 
@@ -24,4 +25,5 @@ __all__ = [
     "DevicePrecomputed", "to_device", "compute_determinant", "compute_determinant_batched",
     "build_M_matrix", "grid_scan", "find_minimum", "newton_search", "NewtonResult", "KlsError",
     "KLS_MODE_FP64", "KLS_MODE_MIXED", "ModelBatch", "autotune", "TuneResult", "release_fp64", "grid_scan_distributed",
+    "harmonic_ranges", "precompute_ksharded", "compute_determinant_ksharded",
 ]

@@ -484,6 +484,74 @@ def grid_scan_distributed(config: KalnajsConfig, precomputed: Optional[Precomput
     return det_grid, Op0, g0
 
 
+def harmonic_ranges(l_min: int, l_max: int, n_ranks: int) -> List[Tuple[int, int]]:
+    """Contiguous (l_lo, l_hi) harmonic slices, inclusive; the first
+    n_l % n_ranks slices one harmonic wider."""
+    n_l = l_max - l_min + 1
+    per, rem = divmod(n_l, n_ranks)
+    out, lo = [], l_min
+    for r in range(n_ranks):
+        hi = lo + per + (1 if r < rem else 0) - 1
+        out.append((lo, hi))
+        lo = hi + 1
+    return out
+
+
+def precompute_ksharded(config: KalnajsConfig, group=None, device: Optional[int] = None
+                        ) -> PrecomputedData:
+    """This rank's slice of the W table: the harmonics harmonic_ranges(...)[rank]
+    (K sharding: the contraction over k = (orbit, l) is a sum, so the slices'
+    partial M(omega) add up to M(omega))."""
+    import torch
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    lo, hi = harmonic_ranges(config.grid.l_min, config.grid.l_max, world)[rank]
+    c = copy_config(config)
+    c.grid.l_min, c.grid.l_max = lo, hi
+    dev = torch.cuda.current_device() if device is None else device
+    return precompute_all(c, device=dev)
+
+
+def compute_determinant_ksharded(omegas: Sequence[complex], config: KalnajsConfig,
+                                 precomputed: Optional[PrecomputedData] = None,
+                                 devprecomp: Optional[DevicePrecomputed] = None, group=None,
+                                 M_fn=None, det_fn=None) -> np.ndarray:
+    """det(I - M(omega)) with the W table split over the ranks by harmonic.
+
+    Every rank forms its partial M(omega) (``M_fn``, default: build_M_matrix on
+    its slice from precompute_ksharded), one all_reduce (sum) of the
+    [n, N_alpha, N_alpha] complex partials gives M on every rank, and the
+    determinant is taken on the device (``det_fn``, default: the library's
+    LU through kls_det_lu_static).  The reference's 2-GPU split
+    (NL_julia_gpu.jl:313-378) loops every GPU over all harmonics; here each
+    harmonic is contracted once.
+    """
+    import torch
+    import torch.distributed as dist
+    om = np.asarray(omegas, dtype=np.complex128).reshape(-1)
+    if M_fn is None:
+        M_fn = lambda w: build_M_matrix(w, precomputed, devprecomp)
+    M = np.stack([np.asarray(M_fn(w), dtype=np.complex128) for w in om])
+    dev = torch.device("cuda", torch.cuda.current_device()) \
+        if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    t = torch.view_as_real(torch.from_numpy(np.ascontiguousarray(M))).to(dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    Mt = torch.view_as_complex(t.contiguous()).cpu().numpy()
+    A = np.eye(M.shape[1])[None, :, :] - Mt
+    if det_fn is not None:
+        return np.array([det_fn(a) for a in A])
+    lib = _lib.load()
+    n, N = A.shape[0], A.shape[1]
+    # row-major I - M on the device for the library's LU
+    dA = torch.view_as_real(torch.from_numpy(np.ascontiguousarray(A))).to("cuda").contiguous()
+    dd = torch.empty((n, 2), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    check(None, lib.kls_det_lu_static(C.c_void_p(dA.data_ptr()), n, N, C.c_void_p(dd.data_ptr()),
+                                      C.c_void_p(None), C.c_void_p(stream)))
+    d = dd.cpu().numpy()
+    return d[:, 0] + 1j * d[:, 1]
+
+
 def column_ranges(n_Op: int, n_gpus: int) -> List[slice]:
     """Contiguous column blocks, the first n_Op % n_gpus one wider (GridScan.jl:133-144)."""
     per, rem = divmod(n_Op, n_gpus)

@@ -1,4 +1,5 @@
-"""Omega-sharded grid scan over processes (gloo, world size 2, CPU).
+"""Omega-sharded grid scan and K-sharded determinants over processes (gloo,
+world size 2, CPU).
 
 The host logic of api.grid_scan_distributed (column split as in
 GridScan.jl:133-144, one all_gather of the det blocks, column-major argmin)
@@ -64,11 +65,36 @@ def _rank(rank, world, port, fail_rank, q):
                 pass
 
 
-def _run(world, fail_rank=-1):
+def _rank_k(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=8))
+    try:
+        pc = O.precompute_all(O.OracleConfig(**BASE))
+        lo, hi = K.harmonic_ranges(BASE["l_min"], BASE["l_max"], world)[rank]
+        il = range(lo - BASE["l_min"], hi - BASE["l_min"] + 1)     # this rank's harmonics
+        d = K.compute_determinant_ksharded(
+            OMEGAS, _config(), M_fn=lambda w: O.build_M(pc, w, l_range=il),
+            det_fn=lambda a: np.linalg.det(a))
+        q.put((rank, "ok", d, None, None))
+    except Exception as e:
+        q.put((rank, "error", repr(e), None, None))
+    finally:
+        dist.destroy_process_group()
+
+
+OMEGAS = [0.88 + 0.12j, 0.6 + 0.05j, 1.2 + 0.3j]
+
+
+def _run(world, fail_rank=-1, target=None):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    ps = [ctx.Process(target=_rank, args=(r, world, port, fail_rank, q)) for r in range(world)]
+    if target is None:
+        ps = [ctx.Process(target=_rank, args=(r, world, port, fail_rank, q)) for r in range(world)]
+    else:
+        ps = [ctx.Process(target=target, args=(r, world, port, q)) for r in range(world)]
     for p in ps:
         p.start()
     out = [q.get(timeout=120) for _ in range(world)]
@@ -102,3 +128,21 @@ def test_column_ranges_split_like_the_reference():
     r = K.api.column_ranges(41, 3)
     assert [(x.start, x.stop) for x in r] == [(0, 14), (14, 28), (28, 41)]
     assert [x.stop - x.start for x in K.api.column_ranges(5, 2)] == [3, 2]
+
+
+def test_k_sharded_determinant_equals_the_full_one():
+    """Each rank contracts only its harmonics; the all-reduced M gives the
+    full determinant (to the FP64 rounding of a regrouped sum)."""
+    res = _run(2, target=_rank_k)
+    pc = O.precompute_all(O.OracleConfig(**BASE))
+    ref = np.array([O.compute_det(pc, w) for w in OMEGAS])
+    for rank, status, d, _, _ in res:
+        assert status == "ok", d
+        assert np.max(np.abs(d - ref) / np.abs(ref)) < 1e-12, (rank, d, ref)
+
+
+def test_harmonic_ranges_cover_each_harmonic_once():
+    r = K.harmonic_ranges(-100, 100, 8)
+    ls = [l for lo, hi in r for l in range(lo, hi + 1)]
+    assert ls == list(range(-100, 101))
+    assert [hi - lo + 1 for lo, hi in r] == [26] + [25] * 7

@@ -140,3 +140,27 @@ def test_release_fp64_keeps_mixed(lib_path):
     mb.close()
     assert np.array_equal(d[0], after)
     pc.close()
+
+
+def test_ksharded_path_on_one_rank(lib_path):
+    """The K-sharded determinant path (partial M per rank, all_reduce, device
+    LU) on a single rank equals the one-context determinant."""
+    import datetime
+    import os
+    import socket
+    import torch.distributed as dist
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=0, world_size=1, timeout=datetime.timedelta(seconds=30))
+    try:
+        c = configs()[0]
+        pc = K.precompute_ksharded(c, device=0)
+        om = omegas(3, 31)
+        d = K.compute_determinant_ksharded(om, c, pc)
+        ref = K.compute_determinant_batched(om, pc)
+        pc.close()
+    finally:
+        dist.destroy_process_group()
+    assert np.max(np.abs(d - ref) / np.abs(ref)) < 1e-12, np.abs(d - ref) / np.abs(ref)
