@@ -373,7 +373,7 @@ def time_to_root(args, K, P, cfg, pc, local, sync):
     dOp, dg = abs(rh.Omega_p - r64.Omega_p), abs(rh.gamma - r64.gamma)
     plain_total = t_scan64 + t_n64
     if args.heldout > 0:
-        out["heldout"] = heldout_eval(args, K, P, mlp, cfg, args.heldout,
+        out["heldout"] = heldout_eval(args, K, P, cfg, args.heldout,
                                       t_scan64 / (s.n_Op * s.n_gamma), local, sync)
     mlp.close()
     learned_total = t_prop + t_hyb
@@ -405,9 +405,30 @@ def time_to_root(args, K, P, cfg, pc, local, sync):
 # Newton against the scan-started FP64 Newton (the scan argmin taken from the
 # split-BF16 scan and confirmed by FP64 determinants of its 5 best points)
 # ---------------------------------------------------------------------------
-def heldout_eval(args, K, P, mlp, base_cfg, n_models: int, t_fp64_det: float, local, sync):
+def polish(K, cfg, pc, Op, g, steps: int = 2):
+    """FP64 Newton steps from (Op, g) past the |det| < tol test: the stopping
+    rule pins a root only to tol / |det'|, which for flat determinants is far
+    above 1e-10; two more steps pin it to the FP64 noise."""
+    c = K.config.copy_config(cfg)
+    c.newton.tol = 0.0
+    c.newton.max_iter = steps
+    r = K.newton_search(c, pc, None, K.GPUType.NVIDIA, "Float64", Op, g)
+    return r.Omega_p, r.gamma
+
+
+def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, sync):
     import numpy as np
     from kalnajs_log_spirals_b200.api import newton_search_hybrid
+    # the network for this size: trained on batched split-BF16 scans of 64
+    # seeded models at the default size (8 models per batch)
+    t0 = time.perf_counter()
+    X, T = P.scan_samples(base_cfg, P.random_models(64, seed=2024), n_Op=32, n_gamma=16,
+                          batch=16, chunk=8, device=local)
+    t_gen = time.perf_counter() - t0
+    mlp = P.MLP(256, 4, seed=0, device=local)
+    t0 = time.perf_counter()
+    hist = mlp.train(X, T, epochs=300, batch=1024, lr=1e-3, seed=0)
+    t_train = time.perf_counter() - t0
     specs = P.random_models(n_models, seed=7)
     rows = []
     for sp in specs:
@@ -437,10 +458,13 @@ def heldout_eval(args, K, P, mlp, base_cfg, n_models: int, t_fp64_det: float, lo
             Op_range=(s.Omega_p_min, s.Omega_p_max), g_range=(s.gamma_min, s.gamma_max))
         rh = newton_search_hybrid(cfg, pc, Op_p, g_p)
         t_learned = time.perf_counter() - t0
-        pc.close()
         growing = bool(r64.converged and r64.gamma > 1e-4)
-        same = bool(growing and rh.converged and abs(rh.Omega_p - r64.Omega_p) <= 1e-10
-                    and abs(rh.gamma - r64.gamma) <= 1e-10)
+        same = False
+        if growing and rh.converged:
+            a, b = polish(K, cfg, pc, r64.Omega_p, r64.gamma), polish(K, cfg, pc, rh.Omega_p,
+                                                                      rh.gamma)
+            same = abs(a[0] - b[0]) <= 1e-10 and abs(a[1] - b[1]) <= 1e-10
+        pc.close()
         rows.append({"n_zang": sp.n_zang, "q1": sp.q1, "m": sp.m, "growing_mode": growing,
                      "same_root": same, "start_equals_scan_argmin": (Op_p, g_p) == (Op0, g0),
                      "plain_fp64_s": s.n_Op * s.n_gamma * t_fp64_det + t_n64,
@@ -449,7 +473,14 @@ def heldout_eval(args, K, P, mlp, base_cfg, n_models: int, t_fp64_det: float, lo
     grow = [r for r in rows if r["growing_mode"]]
     ok = [r for r in grow if r["same_root"]]
     mean = lambda k, rs: float(np.mean([r[k] for r in rs])) if rs else None
+    mlp.close()
     return {"models": n_models, "model_seed": 7, "size": "default (NR=501 Ne=51 N_alpha=301 l=+-100)",
+            "training": {"samples": int(X.shape[0]), "models": 64, "model_seed": 2024,
+                         "grid": "32 x 16 over Omega_p [0.2, 0.8], gamma [0.01, 0.30]",
+                         "size": "default", "sample_gen_s": t_gen, "train_s": t_train,
+                         "epochs": 300, "loss_first_last": [float(hist[0]), float(hist[-1])]},
+            "same_root_rule": "both roots polished by 2 FP64 Newton steps, then |dOmega_p|, "
+                              "|dgamma| <= 1e-10",
             "with_growing_mode": len(grow), "same_root_within_1e-10": len(ok),
             "success_rate": len(ok) / len(grow) if grow else None,
             "mean_time_to_root_s": {"plain_fp64 (scan at the measured FP64 det time)":

@@ -436,6 +436,8 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
           wi[u][2 * q] = bf_lo(bh) + bf_lo(bl);
           wi[u][2 * q + 1] = bf_hi(bh) + bf_hi(bl);
         }
+      // the next k-block's rows load while this one's U is formed and stored
+      if (i + 1 < nkb) prefetch(i + 1);
       const int c = c_u[0];
       // weights of k = 2q, 2q+1 of the chunk, both omegas loaded up front
       float4 wq[MX_OMEGA][4];
@@ -483,7 +485,6 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
         mbar_arrive(smem_u32(&bar_w_empty[ws]));
         mbar_arrive(smem_u32(&bar_full_y[s]));
       }
-      if (i + 1 < nkb) prefetch(i + 1);
     }
   } else if (warp >= MX_DRAIN0) {
     // ---------------- drain: TMEM chunk -> FP64 partial (row per thread)
@@ -534,13 +535,13 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
     }
   }
   __syncwarp();
-  // all MMAs have completed before TMEM is released (bounded; ignores abort)
-  if (warp == 2 && nkb > 0) {
-    mbar_wait(smem_u32(&bar_done), 0, nullptr, err, 5);
-  }
   tc_fence_before();
   __syncthreads();
+  // every role has finished; all MMAs complete before TMEM is released
+  // (bounded, ignores abort; the wait starts only now, so its bound does not
+  // depend on how long the CTA worked)
   if (warp == 2 && nkb > 0) {
+    mbar_wait(smem_u32(&bar_done), 0, nullptr, err, 5);
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(MX_TMEM_COLS));
@@ -904,10 +905,11 @@ mixed_pair_kernel(const __grid_constant__ CUtensorMap tm_h, const __grid_constan
     }
   }
   __syncwarp();
-  // every MMA of the pair has completed (bounded; ignores abort)
-  if (warp == 2 && nkb > 0) mbar_wait_cl(smem_u32(&bar_done), 0, nullptr, err, 5);
   tc_fence_before();
   __syncthreads();
+  // every role has finished; every MMA of the pair completes (bounded from
+  // now, ignores abort) before the cluster barrier that both CTAs leave by
+  if (warp == 2 && nkb > 0) mbar_wait_cl(smem_u32(&bar_done), 0, nullptr, err, 5);
   cluster_sync_all();            // no CTA leaves while its peer may still touch it
   if (warp == 2 && nkb > 0) {
     tc_fence_after();
@@ -1307,10 +1309,12 @@ mixed_multi_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict_
     }
   }
   __syncwarp();
-  if (warp == 2 && any) mbar_wait(smem_u32(&bar_done), 0, nullptr, err, 5);
   tc_fence_before();
   __syncthreads();
+  // the wait for the last commit starts after every role has finished: a
+  // persistent CTA may work for longer than any single wait's bound
   if (warp == 2 && any) {
+    mbar_wait(smem_u32(&bar_done), 0, nullptr, err, 5);
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(MX_TMEM_COLS));

@@ -152,19 +152,32 @@ def model_config(base: KalnajsConfig, spec: ModelSpec) -> KalnajsConfig:
 
 def scan_samples(base: KalnajsConfig, specs: Sequence[ModelSpec], n_Op: int, n_gamma: int,
                  Op_range=(0.2, 0.8), g_range=(0.01, 0.30), mixed: bool = True,
-                 device: int = 0, batch: int = 16):
-    """Features and targets of every (model, omega) point of one batched scan
-    over all models (api.ModelBatch: every pass is one persistent launch over
-    the uneven batch)."""
+                 device: int = 0, batch: int = 16, chunk: int = 0):
+    """Features and targets of every (model, omega) point of batched scans
+    over the models (api.ModelBatch: every pass is one launch over the uneven
+    batch).  ``chunk`` > 0 scans that many models per batch, with mixed-only
+    contexts (FP64 tables released), so that many large models fit one GPU."""
     from . import api
-    pcs = [api.precompute_all(model_config(base, s), device=device) for s in specs]
-    try:
-        mb = api.ModelBatch(pcs, "Float32" if mixed else "Float64", batch=batch)
-        d, la, _, _ = mb.scan(n_Op, n_gamma, Op_range, g_range)   # [n_models, n_gamma, n_Op]
-        mb.close()
-    finally:
-        for pc in pcs:
-            pc.close()
+    groups = [list(specs)] if chunk <= 0 else [list(specs[i:i + chunk])
+                                              for i in range(0, len(specs), chunk)]
+    ds, las = [], []
+    for group in groups:
+        pcs = []
+        try:
+            for sp in group:
+                pc = api.precompute_all(model_config(base, sp), device=device)
+                pcs.append(pc)
+                if chunk > 0 and mixed:
+                    api.release_fp64(pc)
+            mb = api.ModelBatch(pcs, "Float32" if mixed else "Float64", batch=batch)
+            dd, ll, _, _ = mb.scan(n_Op, n_gamma, Op_range, g_range)  # [models, n_gamma, n_Op]
+            mb.close()
+            ds.append(dd)
+            las.append(ll)
+        finally:
+            for pc in pcs:
+                pc.close()
+    d, la = np.concatenate(ds), np.concatenate(las)
     Op = np.linspace(*Op_range, n_Op)
     gm = np.linspace(*g_range, n_gamma)
     OP, GM = np.meshgrid(Op, gm, indexing="xy")                   # [n_gamma, n_Op]
