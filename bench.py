@@ -773,6 +773,14 @@ def ours(args):
     if rank == 0 and not args.no_cpu:
         rate, threads, sample = cpu_det_rate(cfg)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
+        try:
+            # the reference's default thread count (configs/default.toml [cpu] max_threads = 4)
+            from threadpoolctl import threadpool_limits
+            with threadpool_limits(limits=4):
+                r4, _, s4 = cpu_det_rate(cfg, budget_s=8.0)
+            cpu["at_4_threads"] = {"value": r4, "cores": 4, "sample": s4}
+        except Exception as e:          # threadpoolctl missing: report why
+            cpu["at_4_threads"] = {"unavailable": repr(e)}
 
     if world > 1:
         import torch.distributed as dist
