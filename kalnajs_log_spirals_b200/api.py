@@ -43,7 +43,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import _lib
-from ._lib import KLS_MODE_FP64, KLS_MODE_MIXED, KlsError, check, dptr
+from ._lib import KLS_MODE_FP64, KLS_MODE_MIXED, check, dptr
 from .config import check_quadrature, KalnajsConfig, copy_config
 
 

@@ -15,7 +15,6 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
-import time
 from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
