@@ -65,6 +65,10 @@ def parse():
                     help="skip the reference GPU algorithm (cuBLAS ZGEMM per harmonic) arm")
     ap.add_argument("--heldout", type=int, default=0,
                     help="also judge the proposer on N held-out models at the default size")
+    ap.add_argument("--heldout-save", default="",
+                    help="save the held-out network's parameters (.npy) after training")
+    ap.add_argument("--heldout-params", default="",
+                    help="load the held-out network's parameters (.npy) instead of training")
     ap.add_argument("--uneven-passes", type=int, default=3)
     ap.add_argument("--uneven-batch", type=int, default=4)
     return ap.parse_args()
@@ -415,16 +419,25 @@ def polish(K, cfg, pc, Op, g, steps: int = 2):
 def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, sync):
     import numpy as np
     from kalnajs_log_spirals_b200.api import newton_search_hybrid
-    # the network for this size: trained on batched split-BF16 scans of 64
-    # seeded models at the default size (6 mixed-only models per batch)
-    t0 = time.perf_counter()
-    X, T = P.scan_samples(base_cfg, P.random_models(64, seed=2024), n_Op=32, n_gamma=16,
-                          batch=16, chunk=6, device=local)
-    t_gen = time.perf_counter() - t0
     mlp = P.MLP(256, 4, seed=0, device=local)
-    t0 = time.perf_counter()
-    hist = mlp.train(X, T, epochs=300, batch=1024, lr=1e-3, seed=0)
-    t_train = time.perf_counter() - t0
+    if args.heldout_params:
+        # parameters of an earlier training run of the same recipe
+        params = np.load(args.heldout_params)
+        mlp.set_params(params)
+        n_samples, t_gen, t_train, hist = None, 0.0, 0.0, [float("nan"), float("nan")]
+    else:
+        # the network for this size: trained on batched split-BF16 scans of 64
+        # seeded models at the default size (6 mixed-only models per batch)
+        t0 = time.perf_counter()
+        X, T = P.scan_samples(base_cfg, P.random_models(64, seed=2024), n_Op=32, n_gamma=16,
+                              batch=16, chunk=6, device=local)
+        t_gen = time.perf_counter() - t0
+        n_samples = int(X.shape[0])
+        t0 = time.perf_counter()
+        hist = mlp.train(X, T, epochs=300, batch=1024, lr=1e-3, seed=0)
+        t_train = time.perf_counter() - t0
+        if args.heldout_save:
+            np.save(args.heldout_save, mlp.params())
     specs = P.random_models(n_models, seed=7)
     rows = []
     for sp in specs:
@@ -471,7 +484,8 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
     mean = lambda k, rs: float(np.mean([r[k] for r in rs])) if rs else None
     mlp.close()
     return {"models": n_models, "model_seed": 7, "size": "default (NR=501 Ne=51 N_alpha=301 l=+-100)",
-            "training": {"samples": int(X.shape[0]), "models": 64, "model_seed": 2024,
+            "training": {"samples": n_samples, "models": 64, "model_seed": 2024,
+                         "from_file": bool(args.heldout_params),
                          "grid": "32 x 16 over Omega_p [0.2, 0.8], gamma [0.01, 0.30]",
                          "size": "default", "sample_gen_s": t_gen, "train_s": t_train,
                          "epochs": 300, "loss_first_last": [float(hist[0]), float(hist[-1])]},

@@ -188,7 +188,10 @@ int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cf
  * |det| < nc->tol on the plain FP64 determinant, holds):
  *   phase 1: Newton on split-BF16 determinants, the finite-difference triple
  *            (omega, omega + m*mixed_delta, omega + i*mixed_delta) evaluated
- *            as one batch, until a step is shorter than mixed_step_tol;
+ *            as one batch, until a step is shorter than mixed_step_tol or
+ *            |det| has not halved for 3 steps (the split form's noise floor;
+ *            its det error is ~5e-5 relative, so mixed_delta ~1e-3 keeps
+ *            the finite-difference Jacobian well above that noise);
  *   phase 2: FP64 determinant at the current point; stop if |det| < tol,
  *            else a chord step with the last Jacobian; the Jacobian is
  *            recomputed in FP64 (step nc->delta) when |det| falls by less

@@ -610,11 +610,16 @@ def newton_search(config: KalnajsConfig, precomputed: PrecomputedData,
 
 @dataclass
 class HybridConfig:
-    """Mixed-precision phase parameters of newton_search_hybrid."""
-    mixed_delta: float = 1e-5
+    """Mixed-precision phase parameters of newton_search_hybrid.
+
+    The split-BF16 determinant carries a ~5e-5 relative error, so the
+    finite-difference step of the mixed phase is 1e-3 (a Jacobian error of
+    ~5e-2 x the distance to the root, truncation ~1e-3); the FP64 phase may
+    take as many steps as the reference's Newton (max_iter 50)."""
+    mixed_delta: float = 1e-3
     mixed_step_tol: float = 1e-7
-    mixed_max_iter: int = 12
-    fp64_max_iter: int = 8
+    mixed_max_iter: int = 30
+    fp64_max_iter: int = 50
 
 
 def newton_search_hybrid(config: KalnajsConfig, precomputed: PrecomputedData,

@@ -601,11 +601,21 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
   double J[2][2] = {{0, 0}, {0, 0}};
   bool haveJ = false;
   const double dm = hc->mixed_delta;
+  double best = INFINITY;
+  int stall = 0;
   for (int it = 0; it < hc->mixed_max_iter; ++it) {
     double w[6] = {m * Op, g, m * (Op + dm), g, m * Op, g + dm}, d[6];
     if ((r = det_batch_host(c, w, 3, KLS_MODE_MIXED, d, nullptr))) return r;
     n_mixed += 3;
-    hist(std::hypot(d[0], d[1]));
+    const double a = std::hypot(d[0], d[1]);
+    hist(a);
+    // |det| no longer halving for 3 steps: the split form's noise floor
+    if (a < 0.5 * best) {
+      best = a;
+      stall = 0;
+    } else if (++stall >= 3) {
+      break;
+    }
     J[0][0] = (d[2] - d[0]) / dm; J[0][1] = (d[4] - d[0]) / dm;
     J[1][0] = (d[3] - d[1]) / dm; J[1][1] = (d[5] - d[1]) / dm;
     haveJ = true;
