@@ -192,10 +192,11 @@ int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cf
  *            |det| has not halved for 3 steps (the split form's noise floor;
  *            its det error is ~5e-5 relative, so mixed_delta ~1e-3 keeps
  *            the finite-difference Jacobian well above that noise);
- *   phase 2: FP64 determinant at the current point; stop if |det| < tol,
- *            else a chord step with the last Jacobian; the Jacobian is
- *            recomputed in FP64 (step nc->delta) when |det| falls by less
- *            than 10x per step.                                            */
+ *   phase 2: FP64 determinant at the current point; if |det| < tol, one
+ *            more chord step when it exceeds 1e-12 (kept if it lowers |det|),
+ *            then stop; else a chord step with the last Jacobian; the
+ *            Jacobian is recomputed in FP64 (step nc->delta) when |det| falls
+ *            by less than 10x per step.                                      */
 typedef struct kls_hybrid_cfg {
     double  mixed_delta;
     double  mixed_step_tol;

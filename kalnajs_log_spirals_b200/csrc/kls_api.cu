@@ -635,7 +635,28 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
     ++n_fp64;
     const double a = std::hypot(dl[0], dl[1]);
     hist(a);
-    if (a < tol) { converged = true; break; }
+    if (a < tol) {
+      converged = true;
+      // |det| < tol fixes the root only to tol / |det'|: quadratically
+      // converging FP64 Newton lands far below tol, a chord iteration just
+      // below it.  One more chord step when it is not negligible (> 1e-12),
+      // kept if it lowers |det|.
+      double F[2] = {dl[0], dl[1]}, x[2];
+      if (haveJ && solve2(J, F, x) && std::hypot(x[0], x[1]) > 1e-12) {
+        const double Op2 = std::min(std::max(Op - x[0], 0.0), 1.0);
+        const double g2 = std::max(g - x[1], 1e-4);
+        double w2[2] = {m * Op2, g2}, d2[2];
+        if ((r = det_batch_host(c, w2, 1, KLS_MODE_FP64, d2, nullptr))) return r;
+        ++n_fp64;
+        if (std::hypot(d2[0], d2[1]) < a) {
+          Op = Op2;
+          g = g2;
+          dl[0] = d2[0];
+          dl[1] = d2[1];
+        }
+      }
+      break;
+    }
     if (!haveJ || a > 0.1 * prev) {
       // Jacobian in FP64 (NewtonSolver.jl:98-109), FD pair in one batch
       double w2[4] = {m * (Op + nc->delta), g, m * Op, g + nc->delta}, d2[4];
