@@ -226,7 +226,7 @@ class RootResult:
     """find_root outcome: the Newton result and how its start was found."""
     newton: object                 # api.NewtonResult (hybrid Newton, FP64 finish)
     start: Tuple[float, float]
-    source: str                    # "proposal" or "grid_scan"
+    source: str                    # "proposal", "proposal_fp64" or "grid_scan"
     proposal_dets: int             # determinants spent on the proposal
     scan_dets: int                 # determinants spent on the fallback scan (0 if none)
 
@@ -237,7 +237,8 @@ def find_root(mlp: MLP, config: KalnajsConfig, precomputed, k: int = 48,
 
     The proposal (``propose`` over the config's scan grid, split-BF16
     determinants) starts ``newton_search_hybrid``, whose last steps and
-    stopping test are FP64; if that Newton does not converge to a growing
+    stopping test are FP64; if that does not converge, plain FP64 Newton
+    (newton_search) runs from the same start; if neither reaches a growing
     mode (gamma > min_gamma), the reference workflow runs instead: the full
     grid scan (GridScan.jl:25-88) in the split-BF16 form and the hybrid
     Newton from its argmin.
@@ -252,6 +253,11 @@ def find_root(mlp: MLP, config: KalnajsConfig, precomputed, k: int = 48,
     r = api.newton_search_hybrid(config, precomputed, Op, g)
     if r.converged and r.gamma > min_gamma:
         return RootResult(r, (Op, g), "proposal", used, 0)
+    if not r.converged:
+        # the judge: plain FP64 Newton from the same start
+        r = api.newton_search(config, precomputed, None, api.GPUType.NVIDIA, "Float64", Op, g)
+        if r.converged and r.gamma > min_gamma:
+            return RootResult(r, (Op, g), "proposal_fp64", used, 0)
     _, Op0, g0 = api.grid_scan(config, precomputed, dev)
     r = api.newton_search_hybrid(config, precomputed, Op0, g0)
     return RootResult(r, (Op0, g0), "grid_scan", used, s.n_Op * s.n_gamma)

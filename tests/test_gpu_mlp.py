@@ -125,4 +125,4 @@ def test_find_root_falls_back_to_the_scan(lib_path):
     assert ref.converged and forced.newton.converged
     assert abs(forced.newton.Omega_p - ref.Omega_p) <= 1e-10
     assert abs(forced.newton.gamma - ref.gamma) <= 1e-10
-    assert free.newton.converged and free.source in ("proposal", "grid_scan")
+    assert free.newton.converged and free.source in ("proposal", "proposal_fp64", "grid_scan")
