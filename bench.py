@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--no-refgpu", action="store_true",
                     help="skip the reference GPU algorithm (cuBLAS ZGEMM per harmonic) arm")
     ap.add_argument("--heldout", type=int, default=0,
-                    help="also judge the proposer on N held-out models at the default size")
+                    help="also evaluate the proposer on N held-out models at the default size")
     ap.add_argument("--heldout-save", default="",
                     help="save the held-out network's parameters (.npy) after training")
     ap.add_argument("--heldout-params", default="",

@@ -254,7 +254,7 @@ def find_root(mlp: MLP, config: KalnajsConfig, precomputed, k: int = 48,
     if r.converged and r.gamma > min_gamma:
         return RootResult(r, (Op, g), "proposal", used, 0)
     if not r.converged:
-        # the judge: plain FP64 Newton from the same start
+        # the arbiter: plain FP64 Newton from the same start
         r = api.newton_search(config, precomputed, None, api.GPUType.NVIDIA, "Float64", Op, g)
         if r.converged and r.gamma > min_gamma:
             return RootResult(r, (Op, g), "proposal_fp64", used, 0)
