@@ -2,7 +2,8 @@
 # package's API (src/KalnajsLogSpiral.jl:23-43).  It reuses the reference's
 # Configuration module for TOML parsing and replaces precompute_all,
 # to_device, compute_determinant(_batched), grid_scan and newton_search with
-# ccalls into libkls.so (include/kls.h).  Not exercised in this repository's
+# ccalls into libkls.so (include/kls.h), and adds newton_search_hybrid,
+# grid_scan_multi, autotune and release_fp64.  Not exercised in this repository's
 # tests (no Julia toolchain in the build image); the Python mirror in
 # kalnajs_log_spirals_b200/api.py calls the same entry points.
 module KalnajsLogSpiralB200
@@ -139,6 +140,98 @@ function newton_search(config, precomp::PrecomputedData, devprecomp, gpu_type, T
     h = permutedims(hist[:, 1:r.iterations])
     return NewtonResult{Float64}(r.Omega_p, r.gamma, complex(r.omega_re, r.omega_im),
                                  complex(r.det_re, r.det_im), r.iterations, r.converged != 0, h)
+end
+
+# ---- beyond the reference's API --------------------------------------------
+
+struct KlsHybridCfg
+    mixed_delta::Float64; mixed_step_tol::Float64; mixed_max_iter::Int32; fp64_max_iter::Int32
+end
+
+struct KlsTuneResult
+    mode::Int32; splits::Int32; default_splits::Int32; candidates::Int32
+    ms_per_omega::Float64; default_ms_per_omega::Float64; form::Int32
+end
+
+"""
+newton_search_hybrid: split-BF16 Newton, then FP64 chord steps to the
+reference's stopping rule |det| < tol on the plain FP64 determinant
+(kls_newton_hybrid).  Keyword defaults are the library's recommended ones.
+"""
+function newton_search_hybrid(config, precomp::PrecomputedData, Omega_p_init::Real,
+                              gamma_init::Real; mixed_delta::Real=1e-3,
+                              mixed_step_tol::Real=1e-7, mixed_max_iter::Integer=30,
+                              fp64_max_iter::Integer=50)
+    n = config.newton
+    check(precomp.handle, ccall((:kls_prepare_mixed, LIBKLS), Cint, (Ptr{Cvoid},), precomp.handle))
+    nc = Ref(KlsNewtonCfg(n.max_iter, n.tol, n.delta, n.use_line_search, n.max_line_search,
+                          KLS_MODE_FP64))
+    hc = Ref(KlsHybridCfg(mixed_delta, mixed_step_tol, mixed_max_iter, fp64_max_iter))
+    res = Ref(KlsNewtonResult())
+    evals = zeros(Int32, 2)
+    hist = zeros(Float64, 3, n.max_iter)
+    check(precomp.handle, ccall((:kls_newton_hybrid, LIBKLS), Cint,
+          (Ptr{Cvoid}, Cdouble, Cdouble, Ref{KlsNewtonCfg}, Ref{KlsHybridCfg},
+           Ref{KlsNewtonResult}, Ptr{Int32}, Ptr{Float64}),
+          precomp.handle, Omega_p_init, gamma_init, nc, hc, res, evals, hist))
+    r = res[]
+    h = permutedims(hist[:, 1:min(r.iterations, n.max_iter)])
+    return NewtonResult{Float64}(r.Omega_p, r.gamma, complex(r.omega_re, r.omega_im),
+                                 complex(r.det_re, r.det_im), r.iterations, r.converged != 0, h)
+end
+
+"autotune: K split count (and the split-BF16 tile form) chosen by timing (kls_autotune)."
+function autotune(precomp::PrecomputedData, Tgpu::Type; batch::Integer=2)
+    mode = Tgpu === Float64 ? KLS_MODE_FP64 : KLS_MODE_MIXED
+    r = Ref{KlsTuneResult}()
+    check(precomp.handle, ccall((:kls_autotune, LIBKLS), Cint,
+          (Ptr{Cvoid}, Cint, Cint, Ref{KlsTuneResult}), precomp.handle, mode, batch, r))
+    return r[]
+end
+
+"release_fp64: keep only the split-BF16 table of a precompute (kls_release_fp64)."
+release_fp64(precomp::PrecomputedData) =
+    check(precomp.handle, ccall((:kls_release_fp64, LIBKLS), Cint, (Ptr{Cvoid},), precomp.handle))
+
+function multi_error(h)
+    unsafe_string(ccall((:kls_multi_last_error, LIBKLS), Cstring, (Ptr{Cvoid},), h))
+end
+
+"""
+grid_scan_multi: grid_scan (GridScan.jl:25) of many precomputes (any sizes) in
+shared launches (kls_multi, kls_scan_multi).  Returns (det_grids
+[n_gamma, n_Op, n_models], Omega_p_init [n_models], gamma_init [n_models]).
+"""
+function grid_scan_multi(config, precomps::Vector{PrecomputedData}, Tgpu::Type;
+                         batch::Integer=16)
+    mode = Tgpu === Float64 ? KLS_MODE_FP64 : KLS_MODE_MIXED
+    if mode == KLS_MODE_MIXED
+        for p in precomps
+            check(p.handle, ccall((:kls_prepare_mixed, LIBKLS), Cint, (Ptr{Cvoid},), p.handle))
+        end
+    end
+    handles = Ptr{Cvoid}[p.handle for p in precomps]
+    mm = Ref{Ptr{Cvoid}}(C_NULL)
+    code = ccall((:kls_multi_create, LIBKLS), Cint,
+                 (Ptr{Ptr{Cvoid}}, Cint, Cint, Cint, Ref{Ptr{Cvoid}}),
+                 handles, length(handles), mode, batch, mm)
+    code == 0 || error("libkls status $code: " * multi_error(C_NULL))
+    s = config.scan
+    nm = length(precomps)
+    sc = Ref(KlsScanCfg(s.n_Op, s.n_gamma, s.Omega_p_min, s.Omega_p_max, s.gamma_min,
+                        s.gamma_max, mode, batch))
+    dets = Array{ComplexF64}(undef, s.n_gamma, s.n_Op, nm)   # column-major block per model
+    Op0 = zeros(Float64, nm)
+    g0 = zeros(Float64, nm)
+    try
+        code = ccall((:kls_scan_multi, LIBKLS), Cint,
+                     (Ptr{Cvoid}, Ref{KlsScanCfg}, Ptr{ComplexF64}, Ptr{Float64}, Ptr{Float64},
+                      Ptr{Float64}), mm[], sc, dets, C_NULL, Op0, g0)
+        code == 0 || error("libkls status $code: " * multi_error(mm[]))
+    finally
+        ccall((:kls_multi_destroy, LIBKLS), Cint, (Ptr{Cvoid},), mm[])
+    end
+    return dets, Op0, g0
 end
 
 end # module
