@@ -46,3 +46,47 @@ def test_random_models_are_seeded():
     b = P.random_models(5, 3)
     assert a == b
     assert all(2 <= s.n_zang <= 6 and 4 <= s.q1 <= 12 and s.m in (2, 3) for s in a)
+
+
+class _StubNet:
+    """Stands in for the device network: predicted log|det| = distance to a point."""
+
+    def __init__(self, Op, g):
+        self.Op, self.g = Op, g
+
+    def forward(self, X):
+        Op = X[:, 3] * 0.3 + 0.5               # undo features() for Omega_p, gamma
+        g = X[:, 4] * 0.145 + 0.155
+        d = np.hypot(Op - self.Op, g - self.g)
+        return np.stack([d, np.zeros_like(d), np.ones_like(d)], axis=1).astype(np.float32)
+
+
+def test_shortlist_takes_the_lowest_predictions_in_column_major_order():
+    spec = P.ModelSpec(4, 7.0, 2)
+    net = _StubNet(0.41, 0.07)
+    Op, g, idx = P.shortlist(net, spec, k=6)
+    assert list(idx) == sorted(idx) and len(idx) == 6
+    grid_Op = np.linspace(0.2, 0.6, 41)
+    grid_g = np.linspace(0.01, 0.2, 20)
+    # column-major index q -> (Op column q // n_gamma, gamma row q % n_gamma)
+    assert np.allclose(Op, grid_Op[idx // 20]) and np.allclose(g, grid_g[idx % 20])
+    # every shortlisted prediction is at most every prediction left out
+    y = net.forward(P.features(4, 7.0, 2, np.repeat(grid_Op, 20), np.tile(grid_g, 41)))[:, 0]
+    rest = np.setdiff1d(np.arange(41 * 20), idx)
+    assert y[idx].max() <= y[rest].min()
+
+
+def test_propose_picks_the_smallest_true_determinant_of_the_shortlist():
+    spec = P.ModelSpec(4, 7.0, 2)
+    net = _StubNet(0.41, 0.07)
+    calls = []
+
+    def det_fn(om):                                # a true root at Omega_p 0.42, gamma 0.06
+        calls.append(len(om))
+        return (om.real / 2 - 0.42) + 1j * (om.imag - 0.06)
+
+    Op, g, used = P.propose(net, spec, det_fn, k=12)
+    assert calls == [12] and used == 12
+    Ops, gs, _ = P.shortlist(net, spec, k=12)
+    best = np.argmin(np.abs((Ops - 0.42) + 1j * (gs - 0.06)))
+    assert (Op, g) == (float(Ops[best]), float(gs[best]))
