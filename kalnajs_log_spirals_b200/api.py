@@ -546,10 +546,29 @@ def compute_determinant_ksharded(omegas: Sequence[complex], config: KalnajsConfi
     dA = torch.view_as_real(torch.from_numpy(np.ascontiguousarray(A))).to("cuda").contiguous()
     dd = torch.empty((n, 2), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    check(None, lib.kls_det_lu_static(C.c_void_p(dA.data_ptr()), n, N, C.c_void_p(dd.data_ptr()),
-                                      C.c_void_p(None), C.c_void_p(stream)))
+    # one call per chunk that fits the static LU's scratch; calls on one
+    # stream run in order, so they do not race on the scratch
+    for lo, hi in static_lu_chunks(n, N):
+        check(None, lib.kls_det_lu_static(C.c_void_p(dA[lo].data_ptr()), hi - lo, N,
+                                          C.c_void_p(dd[lo].data_ptr()), C.c_void_p(None),
+                                          C.c_void_p(stream)))
     d = dd.cpu().numpy()
     return d[:, 0] + 1j * d[:, 1]
+
+
+STATIC_LU_MAX = 1 << 20     # complex elements of kls_det_lu_static's scratch
+
+
+def static_lu_chunks(n: int, N: int) -> List[Tuple[int, int]]:
+    """[lo, hi) ranges of at most STATIC_LU_MAX // N^2 matrices each, the
+    batches one kls_det_lu_static call accepts.  A single N x N matrix larger
+    than the scratch (N > 1024) cannot be factored there: _lib.KlsError."""
+    per = STATIC_LU_MAX // (N * N)
+    if per < 1:
+        raise _lib.KlsError(_lib.KLS_ERR_CONFIG,
+                            f"N_alpha = {N} > 1024: one matrix exceeds the fixed scratch of "
+                            "kls_det_lu_static; pass det_fn")
+    return [(lo, min(n, lo + per)) for lo in range(0, n, per)]
 
 
 def column_ranges(n_Op: int, n_gpus: int) -> List[slice]:

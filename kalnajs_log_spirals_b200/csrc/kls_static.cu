@@ -170,6 +170,12 @@ int kls_det_lu_static(const double* d_A_ri, int n_matrices, int N, double* d_det
   if (n_matrices < 0 || N < 1 || (n_matrices > 0 && (!d_A_ri || !d_det_ri)))
     return static_fail(KLS_ERR_CONFIG, "kls_det_lu_static: bad arguments");
   if (n_matrices == 0) return KLS_OK;
+  // One matrix of 1024^2 complex elements fills the scratch, so N <= 1024;
+  // the kernel's two row buffers then take at most 2 * 1024 * 16 B = 32 KiB
+  // of shared memory, inside the default 48 KiB (no opt-in needed).
+  if (N > 1024)
+    return static_fail(KLS_ERR_CONFIG, "kls_det_lu_static: N = " + std::to_string(N) +
+                                           " > 1024: one matrix exceeds the fixed scratch");
   if ((long long)n_matrices * N * N > KLS_STATIC_LU_MAX) {
     return static_fail(KLS_ERR_CONFIG,
                        "kls_det_lu_static: n_matrices * N * N = " +
@@ -177,13 +183,16 @@ int kls_det_lu_static(const double* d_A_ri, int n_matrices, int N, double* d_det
                            " exceeds the fixed scratch of " + std::to_string(KLS_STATIC_LU_MAX) +
                            " complex elements");
   }
-  if ((size_t)2 * N * sizeof(double2) > 200 * 1024)
-    return static_fail(KLS_ERR_CONFIG, "kls_det_lu_static: N too large for the row buffers");
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= SLU_MAX_DEVICES)
+  if (e != cudaSuccess)
     return static_fail(KLS_ERR_CUDA, std::string("kls_det_lu_static: cudaGetDevice: ") +
                                          cudaGetErrorString(e));
+  if (dev < 0 || dev >= SLU_MAX_DEVICES)
+    return static_fail(KLS_ERR_UNSUPPORTED,
+                       "kls_det_lu_static: device index " + std::to_string(dev) +
+                           " is beyond the " + std::to_string(SLU_MAX_DEVICES) +
+                           " devices whose scratch addresses are cached");
   double2* scratch;
   {
     std::lock_guard<std::mutex> lk(g_scratch_mu);
@@ -200,12 +209,6 @@ int kls_det_lu_static(const double* d_A_ri, int n_matrices, int N, double* d_det
     scratch = g_scratch_ptr[dev];
   }
   const size_t sm = 2 * (size_t)N * sizeof(double2);
-  if (sm > 48 * 1024) {
-    e = cudaFuncSetAttribute(lu_det_static_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm);
-    if (e != cudaSuccess)
-      return static_fail(KLS_ERR_CUDA, std::string("kls_det_lu_static: ") + cudaGetErrorString(e));
-  }
   lu_det_static_kernel<<<n_matrices, SLU_THREADS, sm, (cudaStream_t)stream>>>(
       N, reinterpret_cast<const double2*>(d_A_ri), scratch, reinterpret_cast<double2*>(d_det_ri),
       d_log_abs);

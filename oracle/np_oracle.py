@@ -290,87 +290,79 @@ class Orbits:
     FL: np.ndarray
 
 
-def compute_orbits(c: OracleConfig, model: ToomreZang, g: Grids) -> Orbits:
-    NR, Ne, nw, nwa = c.NR, c.Ne, c.nw, c.nwa
+def orbit_grid(c: OracleConfig):
+    """The w grid of the orbit integrals and its subsampling
+    (OrbitIntegration.jl:188-197): (w, dw, cos w, sin w, Ia, w[Ia])."""
     eps_w = 1e-8
-    w = linspace(eps_w, math.pi - eps_w, nw)
+    w = linspace(eps_w, math.pi - eps_w, c.nw)
     dw = w[1] - w[0]
-    cosw = np.cos(w)
-    sinw = np.sin(w)
-    nwai = (nw - 1) // (nwa - 1)
-    Ia = np.arange(0, nw, nwai)
-    wa = w[Ia]
+    nwai = (c.nw - 1) // (c.nwa - 1)
+    Ia = np.arange(0, c.nw, nwai)
+    return w, dw, np.cos(w), np.sin(w), Ia, w[Ia]
 
-    Om1 = np.zeros((NR, Ne))
-    Om2 = np.zeros((NR, Ne))
-    w1 = np.full((NR, Ne, len(Ia)), np.nan)
-    ra = np.full((NR, Ne, len(Ia)), np.nan)
-    pha = np.full((NR, Ne, len(Ia)), np.nan)
 
-    with np.errstate(all="ignore"):
-        for iR in range(NR):
-            R_i = g.Rc[iR, 0]
-            kap = math.sqrt(2.0) / R_i
-            Om = 1.0 / R_i
-            for ie in range(Ne):
-                E_i = g.E[iR, ie]
-                L_j = g.L_m[iR, ie]
-                L2_j = g.L2_m[iR, ie]
-                ecc = g.e[iR, ie]
-                r1, r2 = g.R1[iR, ie], g.R2[iR, ie]
-                sg = g.SGNL[iR, ie]
-                if abs(ecc) < 1e-10:                    # :222-229
-                    Om1[iR, ie] = kap
-                    Om2[iR, ie] = Om * sg
-                    w1[iR, ie] = wa
-                    ra[iR, ie] = R_i
-                    pha[iR, ie] = wa * Om2[iR, ie] / Om1[iR, ie]
-                    continue
-                if ecc < 0.01:                          # :232-241
-                    a_j = (r2 - r1) / 2
-                    Om1[iR, ie] = kap
-                    Om2[iR, ie] = Om * sg
-                    w1[iR, ie] = wa
-                    ra[iR, ie] = R_i - a_j * cosw[Ia]
-                    pha[iR, ie] = (wa * Om2[iR, ie] / Om1[iR, ie]
-                                   + 2 * Om / kap * a_j / R_i * sinw[Ia] * sg)
-                    continue
-                rs = (r1 + r2) / 2                      # :244-302
-                drs = (r2 - r1) / 2
-                xs = rs - drs * cosw
-                if L2_j > 1e-12:
-                    vr_sq = 2.0 * (E_i - _ln(xs)) * xs ** 2 - L2_j
-                    rvr = np.sqrt(np.maximum(0.0, vr_sq))
-                    svr = sinw * xs / rvr
-                    svr[0] = 2.0 * svr[1] - svr[2]
-                    svr[-1] = 2.0 * svr[-2] - svr[-3]
-                else:
-                    vr_sq = 2.0 * (E_i - _ln(xs))
-                    rvr = np.sqrt(np.maximum(0.0, vr_sq))
-                    svr = sinw / rvr
-                    svr[-1] = 2.0 * svr[-2] - svr[-3]
-                dt1 = drs * dw * svr
-                dt2 = np.zeros(nw)
-                dt2[1:] = (dt1[:-1] + dt1[1:]) / 2
-                t = np.cumsum(dt2)
-                Om1[iR, ie] = math.pi / t[-1]
-                w1[iR, ie] = t[Ia] * Om1[iR, ie]
-                ra[iR, ie] = xs[Ia]
-                if abs(1.0 - ecc) > 1e-10 and L2_j > 1e-12:
-                    sp = sinw / rvr
-                    sp[0] = 2.0 * sp[1] - sp[2]
-                    sp[-1] = 2.0 * sp[-2] - sp[-3]
-                    dt3 = drs * dw * sp / xs
-                    dt4 = np.zeros(nw)
-                    dt4[1:] = (dt3[:-1] + dt3[1:]) / 2
-                    ph = L_j * np.cumsum(dt4)[Ia]
-                else:
-                    ph = math.pi / 2 * np.ones(len(Ia)) * sg
-                    ph[0] = 0.0
-                Om2[iR, ie] = Om1[iR, ie] * ph[-1] / math.pi
-                pha[iR, ie] = ph
+def orbit_samples(g: Grids, iR: int, ie: int, wg):
+    """One orbit (OrbitIntegration.jl:222-302): Omega_1, Omega_2 and the
+    subsampled w1, r, theta along it (three branches, endpoint extrapolation)."""
+    w, dw, cosw, sinw, Ia, wa = wg
+    nw = len(w)
+    R_i = g.Rc[iR, 0]
+    kap = math.sqrt(2.0) / R_i
+    Om = 1.0 / R_i
+    E_i = g.E[iR, ie]
+    L_j = g.L_m[iR, ie]
+    L2_j = g.L2_m[iR, ie]
+    ecc = g.e[iR, ie]
+    r1, r2 = g.R1[iR, ie], g.R2[iR, ie]
+    sg = g.SGNL[iR, ie]
+    if abs(ecc) < 1e-10:                    # :222-229
+        om1, om2 = kap, Om * sg
+        return om1, om2, wa.copy(), np.full(len(Ia), R_i), wa * om2 / om1
+    if ecc < 0.01:                          # :232-241
+        a_j = (r2 - r1) / 2
+        om1, om2 = kap, Om * sg
+        return (om1, om2, wa.copy(), R_i - a_j * cosw[Ia],
+                wa * om2 / om1 + 2 * Om / kap * a_j / R_i * sinw[Ia] * sg)
+    rs = (r1 + r2) / 2                      # :244-302
+    drs = (r2 - r1) / 2
+    xs = rs - drs * cosw
+    if L2_j > 1e-12:
+        vr_sq = 2.0 * (E_i - _ln(xs)) * xs ** 2 - L2_j
+        rvr = np.sqrt(np.maximum(0.0, vr_sq))
+        svr = sinw * xs / rvr
+        svr[0] = 2.0 * svr[1] - svr[2]
+        svr[-1] = 2.0 * svr[-2] - svr[-3]
+    else:
+        vr_sq = 2.0 * (E_i - _ln(xs))
+        rvr = np.sqrt(np.maximum(0.0, vr_sq))
+        svr = sinw / rvr
+        svr[-1] = 2.0 * svr[-2] - svr[-3]
+    dt1 = drs * dw * svr
+    dt2 = np.zeros(nw)
+    dt2[1:] = (dt1[:-1] + dt1[1:]) / 2
+    t = np.cumsum(dt2)
+    om1 = math.pi / t[-1]
+    w1 = t[Ia] * om1
+    ra = xs[Ia]
+    if abs(1.0 - ecc) > 1e-10 and L2_j > 1e-12:
+        sp = sinw / rvr
+        sp[0] = 2.0 * sp[1] - sp[2]
+        sp[-1] = 2.0 * sp[-2] - sp[-3]
+        dt3 = drs * dw * sp / xs
+        dt4 = np.zeros(nw)
+        dt4[1:] = (dt3[:-1] + dt3[1:]) / 2
+        ph = L_j * np.cumsum(dt4)[Ia]
+    else:
+        ph = math.pi / 2 * np.ones(len(Ia)) * sg
+        ph[0] = 0.0
+    om2 = om1 * ph[-1] / math.pi
+    return om1, om2, w1, ra, ph
 
-    jac = compute_jacobian(g, Om1)
+
+def df_fields(model: ToomreZang, g: Grids):
+    """F0, FE, FL on the grid with non-finite values set to 0
+    (OrbitIntegration.jl:315-333)."""
+    NR, Ne = g.E.shape
     F0 = np.zeros((NR, Ne))
     FE = np.zeros((NR, Ne))
     FL = np.zeros((NR, Ne))
@@ -382,6 +374,25 @@ def compute_orbits(c: OracleConfig, model: ToomreZang, g: Grids) -> Orbits:
             FL[iR, ie] = model.df_L(E, L)
     for a in (F0, FE, FL):
         a[~np.isfinite(a)] = 0.0
+    return F0, FE, FL
+
+
+def compute_orbits(c: OracleConfig, model: ToomreZang, g: Grids) -> Orbits:
+    NR, Ne = c.NR, c.Ne
+    wg = orbit_grid(c)
+    na = len(wg[4])
+    Om1 = np.zeros((NR, Ne))
+    Om2 = np.zeros((NR, Ne))
+    w1 = np.full((NR, Ne, na), np.nan)
+    ra = np.full((NR, Ne, na), np.nan)
+    pha = np.full((NR, Ne, na), np.nan)
+    with np.errstate(all="ignore"):
+        for iR in range(NR):
+            for ie in range(Ne):
+                Om1[iR, ie], Om2[iR, ie], w1[iR, ie], ra[iR, ie], pha[iR, ie] = \
+                    orbit_samples(g, iR, ie, wg)
+    jac = compute_jacobian(g, Om1)
+    F0, FE, FL = df_fields(model, g)
     return Orbits(g, Om1, Om2, w1, ra, pha, jac, F0, FE, FL)
 
 
@@ -413,6 +424,21 @@ def compute_jacobian(g: Grids, Om1: np.ndarray) -> np.ndarray:
 # --------------------------------------------------------------------------
 # BasisFunctions.jl:199-304
 # --------------------------------------------------------------------------
+def w_orbit(m: int, om1: float, om2: float, w1v, rv, thv, alpha, l_arr):
+    """W_l(alpha) of one orbit, [n_l, N_alpha] (BasisFunctions.jl:217-252), or
+    None for an orbit with non-finite samples (skipped, i.e. zero)."""
+    if not (np.all(np.isfinite(rv)) and np.all(np.isfinite(thv)) and np.all(np.isfinite(w1v))):
+        return None
+    Sw1 = trapezoid_coef(w1v)
+    ratio = om2 / om1
+    phi = ratio * w1v - thv
+    C = Sw1[None, :] * np.cos(l_arr[:, None] * w1v[None, :] + m * phi[None, :])
+    C[~np.isfinite(C)] = 0.0
+    E = np.exp(-1j * alpha[None, :] * np.log(rv)[:, None]) / np.sqrt(rv)[:, None]
+    E[~np.isfinite(E)] = 0.0
+    return (C @ E) / math.pi
+
+
 def compute_W_l(c: OracleConfig, o: Orbits, alpha: np.ndarray, l_arr: np.ndarray) -> np.ndarray:
     """W[p, a, il] complex128 (p = iR + NR*ie, i.e. column-major orbit index)."""
     NR, Ne, m = c.NR, c.Ne, c.m
@@ -420,17 +446,10 @@ def compute_W_l(c: OracleConfig, o: Orbits, alpha: np.ndarray, l_arr: np.ndarray
     with np.errstate(all="ignore"):
         for iR in range(NR):
             for ie in range(Ne):
-                w1v, rv, thv = o.w1[iR, ie], o.ra[iR, ie], o.pha[iR, ie]
-                if not (np.all(np.isfinite(rv)) and np.all(np.isfinite(thv)) and np.all(np.isfinite(w1v))):
-                    continue
-                Sw1 = trapezoid_coef(w1v)
-                ratio = o.Omega_2[iR, ie] / o.Omega_1[iR, ie]
-                phi = ratio * w1v - thv
-                C = Sw1[None, :] * np.cos(l_arr[:, None] * w1v[None, :] + m * phi[None, :])
-                C[~np.isfinite(C)] = 0.0
-                E = np.exp(-1j * alpha[None, :] * np.log(rv)[:, None]) / np.sqrt(rv)[:, None]
-                E[~np.isfinite(E)] = 0.0
-                W[iR, ie] = (C @ E).T / math.pi
+                blk = w_orbit(m, o.Omega_1[iR, ie], o.Omega_2[iR, ie], o.w1[iR, ie], o.ra[iR, ie],
+                              o.pha[iR, ie], alpha, l_arr)
+                if blk is not None:
+                    W[iR, ie] = blk.T
     return W.reshape(NR * Ne, len(alpha), len(l_arr), order="F")
 
 

@@ -14,6 +14,7 @@ import os
 import socket
 
 import numpy as np
+import pytest
 
 import kalnajs_log_spirals_b200 as K
 from oracle import np_oracle as O
@@ -146,3 +147,17 @@ def test_harmonic_ranges_cover_each_harmonic_once():
     ls = [l for lo, hi in r for l in range(lo, hi + 1)]
     assert ls == list(range(-100, 101))
     assert [hi - lo + 1 for lo, hi in r] == [26] + [25] * 7
+
+
+def test_static_lu_chunks_fit_the_scratch():
+    from kalnajs_log_spirals_b200.api import STATIC_LU_MAX, static_lu_chunks
+    assert static_lu_chunks(13, 301) == [(0, 11), (11, 13)]
+    assert static_lu_chunks(16, 256) == [(0, 16)]
+    assert static_lu_chunks(0, 301) == []
+    for n, N in [(100, 301), (7, 1024), (3, 33)]:
+        ch = static_lu_chunks(n, N)
+        assert ch[0][0] == 0 and ch[-1][1] == n
+        assert all(a[1] == b[0] for a, b in zip(ch, ch[1:]))
+        assert all((hi - lo) * N * N <= STATIC_LU_MAX for lo, hi in ch)
+    with pytest.raises(K.KlsError):
+        static_lu_chunks(2, 1025)

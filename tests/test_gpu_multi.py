@@ -164,3 +164,28 @@ def test_ksharded_path_on_one_rank(lib_path):
     finally:
         dist.destroy_process_group()
     assert np.max(np.abs(d - ref) / np.abs(ref)) < 1e-12, np.abs(d - ref) / np.abs(ref)
+
+
+def test_ksharded_lu_batch_larger_than_one_chunk(lib_path):
+    """13 matrices of N = 301 need two kls_det_lu_static calls (11 fit its
+    scratch); the chunked path equals numpy's LAPACK determinant."""
+    import datetime
+    import os
+    import socket
+    import torch.distributed as dist
+    N, n = 301, 13
+    assert K.api.static_lu_chunks(n, N) == [(0, 11), (11, 13)]
+    rng = np.random.default_rng(5)
+    mats = (rng.standard_normal((n, N, N)) + 1j * rng.standard_normal((n, N, N))) * (0.3 / N ** 0.5)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=0, world_size=1, timeout=datetime.timedelta(seconds=30))
+    try:
+        d = K.compute_determinant_ksharded(np.arange(n) * (1 + 0.1j), None,
+                                           M_fn=lambda w: mats[int(round(w.real))])
+    finally:
+        dist.destroy_process_group()
+    ref = np.linalg.det(np.eye(N)[None] - mats)
+    assert np.max(np.abs(d - ref) / np.abs(ref)) < 1e-11

@@ -55,9 +55,34 @@ def test_det_lu_static_matches_det_batch(lib_path):
     assert np.array_equal(a.cpu().numpy(), np.ascontiguousarray(mats).view(np.float64))
 
 
+def test_det_lu_static_at_the_scratch_limit(lib_path):
+    """16 matrices of N = 256 fill the 2^20-element scratch exactly (the last
+    CTA's block ends at the array's end); results equal numpy's LAPACK det."""
+    import torch
+    lib = _lib.load(lib_path)
+    n, N = 16, 256
+    rng = np.random.default_rng(3)
+    mats = np.eye(N)[None] + (rng.standard_normal((n, N, N))
+                              + 1j * rng.standard_normal((n, N, N))) * (0.3 / N ** 0.5)
+    ref = np.linalg.det(mats)
+    a = torch.tensor(np.ascontiguousarray(mats).view(np.float64), dtype=torch.float64,
+                     device="cuda")
+    det = torch.zeros((n, 2), dtype=torch.float64, device="cuda")
+    code = lib.kls_det_lu_static(C.c_void_p(a.data_ptr()), n, N, C.c_void_p(det.data_ptr()),
+                                 None, None)
+    assert code == 0, lib.kls_create_error()
+    torch.cuda.synchronize()
+    d = det.cpu().numpy()
+    got = d[:, 0] + 1j * d[:, 1]
+    assert np.max(np.abs(got - ref) / np.abs(ref)) <= 1e-11
+
+
 def test_det_lu_static_rejects_oversize(lib_path):
     lib = _lib.load(lib_path)
     dummy = C.c_void_p(1)
     code = lib.kls_det_lu_static(dummy, 12, 301, dummy, None, None)   # 12 * 301^2 > 2^20
     assert code == _lib.KLS_ERR_CONFIG
     assert b"exceeds the fixed scratch" in lib.kls_create_error()
+    code = lib.kls_det_lu_static(dummy, 1, 1025, dummy, None, None)   # one matrix > 2^20
+    assert code == _lib.KLS_ERR_CONFIG
+    assert b"1025 > 1024" in lib.kls_create_error()
