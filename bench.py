@@ -39,8 +39,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Newton time-to-root & det(I−M) evals/s at |Δω|≤1e-10, mixed vs plain FP64"
 UNIT = "det_evals/s"
-WORKLOAD = ("plain FP64 det(I-M(omega)) at default size: Toomre-Zang n=4 m=2 q1=7, NR=501 Ne=51 "
-            "N_alpha=301 alpha_max=30 l=[-100,100]; step = Newton FD triple")
+def workload(cfg) -> str:
+    """The benchmark workload named by what it is, with its sizes."""
+    g, md = cfg.grid, cfg.model
+    return (f"plain FP64 det(I-M(omega)): Toomre-Zang n={md.n_zang} m={cfg.physics.m} "
+            f"q1={md.q1:g}, NR={g.NR} Ne={g.Ne} N_alpha={g.N_alpha} alpha_max={g.alpha_max:g} "
+            f"l=[{g.l_min},{g.l_max}]")
 
 
 def parse():
@@ -80,68 +84,196 @@ def dist_env():
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's BLAS form (NL_julia_direct.jl:299-310) via the
-# oracle's numpy restatement, timed on a bounded sample of harmonics
+# CPU reference: the oracle's restatement of the reference CPU algorithm
+# (NL_julia_direct.jl:177-310: orbits, W_l table, then per determinant one
+# weighted copy + one ZGEMM per harmonic and LAPACK zgetrf), on the real model
+# at the benchmark's own size, on all host threads
 # ---------------------------------------------------------------------------
-def cpu_det_rate(cfg, budget_s: float = 12.0):
-    import numpy as np
+def oracle_config(cfg):
+    from oracle import np_oracle as O
+    g, md = cfg.grid, cfg.model
+    return O.OracleConfig(m=int(cfg.physics.m), G=float(cfg.physics.G), L0=float(md.L0),
+                          n_zang=int(md.n_zang), q1=float(md.q1), NR=g.NR, Ne=g.Ne,
+                          Rc_min=g.Rc_min, Rc_max=g.Rc_max, v_min=g.v_min, N_alpha=g.N_alpha,
+                          alpha_max=g.alpha_max, l_min=g.l_min, l_max=g.l_max, nw=g.nw,
+                          nwa=g.nwa, quad=g.quadrature)
+
+
+def blas_threads() -> int:
     try:
         from threadpoolctl import threadpool_info
-        threads = max([i.get("num_threads", 1) for i in threadpool_info()
-                       if i.get("internal_api") == "openblas"] or [os.cpu_count() or 1])
+        return max([i.get("num_threads", 1) for i in threadpool_info()
+                    if i.get("internal_api") == "openblas"] or [os.cpu_count() or 1])
     except Exception:
-        threads = os.cpu_count() or 1
-    g = cfg.grid
-    NPh, Na, n_l = g.NR * g.Ne, g.N_alpha, g.l_max - g.l_min + 1
-    rng = np.random.default_rng(0)
-    W = (rng.standard_normal((NPh, Na)) + 1j * rng.standard_normal((NPh, Na))) * 0.1
-    Ores = rng.uniform(-3, 3, NPh)
-    G = rng.standard_normal(NPh)
-    omega = 0.88 + 0.12j
-    M = np.zeros((Na, Na), dtype=np.complex128)
-    # warm one harmonic, then time as many as fit in the budget
-    den = omega - Ores
-    M += W.T @ ((G / den)[:, None] * np.conj(W))
-    t0 = time.perf_counter()
-    done = 0
-    while done < n_l and time.perf_counter() - t0 < budget_s:
-        den = omega - Ores
-        den = np.where(np.abs(den) < 1e-12, 1e-12 + 1e-12j, den)
-        wgt = G / den
-        M += W.T @ (wgt[:, None] * np.conj(W))
-        done += 1
-    t_l = (time.perf_counter() - t0) / done
-    t1 = time.perf_counter()
-    np.linalg.det(np.eye(Na) - M * 1e-3)
-    t_lu = time.perf_counter() - t1
-    t_det = n_l * t_l + t_lu
-    sample = (f"{done} of {n_l} harmonics (one ZGEMM {Na}x{NPh}x{Na} each) + zgetrf {Na}x{Na}, "
-              f"extrapolated to the full K = {NPh * n_l}")
-    return 1.0 / t_det, threads, sample
+        return os.cpu_count() or 1
+
+
+def table_storage(nbytes: float):
+    """Shared memory when /dev/shm holds the table with room to spare, else a
+    file in the temporary directory (None: shared memory)."""
+    import shutil
+    try:
+        if shutil.disk_usage("/dev/shm").free > 1.2 * nbytes:
+            return None
+    except OSError:
+        pass
+    return os.path.join(tempfile.mkdtemp(prefix="kls_ref_"), "W.c128")
+
+
+def fixture_check(dets_fn, m: int):
+    """The oracle's det at the default-size fixture's first omega against the
+    committed value (tests/golden/size_d.npz), when the run is at that size."""
+    import numpy as np
+    path = os.path.join(ROOT, "tests", "golden", "size_d.npz")
+    if not os.path.exists(path):
+        return None
+    f = np.load(path)
+    w = complex(f["omegas"][0])
+    d = dets_fn(w)
+    ref = complex(f["dets"][0])
+    return {"omega": [w.real, w.imag], "det": [d.real, d.imag],
+            "rel_diff_vs_fixture": abs(d - ref) / abs(ref)}
 
 
 def reference_arm(args):
     rank, _, world = dist_env()
     if rank != 0:
         return 0
+    import numpy as np
     import kalnajs_log_spirals_b200 as K
+    from oracle import np_oracle_large as L
     cfg = K.load_model(K.load_config(args.config), args.model)
-    steps = []
-    for _ in range(args.warmup):
-        cpu_det_rate(cfg, budget_s=2.0)
-    for _ in range(max(1, min(args.steps, 3))):
-        steps.append(cpu_det_rate(cfg, budget_s=8.0))
-    rate = statistics.median(s[0] for s in steps)
-    threads, sample = steps[0][1], steps[0][2]
+    oc = oracle_config(cfg)
+    threads = blas_threads()
+    nbytes = 16.0 * oc.NPh * oc.N_alpha * oc.n_l
+    path = table_storage(nbytes)
+    t0 = time.perf_counter()
+    pc = L.precompute_large(oc, workers=os.cpu_count() or 1, table_path=path)
+    t_pre = time.perf_counter() - t0
+    try:
+        m = oc.m
+        # one determinant per step, the omegas of the GPU arm's Newton triples
+        n_steps = args.warmup + args.steps
+        oms = [omegas_for_step(s // 3, 0, m, cfg.reference.Omega_p, cfg.reference.gamma,
+                               cfg.newton.delta)[s % 3] for s in range(n_steps)]
+        for s in range(args.warmup):
+            L.compute_det_large(pc, oms[s])
+        dets = []
+        t0 = time.perf_counter()
+        for s in range(args.warmup, n_steps):
+            dets.append(L.compute_det_large(pc, oms[s]))
+        t = time.perf_counter() - t0
+        same_size = (oc.NR, oc.Ne, oc.N_alpha, oc.l_min, oc.l_max) == (501, 51, 301, -100, 100)
+        check = fixture_check(lambda w: L.compute_det_large(pc, w), m) if same_size else None
+    finally:
+        pc.close()
+        if path:
+            import shutil
+            shutil.rmtree(os.path.dirname(path), ignore_errors=True)
+    rate = args.steps / t
+    sample = (f"whole determinants at {oc.NR}x{oc.Ne} orbits, N_alpha={oc.N_alpha}, "
+              f"l=[{oc.l_min},{oc.l_max}] ({oc.n_l} ZGEMMs {oc.N_alpha}x{oc.NPh}x{oc.N_alpha} "
+              f"+ zgetrf per det), one det per step; table precompute {t_pre:.0f} s untimed")
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
-            "steps": len(steps), "warmup": args.warmup, "ms_per_step": 3e3 / rate,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD},
+            "data": "synthetic (the model's own grids)",
+            "config": {"workload": workload(cfg), "NR": oc.NR, "Ne": oc.Ne, "N_alpha": oc.N_alpha,
+                       "l": [oc.l_min, oc.l_max], "omegas_per_step": 1,
+                       "step": "one whole determinant (the omegas of the GPU arm's Newton "
+                               "triples, in order)"},
             "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": sample},
-            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "precompute_s": t_pre, "host_cores": os.cpu_count(),
+            "dets": [[d.real, d.imag] for d in dets[:3]], "oracle_fixture_check": check}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def oracle_parity(K, cfg, pc, newton, mixed: bool):
+    """FP64 and split-BF16 results against the oracle at the default size
+    (tests/golden/size_d.npz, made by tests/golden/make_size_d.py: the
+    oracle's Newton root, M at that root and dets at 23 omegas).  FP64
+    tolerances as in the parity tests: 1e-11 of the scale plus 4x the oracle's
+    own 2-ulp-ln sensitivity; roots 1e-10."""
+    import numpy as np
+    path = os.path.join(ROOT, "tests", "golden", "size_d.npz")
+    g = cfg.grid
+    if not os.path.exists(path) or (g.NR, g.Ne, g.N_alpha, g.l_min, g.l_max) != \
+            (501, 51, 301, -100, 100):
+        return None
+    f = np.load(path)
+    om, d_or = f["omegas"], f["dets"]
+    sens = f["sens_dets"] if "sens_dets" in f.files else np.zeros(len(om))
+    d64 = K.compute_determinant_batched(om, pc, None, batch_size=16)
+    err64 = np.abs(d64 - d_or)
+    M = K.build_M_matrix(complex(f["omega_root"][0]), pc)
+    M0 = f["M0"]
+    sM = f["sens_M0"] if "sens_M0" in f.files else np.zeros(M0.shape)
+    errM = np.abs(M - M0)
+    root = f["root"]
+    out = {"fixture": "tests/golden/size_d.npz (oracle, NL_julia_direct.jl BLAS form)",
+           "omegas": int(len(om)),
+           "fp64": {"det_rel_err_max": float(np.max(err64 / np.abs(d_or))),
+                    "det_within_tol": bool(np.all(err64 <= 1e-11 * np.abs(d_or) + 4 * sens)),
+                    "M_at_root_err_over_max": float(errM.max() / np.abs(M0).max()),
+                    "M_within_tol": bool(np.all(errM <= 1e-11 * np.abs(M0).max() + 4 * sM))},
+           "oracle_root": [float(root[0]), float(root[1])]}
+    if newton:
+        r = newton["plain_fp64"]
+        out["fp64"]["root_abs_diff"] = [abs(r["Omega_p"] - root[0]), abs(r["gamma"] - root[1])]
+        h = newton.get("mixed_fp64_finish")
+        if h:
+            out["hybrid_root_abs_diff"] = [abs(h["Omega_p"] - root[0]), abs(h["gamma"] - root[1])]
+    if mixed:
+        try:
+            dev = K.to_device(pc, K.GPUType.NVIDIA, "Float32")
+            dmx = K.compute_determinant_batched(om, pc, dev, batch_size=16)
+            rel = np.abs(dmx - d_or) / np.abs(d_or)
+            out["mixed"] = {"det_rel_err_vs_oracle": {"median": float(np.median(rel)),
+                                                      "max": float(rel.max())}}
+        except K.KlsError as e:
+            out["mixed"] = {"unavailable": str(e)}
+    return out
+
+
+def cpu_det_baseline(pc, cfg, omega: complex):
+    """The oracle's BLAS-form determinant (one ZGEMM per harmonic + zgetrf) on
+    the host cores, timed on one whole determinant of the benchmark model; the
+    table is the device's own, exported harmonic by harmonic (the oracle's
+    table build is timed by --impl reference).  Returns (det/s, det, note)."""
+    import numpy as np
+    from oracle import np_oracle_large as L
+    oc = oracle_config(cfg)
+    dims = pc.ctx.dims
+    W = np.empty((oc.n_l, dims.NPh, oc.N_alpha), dtype=np.complex128)
+    buf = np.empty(dims.NPh * oc.N_alpha, dtype=np.complex128)
+    for il in range(oc.n_l):
+        pc.ctx.call("kls_export_W", il, 1, buf.view(np.float64).ctypes.data_as(
+            C.POINTER(C.c_double)))
+        W[il] = buf.reshape(oc.N_alpha, dims.NPh).T
+    DJ = pc.DJ_vec
+    F0l = pc.F0l_all.reshape(dims.NPh, oc.n_l, order="F")
+    Ores = pc.Omega_res.reshape(dims.NPh, oc.n_l, order="F")
+
+    class _T:
+        arr = W
+
+        @staticmethod
+        def close(unlink=False):
+            pass
+
+    lp = L.LargePrecomputed(oc, pc.alpha_arr, pc.d_alpha, pc.N_kernel, None, None, DJ, F0l,
+                            Ores, _T())
+    L.compute_det_large(lp, omega + 1e-3)            # warm the BLAS pool
+    t0 = time.perf_counter()
+    d = L.compute_det_large(lp, omega)
+    t = time.perf_counter() - t0
+    del W
+    return 1.0 / t, d, (f"one whole determinant (all {oc.n_l} harmonics, ZGEMM "
+                        f"{oc.N_alpha}x{dims.NPh}x{oc.N_alpha} each, + zgetrf) on the device's "
+                        f"exported table")
 
 
 # ---------------------------------------------------------------------------
@@ -211,16 +343,14 @@ def dgemm_peak_tflops(torch) -> float:
     return 2 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def read_traffic(name: str):
-    """dram bytes per launch from a committed ncu summary line 'traffic_bytes_per_launch: N'."""
-    path = os.path.join(ROOT, "profiles", name)
+def read_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the data file beside the ncu
+    summaries (profiles/traffic.json): (bytes, scaled from a smaller case)."""
     try:
-        for line in open(path):
-            if line.strip().startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
-    return None
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))[kernel]
+        return float(d["bytes_per_launch"]), bool(d.get("scaled", False))
+    except (OSError, KeyError, ValueError):
+        return None, None
 
 
 def precompute_roofline(cfg, dims, pre_ms, peak64: float, peaks: dict):
@@ -710,6 +840,9 @@ def ours(args):
         _lib.check(h, lib.kls_prepare_mixed(h))
         t_split = time.perf_counter() - t0
         tunes["mixed"] = K.autotune(pc, "Float32", batch=nb)
+        mixed_kernel = {_lib.KLS_MIXED_TMEM: "mixed_tm_kernel",
+                        _lib.KLS_MIXED_PAIR: "mixed_pair_kernel"}.get(tunes["mixed"].form,
+                                                                    "mixed_contract_kernel")
         ms_mx, launches_mx, _ = time_device(_lib.KLS_MODE_MIXED)
         stage_mx = stage_times(_lib.KLS_MODE_MIXED)
         ach_mx = nb * mixed_flops_per_det / (stage_mx[1] * 1e-3) / 1e12
@@ -727,11 +860,12 @@ def ours(args):
         mixed = {"det_evals_per_s": world * nb * args.steps / (ms_mx * 1e-3),
                  "ms_per_step": ms_mx / args.steps, "gpu_launches": int(launches_mx),
                  "split_table_s": t_split,
-                 "roofline": {"bound": "tensor", "kernel": "mixed_contract_kernel (tcgen05 kind::f16, TMEM)",
+                 "roofline": {"bound": "tensor", "kernel": mixed_kernel + " (tcgen05 kind::f16, TMEM)",
                               "achieved": ach_mx, "peak": peak_bf16, "unit": "TFLOP/s",
                               "frac": ach_mx / peak_bf16, "peak_note": peak_bf16_note,
                               "algorithmic_flops_per_launch": nb * mixed_flops_per_det,
-                              "traffic": read_traffic("contract_mixed_default.md"),
+                              "traffic": read_traffic(mixed_kernel)[0],
+                              "traffic_scaled": read_traffic(mixed_kernel)[1],
                               "stage_ms": {"weights": stage_mx[0], "contract": stage_mx[1],
                                            "reduce": stage_mx[2], "lu": stage_mx[3]}},
                  "rel_det_err_vs_fp64": {"points": int(len(om)), "seed": 0,
@@ -763,6 +897,30 @@ def ours(args):
                 "abs_dOmega_p_vs_plain": abs(rh.Omega_p - r.Omega_p),
                 "abs_dgamma_vs_plain": abs(rh.gamma - r.gamma)}
             newton["speedup_hybrid_vs_plain"] = t_plain / t_h
+            # conditioning at the FP64 root: |det'| (complex derivative,
+            # forward difference) and the split form's residual there, whose
+            # ratio is the split form's own root error
+            w_r = complex(m * r.Omega_p, r.gamma)
+            d_pair = K.compute_determinant_batched(np.array([w_r, w_r + 1e-7]), pc, None)
+            dprime = abs((d_pair[1] - d_pair[0]) / 1e-7)
+            d_mx = K.compute_determinant(w_r, pc, K.to_device(pc, K.GPUType.NVIDIA, "Float32"))
+            newton["at_fp64_root"] = {"abs_det_prime": dprime, "abs_mixed_det": abs(d_mx),
+                                      "mixed_root_error_estimate": abs(d_mx) / dprime}
+
+    # ---- parity against the oracle's default-size fixture ----------------------
+    parity = None
+    if rank == 0:
+        parity = oracle_parity(K, cfg, pc, newton, not args.no_mixed)
+
+    # ---- CPU baseline: the oracle's BLAS-form determinant on the host cores ---
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        w0 = complex(*all_om[args.warmup][0])
+        rate, d_cpu, sample = cpu_det_baseline(pc, cfg, w0)
+        d_gpu = K.compute_determinant(w0, pc)
+        cpu = {"value": rate, "unit": UNIT, "cores": blas_threads(), "kind": "port",
+               "sample": sample, "host_cores": os.cpu_count(),
+               "det_rel_diff_vs_gpu_fp64": abs(d_cpu - d_gpu) / abs(d_gpu)}
 
     refgpu = None
     if world == 1 and not args.no_refgpu:
@@ -785,31 +943,20 @@ def ours(args):
         from kalnajs_log_spirals_b200 import proposer as P
         uneven = uneven_batch(args, K, P, local, torch.cuda.synchronize)
 
-    cpu = None
-    if rank == 0 and not args.no_cpu:
-        rate, threads, sample = cpu_det_rate(cfg)
-        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
-        try:
-            # the reference's default thread count (configs/default.toml [cpu] max_threads = 4)
-            from threadpoolctl import threadpool_limits
-            with threadpool_limits(limits=4):
-                r4, _, s4 = cpu_det_rate(cfg, budget_s=8.0)
-            cpu["at_4_threads"] = {"value": r4, "cores": 4, "sample": s4}
-        except Exception as e:          # threadpoolctl missing: report why
-            cpu["at_4_threads"] = {"unavailable": repr(e)}
-
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    traffic = read_traffic("contract_f64_default.md")
+    traffic, traffic_scaled = read_traffic("contract_kernel")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (no dataset: the workload is the model's own grids)",
-        "config": {"workload": WORKLOAD, "NR": cfg.grid.NR, "Ne": cfg.grid.Ne,
+        "config": {"workload": workload(cfg), "step": "one Newton finite-difference triple "
+                   "(omega, omega + m delta, omega + i delta) in one batch",
+                   "NR": cfg.grid.NR, "Ne": cfg.grid.Ne,
                    "N_alpha": cfg.grid.N_alpha, "l": [cfg.grid.l_min, cfg.grid.l_max],
                    "K": dims.K, "omegas_per_step": nb, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (W table %.1f GB in HBM)" % (
@@ -819,15 +966,17 @@ def ours(args):
                      "frac": achieved / peak64,
                      "peak_note": "of measured: cuBLAS DGEMM 8192^3 best-of-5 in this run",
                      "algorithmic_flops_per_launch": nb * flops_per_det,
-                     "traffic": traffic, "stage_ms": {"weights": stage[0], "contract": stage[1],
+                     "traffic": traffic, "traffic_scaled": traffic_scaled, "stage_ms": {"weights": stage[0], "contract": stage[1],
                                                       "reduce": stage[2], "lu": stage[3]}},
         "cpu_baseline": cpu,
+        "parity_vs_oracle": parity,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nb * 16,
                 "d2h_bytes_per_step": nb * 24},
         "gpu_launches": int(launches),
         "clocks": clk,
         "autotune": {k: {"splits": t.splits, "default_splits": t.default_splits,
-                         "form": {0: "fp64", 1: "one CTA", 2: "CTA pair"}.get(t.form, t.form),
+                         "form": {0: "fp64", 1: "one CTA", 2: "CTA pair",
+                                  3: "TMEM-operand CTA pair"}.get(t.form, t.form),
                          "candidates": t.candidates, "ms_per_omega": t.ms_per_omega,
                          "default_ms_per_omega": t.default_ms_per_omega}
                      for k, t in tunes.items()},

@@ -39,6 +39,9 @@ extern "C" {
 #define KLS_ERR_NONFINITE    5  /* non-finite value in an input or result     */
 #define KLS_ERR_SINGULAR     6  /* singular 2x2 Newton Jacobian               */
 #define KLS_ERR_UNSUPPORTED  7  /* mode not available on this device          */
+#define KLS_ERR_TIMEOUT      8  /* a bounded device-side wait ran out: the
+                                   contraction pipeline stalled; the call's
+                                   results are invalid, the context stays usable */
 
 /* ---- precision modes of the contraction -------------------------------- */
 #define KLS_MODE_FP64        0  /* plain FP64 (the oracle form)               */
@@ -253,7 +256,8 @@ int kls_mlp_train(kls_mlp* mlp, const float* X, const float* T, int n, int epoch
  * result download) is one CUDA graph replay.  Each model keeps its
  * context's K split count (tune with kls_autotune before creating the
  * batch), so every determinant is bitwise what kls_det_batch returns for
- * that context.  The contexts must outlive the batch and are not modified;
+ * that context (split-BF16: in the KLS_MIXED_ONE_CTA form, whose kernel body
+ * the batch runs; the KLS_MIXED_TMEM form sums in another order).  The contexts must outlive the batch and are not modified;
  * a batch is not re-entrant.  Errors: kls_multi_last_error (NULL handle:
  * errors of kls_multi_create).                                              */
 typedef struct kls_multi kls_multi;
@@ -321,17 +325,39 @@ int kls_set_splits(kls_ctx* ctx, int mode, int splits);
 int kls_set_lu_mode(kls_ctx* ctx, int mode);
 
 /* ---- split-BF16 contraction kernel (no reference counterpart) ------------- *
+ * KLS_MIXED_TMEM (the default when N_alpha_pad <= 384): a CTA pair
+ * (tcgen05 cta_group::2, M = 256) per two 64-alpha x 1-omega tiles; the
+ * omega-dependent operand w conj(W) is formed once per omega, written from
+ * registers straight into tensor memory and read by the MMA from there, the
+ * table rows (all N_alpha_pad of them, half per CTA) come from shared memory
+ * by TMA.  The older forms re-form that operand once per 128-row tile:
  * KLS_MIXED_ONE_CTA: one CTA per 128-row x 64-alpha x 2-omega tile.
  * KLS_MIXED_PAIR: a cluster of two CTAs per 256-row tile (tcgen05
  * cta_group::2, M = 256): each SM forms half as much of the per-omega
  * operand; it pays off when 2 N_alpha_pad is a multiple of 256 (otherwise
- * the last pair's odd CTA has no rows).  Both return the same bits.
- * KLS_MIXED_AUTO (the default) is the one-CTA form; kls_autotune times both.
+ * the last pair's odd CTA has no rows).  ONE_CTA and PAIR return the same
+ * bits (and the bits of the uneven multi-model batch); TMEM sums in another
+ * order (same accuracy).  KLS_MIXED_AUTO picks TMEM where it applies, else
+ * ONE_CTA; kls_autotune times all of them.
  * Calls kls_prepare_mixed first if needed.                                    */
 #define KLS_MIXED_AUTO       0
 #define KLS_MIXED_ONE_CTA    1
 #define KLS_MIXED_PAIR       2
+#define KLS_MIXED_TMEM       3
 int kls_set_mixed_form(kls_ctx* ctx, int form);
+
+/* ---- failure handling of the device pipeline (no reference counterpart) --- *
+ * Every wait of the KLS_MIXED_TMEM contraction (on a copy, an MMA or another
+ * warp) is bounded by this limit (default 2 s; the older mixed forms keep a
+ * fixed 2 s).  A wait that runs out makes the call return KLS_ERR_TIMEOUT
+ * instead of hanging the GPU; the context stays usable.                     */
+int kls_set_wait_limit(kls_ctx* ctx, double seconds);
+/* Test hook for that path: mode 1 makes the next KLS_MIXED_TMEM contraction
+ * skip one producer warp's "operand ready" arrival in its first CTA pair, so
+ * the MMA warp's bounded wait runs out and the call returns KLS_ERR_TIMEOUT
+ * (no trap, no fault, no unbounded wait); the mode clears itself after that
+ * launch.  mode 0 clears it.                                               */
+int kls_set_fault_injection(kls_ctx* ctx, int mode);
 
 /* ---- instrumentation ----------------------------------------------------- */
 /* Per-stage device time (ms) of the last det batch when timing is enabled:

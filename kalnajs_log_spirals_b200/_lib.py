@@ -19,6 +19,7 @@ KLS_ERR_STATE = 4
 KLS_ERR_NONFINITE = 5
 KLS_ERR_SINGULAR = 6
 KLS_ERR_UNSUPPORTED = 7
+KLS_ERR_TIMEOUT = 8
 
 KLS_MODE_FP64 = 0
 KLS_MODE_MIXED = 1
@@ -32,6 +33,7 @@ QUAD_CODES = {"t": KLS_QUAD_TRAPEZOID, "s": KLS_QUAD_SIMPSON, "b": KLS_QUAD_BOOL
 KLS_MIXED_AUTO = 0
 KLS_MIXED_ONE_CTA = 1
 KLS_MIXED_PAIR = 2
+KLS_MIXED_TMEM = 3
 
 KLS_LU_AUTO = 0
 KLS_LU_CTA = 1
@@ -39,7 +41,7 @@ KLS_LU_CLUSTER = 2
 
 STATUS_NAMES = {0: "KLS_OK", 1: "KLS_ERR_CONFIG", 2: "KLS_ERR_CUDA", 3: "KLS_ERR_OOM",
                 4: "KLS_ERR_STATE", 5: "KLS_ERR_NONFINITE", 6: "KLS_ERR_SINGULAR",
-                7: "KLS_ERR_UNSUPPORTED"}
+                7: "KLS_ERR_UNSUPPORTED", 8: "KLS_ERR_TIMEOUT"}
 
 
 class KlsError(RuntimeError):
@@ -149,6 +151,8 @@ SIGNATURES = {
     "kls_set_splits": (C.c_int, [_P, C.c_int, C.c_int]),
     "kls_set_lu_mode": (C.c_int, [_P, C.c_int]),
     "kls_set_mixed_form": (C.c_int, [_P, C.c_int]),
+    "kls_set_wait_limit": (C.c_int, [_P, C.c_double]),
+    "kls_set_fault_injection": (C.c_int, [_P, C.c_int]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_get_precompute_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),

@@ -821,16 +821,24 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
       return KLS_OK;
     }
   }
-  std::vector<int> cand = {std::max(1, def / 2), def, 2 * def, 3 * def};
-  for (int& s : cand) s = std::max(1, std::min(s, max_s));
-  std::sort(cand.begin(), cand.end());
-  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-  // the split-BF16 form also chooses its tile: one CTA or a CTA pair
+  // the split-BF16 form also chooses its kernel: one CTA, a CTA pair, or the
+  // TMEM-operand pair; split candidates around each form's own default
   std::vector<int> forms = mixed ? std::vector<int>{KLS_MIXED_ONE_CTA, KLS_MIXED_PAIR}
                                  : std::vector<int>{0};
+  if (mixed && kls_mixed_set_form(c, KLS_MIXED_TMEM) == KLS_OK) forms.push_back(KLS_MIXED_TMEM);
+  if (mixed) kls_mixed_set_form(c, def_form);
   double best_ms = INFINITY;
   int best = def, best_form = def_form;
-  for (int form : forms)
+  for (int form : forms) {
+    int fdef = def;
+    if (mixed) {
+      if ((r = kls_mixed_set_form(c, form))) return r;
+      fdef = kls_mixed_default_splits(c);
+    }
+    std::vector<int> cand = {std::max(1, fdef / 2), fdef, 2 * fdef, 3 * fdef};
+    for (int& s : cand) s = std::max(1, std::min(s, max_s));
+    std::sort(cand.begin(), cand.end());
+    cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
     for (int s : cand) {
       if ((r = apply(s, form))) return r;
       double ms = 0.0;
@@ -843,6 +851,7 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
       }
       res.candidates++;
     }
+  }
   if ((r = apply(best, best_form))) return r;
   res.splits = best;
   res.form = best_form;
@@ -871,10 +880,30 @@ int kls_set_splits(kls_ctx* c, int mode, int splits) {
 int kls_set_mixed_form(kls_ctx* c, int form) {
   int r = check_ready(c);
   if (r) return r;
-  if (form != KLS_MIXED_AUTO && form != KLS_MIXED_ONE_CTA && form != KLS_MIXED_PAIR)
+  if (form != KLS_MIXED_AUTO && form != KLS_MIXED_ONE_CTA && form != KLS_MIXED_PAIR &&
+      form != KLS_MIXED_TMEM)
     return kls_fail(c, KLS_ERR_CONFIG, "unknown mixed contraction form");
   if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
-  return kls_mixed_set_form(c, form == KLS_MIXED_AUTO ? KLS_MIXED_ONE_CTA : form);
+  if (form == KLS_MIXED_AUTO)
+    form = kls_mixed_set_form(c, KLS_MIXED_TMEM) == KLS_OK ? KLS_MIXED_TMEM : KLS_MIXED_ONE_CTA;
+  return kls_mixed_set_form(c, form);
+}
+
+int kls_set_wait_limit(kls_ctx* c, double seconds) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (!(seconds > 0.0) || seconds > 60.0)
+    return kls_fail(c, KLS_ERR_CONFIG, "wait limit must be in (0, 60] seconds");
+  if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
+  return kls_mixed_set_wait(c, (unsigned long long)(seconds * 1e9), -1);
+}
+
+int kls_set_fault_injection(kls_ctx* c, int mode) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (mode != 0 && mode != 1) return kls_fail(c, KLS_ERR_CONFIG, "fault injection mode is 0 or 1");
+  if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
+  return kls_mixed_set_wait(c, 0, mode);
 }
 
 int kls_set_lu_mode(kls_ctx* c, int mode) {

@@ -180,9 +180,23 @@ int kls_multi_launch_mixed(cudaStream_t st, const kls_mdesc* d_md, const int2* d
                            int64_t max_K_pad, int* d_err);
 int kls_mixed_slots(int device);
 int kls_mixed_splits_of(const kls_ctx* c);
+// K splits of the one-CTA form (the uneven batch runs that kernel body)
+int kls_mixed_legacy_splits(const kls_ctx* c);
 int kls_mixed_default_splits(const kls_ctx* c);
 int kls_mixed_set_form(kls_ctx* c, int form);
 int kls_mixed_form_of(const kls_ctx* c);
 int kls_mixed_set_splits(kls_ctx* c, int splits);
 const void* kls_mixed_tables(const kls_ctx* c, const void** Xl, const void** tmap_h,
                              const void** tmap_l);
+int kls_mixed_set_wait(kls_ctx* c, unsigned long long ns, int fault_mode);
+// TMEM-operand form of the split-BF16 contraction (kls_mixed_tm.cu)
+struct kls_mixed_tm;
+bool kls_tm_supported(const kls_ctx* c);
+int kls_tm_default_splits(const kls_ctx* c);
+int kls_tm_create(kls_ctx* c, const void* Xh, const void* Xl, kls_mixed_tm** out);
+void kls_tm_destroy(kls_mixed_tm* t);
+int kls_tm_splits(const kls_mixed_tm* t);
+void kls_tm_set_splits(const kls_ctx* c, kls_mixed_tm* t, int s);
+int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned long long wait_ns,
+                    int fault_skip);
+int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M);

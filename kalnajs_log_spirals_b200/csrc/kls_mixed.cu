@@ -31,6 +31,7 @@
 // (error flag for the host), and TMEM is released only after all issued MMAs
 // have completed.
 #include "kls_internal.cuh"
+#include "kls_tcgen05.cuh"
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <algorithm>
@@ -59,6 +60,18 @@ constexpr int MX_ACC_COLS = MX_OMEGA * MX_BN;          // 256 fp32 columns per b
 constexpr int MX_TMEM_COLS = 2 * MX_ACC_COLS;          // 512
 constexpr unsigned long long MX_WAIT_NS = 2000000000ull;   // 2 s per wait
 
+using namespace kls_tc;
+
+// bounded waits of the legacy kernels: the fixed MX_WAIT_NS bound
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort,
+                                          int* err, int code) {
+  return mbar_wait_lim(a, parity, abort, err, code, MX_WAIT_NS);
+}
+__device__ __forceinline__ bool mbar_wait_cl(uint32_t a, uint32_t parity, volatile int* abort,
+                                             int* err, int code) {
+  return mbar_wait_cl_lim(a, parity, abort, err, code, MX_WAIT_NS);
+}
+
 struct MixedParams {
   int Npad;            // N_alpha_pad
   int rows;            // 2 * Npad
@@ -69,122 +82,6 @@ struct MixedParams {
   int n_omega;
   int tiles_a;
 };
-
-// ---- small PTX helpers ----------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ unsigned long long globaltimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t a) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(uint32_t a, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t a, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      "selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(a), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait: false when the CTA is aborting or the wait timed out.
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort,
-                                          int* err, int code) {
-  unsigned long long t0 = 0;
-  for (uint32_t it = 0;; ++it) {
-    if (mbar_try(a, parity)) return true;
-    if (abort && *abort) return false;
-    if ((it & 63) == 0) {
-      unsigned long long t = globaltimer();
-      if (t0 == 0) t0 = t;
-      else if (t - t0 > MX_WAIT_NS) {
-        if (abort) *abort = 1;
-        atomicCAS(err, 0, code);
-        return false;
-      }
-    }
-  }
-}
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-// K-major, 128-byte swizzle UMMA shared-memory descriptor (sm100 format):
-// start >> 4 in [0,14), LBO >> 4 in [16,30) (unused here), SBO = 1024 B
-// (8 rows of 128 B) >> 4 in [32,46), version 1 at [46,48), layout
-// SWIZZLE_128B = 2 at [61,64).
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
-  d |= (uint64_t)1 << 16;
-  d |= (uint64_t)(1024 >> 4) << 32;
-  d |= (uint64_t)1 << 46;
-  d |= (uint64_t)2 << 61;
-  return d;
-}
-// kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major,
-// N >> 3 at [17,23), M >> 4 at [24,29).
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
-}
-__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
-                                     uint32_t acc) {
-  asm volatile(
-      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc));
-}
-__device__ __forceinline__ void umma_commit(uint32_t mbar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
-      : "memory");
-}
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                            uint32_t mbar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(mbar)
-      : "memory");
-}
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
-                                          uint32_t mbar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(dst),
-      "l"((uint64_t)src), "r"(bytes), "r"(mbar)
-      : "memory");
-}
-#define TMEM_LD32(taddr, r)                                                                      \
-  asm volatile(                                                                                  \
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13," \
-      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"        \
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),     \
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),              \
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),           \
-        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),           \
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),           \
-        "=r"(r[31])                                                                              \
-      : "r"(taddr))
 
 // ---- error-free split of the FP64 table --------------------------------------
 __device__ __forceinline__ void split2(double v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
@@ -233,20 +130,6 @@ __global__ void weights32_kernel(int64_t total, const double2* __restrict__ wt,
 }
 
 // ---- contraction -------------------------------------------------------------
-__device__ __forceinline__ float bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
-__device__ __forceinline__ float bf_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
-__device__ __forceinline__ uint32_t pack_split(float a, float b, uint32_t& lo) {
-  __nv_bfloat162 h = __floats2bfloat162_rn(a, b);          // .x = a (low half)
-  float ha = __low2float(h), hb = __high2float(h);
-  __nv_bfloat162 l = __floats2bfloat162_rn(a - ha, b - hb);
-  lo = *reinterpret_cast<uint32_t*>(&l);
-  return *reinterpret_cast<uint32_t*>(&h);
-}
-// byte offset of the 16-byte chunk (row n, k-chunk c) in a K-major SW128 tile
-__device__ __forceinline__ uint32_t sw128_off(int n, int c) {
-  return (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4));
-}
-
 __global__ void __launch_bounds__(MX_THREADS, 1)
 mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
                       const __grid_constant__ CUtensorMap tm_l, MixedParams P,
@@ -576,72 +459,6 @@ struct PairParams {
   int64_t K_pad;
   int nkb_total, kb_per_split, splits, n_omega, tiles_a;
 };
-
-__device__ __forceinline__ uint32_t mapa_u32(uint32_t a, uint32_t rank) {
-  uint32_t r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
-  return r;
-}
-__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_cl(uint32_t a, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n.reg .pred p;\nmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
-      "selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(a), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait, cluster-scope acquire (barriers that the peer CTA completes)
-__device__ __forceinline__ bool mbar_wait_cl(uint32_t a, uint32_t parity, volatile int* abort,
-                                             int* err, int code) {
-  unsigned long long t0 = 0;
-  for (uint32_t it = 0;; ++it) {
-    if (mbar_try_cl(a, parity)) return true;
-    if (abort && *abort) return false;
-    if ((it & 63) == 0) {
-      unsigned long long t = globaltimer();
-      if (t0 == 0) t0 = t;
-      else if (t - t0 > MX_WAIT_NS) {
-        if (abort) *abort = 1;
-        atomicCAS(err, 0, code);
-        return false;
-      }
-    }
-  }
-}
-__device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
-                                          uint32_t acc) {
-  asm volatile(
-      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc));
-}
-// commit of the leader's MMAs to the barrier at this offset in both CTAs
-__device__ __forceinline__ void umma_pair_commit(uint32_t mbar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
-      " [%0], %1;" ::"r"(mbar),
-      "h"((unsigned short)3)
-      : "memory");
-}
-// TMA into this CTA's shared memory, completing on the leader's barrier
-__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                                 uint32_t mbar_cluster) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(mbar_cluster)
-      : "memory");
-}
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" ::
-                   : "memory");
-}
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(MX_THREADS, 1)
 mixed_pair_kernel(const __grid_constant__ CUtensorMap tm_h, const __grid_constant__ CUtensorMap tm_l,
@@ -980,10 +797,6 @@ __global__ void multi_mixed_reduce_kernel(const kls_mdesc* __restrict__ md,
                     nullptr);
 }
 
-__device__ __forceinline__ void tensormap_acquire(const void* map) {
-  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((uint64_t)map)
-               : "memory");
-}
 
 // Persistent form of mixed_contract_kernel over an uneven batch of models.
 // CTA b takes items [starts[b], starts[b+1]) of a list the host ordered
@@ -1338,7 +1151,10 @@ struct kls_mixed {
   size_t wt32_elems = 0;
   int* err = nullptr;
   int splits = 1;
-  int form = KLS_MIXED_ONE_CTA;   // contraction kernel: one CTA or a CTA pair per tile
+  int form = KLS_MIXED_ONE_CTA;   // contraction kernel (KLS_MIXED_*)
+  kls_mixed_tm* tm = nullptr;     // TMEM-operand form (N_alpha_pad <= 384)
+  unsigned long long wait_ns = 2000000000ull;   // its wait bound
+  int fault_mode = 0;             // test hook of the failure path (one-shot)
 };
 
 static int mixed_splits(const kls_ctx* c) {
@@ -1394,6 +1210,11 @@ int kls_mixed_prepare(kls_ctx* c) {
     if (r != CUDA_SUCCESS) return kls_fail(c, KLS_ERR_CUDA, "cuTensorMapEncodeTiled failed");
   }
   m->splits = mixed_splits(c);
+  if (kls_tm_supported(c)) {
+    int r = kls_tm_create(c, m->Xh, m->Xl, &m->tm);
+    if (r) return r;
+    m->form = KLS_MIXED_TMEM;
+  }
   KLS_CK(c, cudaFuncSetAttribute(mixed_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)MX_SMEM));
   KLS_CK(c, cudaFuncSetAttribute(mixed_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1404,6 +1225,11 @@ int kls_mixed_prepare(kls_ctx* c) {
 
 int kls_mixed_contract(kls_ctx* c, int n, int) {
   kls_mixed* m = c->mixed;
+  if (m->form == KLS_MIXED_TMEM) {
+    const int fault = m->fault_mode;
+    m->fault_mode = 0;
+    return kls_tm_contract(c, m->tm, n, m->err, m->wait_ns, fault);
+  }
   const size_t R = 2 * (size_t)c->Na_pad;
   const size_t need = (size_t)n * m->splits * R * R;
   if (need > m->part_elems) {
@@ -1459,6 +1285,7 @@ int kls_mixed_contract(kls_ctx* c, int n, int) {
 
 int kls_mixed_reduce(kls_ctx* c, int n, bool export_M) {
   kls_mixed* m = c->mixed;
+  if (m->form == KLS_MIXED_TMEM) return kls_tm_reduce(c, m->tm, n, export_M);
   int blocks = std::min((c->Na * c->Na + 255) / 256, 1024);
   mixed_reduce_kernel<<<dim3(blocks, n), 256, 0, c->stream>>>(
       c->Na, c->Na_pad, m->splits, c->cfg.G, c->d_N, m->part, c->d_A, export_M ? c->d_M : nullptr);
@@ -1472,8 +1299,9 @@ int kls_mixed_check(kls_ctx* c) {
   KLS_CK(c, cudaMemcpy(&h, c->mixed->err, sizeof(int), cudaMemcpyDeviceToHost));
   if (h) {
     cudaMemset(c->mixed->err, 0, sizeof(int));
-    return kls_fail(c, KLS_ERR_CUDA, "mixed contraction pipeline timed out (code " +
-                                         std::to_string(h) + ")");
+    return kls_fail(c, KLS_ERR_TIMEOUT,
+                    "mixed contraction pipeline: a bounded wait ran out (code " +
+                        std::to_string(h) + "); results of this call are invalid");
   }
   return KLS_OK;
 }
@@ -1485,6 +1313,7 @@ void kls_mixed_free(kls_ctx* c) {
   cudaFree(c->mixed->part);
   cudaFree(c->mixed->wt32);
   cudaFree(c->mixed->err);
+  kls_tm_destroy(c->mixed->tm);
   delete c->mixed;
   c->mixed = nullptr;
 }
@@ -1517,13 +1346,30 @@ int kls_mixed_slots(int device) {
   return sms * per_sm;
 }
 
-int kls_mixed_splits_of(const kls_ctx* c) { return c->mixed ? c->mixed->splits : 0; }
+int kls_mixed_splits_of(const kls_ctx* c) {
+  if (!c->mixed) return 0;
+  return c->mixed->form == KLS_MIXED_TMEM ? kls_tm_splits(c->mixed->tm) : c->mixed->splits;
+}
 
-int kls_mixed_default_splits(const kls_ctx* c) { return mixed_splits(c); }
+int kls_mixed_legacy_splits(const kls_ctx* c) { return c->mixed ? c->mixed->splits : 0; }
+
+int kls_mixed_default_splits(const kls_ctx* c) {
+  if (c->mixed && c->mixed->form == KLS_MIXED_TMEM) return kls_tm_default_splits(c);
+  return mixed_splits(c);
+}
 
 int kls_mixed_set_form(kls_ctx* c, int form) {
   if (!c->mixed) return KLS_ERR_STATE;
+  if (form == KLS_MIXED_TMEM && !c->mixed->tm)
+    return kls_fail(c, KLS_ERR_UNSUPPORTED, "KLS_MIXED_TMEM needs N_alpha_pad <= 384");
   c->mixed->form = form;
+  return KLS_OK;
+}
+
+int kls_mixed_set_wait(kls_ctx* c, unsigned long long ns, int fault_mode) {
+  if (!c->mixed) return KLS_ERR_STATE;
+  if (ns) c->mixed->wait_ns = ns;
+  if (fault_mode >= 0) c->mixed->fault_mode = fault_mode;
   return KLS_OK;
 }
 
@@ -1531,6 +1377,10 @@ int kls_mixed_form_of(const kls_ctx* c) { return c->mixed ? c->mixed->form : 0; 
 
 int kls_mixed_set_splits(kls_ctx* c, int splits) {
   if (!c->mixed) return KLS_ERR_STATE;
+  if (c->mixed->form == KLS_MIXED_TMEM) {
+    kls_tm_set_splits(c, c->mixed->tm, splits);
+    return KLS_OK;
+  }
   const int nkb = (int)(c->K_pad / MX_BK);
   c->mixed->splits = std::max(1, std::min(splits, nkb));
   return KLS_OK;

@@ -1,0 +1,534 @@
+// Split-BF16 contraction with the omega-dependent operand in tensor memory
+// (KLS_MIXED_TMEM, the default form of KLS_MODE_MIXED for N_alpha_pad <= 384).
+//
+//   M(omega)[b, a] = sum_k W[k, b] U[k, a],   U = w(omega) conj(W)
+//   M_r = sum_k ReW_b ReU_a - ImW_b ImU_a,    M_i = sum_k ReW_b ImU_a + ImW_b ReU_a
+//
+// A stage covers 32 complex k and 64 real contraction indices k': the first
+// 32 pair Re W with the coefficient rows, the next 32 pair Im W.  With
+//   B row b     = [ReW_b(k) | ImW_b(k)]            (omega-independent table)
+//   A row (a,r) = [ReU_a(k) | -ImU_a(k)],  A row (a,i) = [ImU_a(k) | ReU_a(k)]
+// one real GEMM D = A B^T gives M_r[b, a] = D[(a,r), b], M_i[b, a] = D[(a,i), b]
+// with every A row formed exactly once per omega (the older forms re-form the
+// omega-dependent operand once per 128-row output tile).
+//
+// CTA pair (cluster of 2, tcgen05 cta_group::2, MMA M = 256).  Each CTA owns
+// one "tile": 64 alphas of one omega = 128 A rows.  Its producer warps form
+// the A rows in FP32 from the table rows of its alphas (TMA-staged), split
+// them error-free into BF16 hi + lo and store them straight into tensor
+// memory (tcgen05.st); the MMA reads A from TMEM and B from shared memory.
+// B is the whole table row range [0, Npad) for the stage: each CTA loads half
+// of it (64-byte swizzled TMA tiles of the split table Xh / Xl, Re rows a and
+// Im rows Npad + a), so each SM reads Npad / 2 table rows per stage.  The
+// accumulator (128 lanes x Npad FP32 columns per CTA) holds every output row
+// b and is flushed every TM_CHUNK stages into an FP64 partial per (tile, K
+// split) in deterministic order; the split sum, G N(a) scaling, I - M, the
+// weights and the LU are FP64.  Products hi*hi + lo*hi + hi*lo (the lo*lo
+// term, ~2^-18 relative, is dropped).
+//
+// Warps (640 threads):
+//   0       TMA: both B half tiles (completing on the leader's barrier) and
+//           this CTA's A-source tiles (its 64 alphas)
+//   1       MMA issuer (leader CTA, one thread)
+//   2       TMEM allocation / release (512 columns: D at [0, Npad), two A
+//           stages at [384, 512))
+//   3       weights ring: bulk copies of the FP32 w(omega) of the CTA's omega
+//   4..11   producers, 2 per TMEM lane quadrant (Re / Im coefficient halves)
+//   12..19  drain, 2 per lane quadrant (halves of the D columns): TMEM ->
+//           FP64 partial
+// Every wait is bounded (the context's wait limit, 2 s by default); a wait
+// that runs out records a code in the error flag (KLS_ERR_TIMEOUT on the
+// host) and the CTA pair winds down; TMEM is released after all issued MMAs
+// completed.
+#include "kls_internal.cuh"
+#include "kls_tcgen05.cuh"
+#include <algorithm>
+
+namespace {
+using namespace kls_tc;
+
+constexpr int TM_AB = 64;              // alphas per CTA (128 A rows)
+constexpr int TM_KB = 32;              // complex k per stage
+constexpr int TM_STAGES = 3;           // shared-memory stages (B halves + A sources)
+constexpr int TM_ASTAGES = 2;          // TMEM stages of A
+constexpr int TM_WSTAGES = 8;          // weights ring
+constexpr int TM_CHUNK = 128;          // stages per FP32 accumulation chunk (4096 complex k)
+constexpr int TM_THREADS = 640;
+constexpr int TM_NPROD = 8;            // producer warps 4..11
+constexpr int TM_NDRAIN = 8;           // drain warps 12..19
+constexpr uint32_t TM_ACOL = 384;      // TMEM column of A stage 0 (64 columns per stage)
+constexpr int TM_TMEM_COLS = 512;
+constexpr int TM_YTILE = TM_AB * TM_KB * 2;   // 4 KB: 64 rows x 64 B
+constexpr int TM_WBYTES = TM_KB * 8;          // float2 weights of one stage
+
+__host__ __device__ constexpr int tm_btile(int Npad) { return (Npad / 2) * TM_KB * 2; }
+__host__ __device__ constexpr int tm_stage_bytes(int Npad) {
+  return 4 * tm_btile(Npad) + 4 * TM_YTILE;
+}
+size_t tm_smem(int Npad) {
+  return (size_t)TM_STAGES * tm_stage_bytes(Npad) + TM_WSTAGES * TM_WBYTES + 1024;
+}
+
+struct TmParams {
+  int Npad;                 // N_alpha_pad (<= 384, multiple of 64)
+  int tiles_a;              // Npad / 64
+  int n_tiles;              // n_omega * tiles_a
+  int splits, kb_per_split, nkb_total;
+  int64_t K_pad;
+  unsigned long long wait_ns;
+  int fault_skip;           // test hook: one producer arrival is skipped
+};
+
+// output row b of the table for accumulator column j (the pair splits each
+// MMA's N columns: the first half from the leader's B rows, the rest from the
+// peer's; CTA c holds table rows [c Npad/2, (c+1) Npad/2))
+__device__ __forceinline__ int tm_brow(int j, int Nh, int Nh2) {
+  const int nh = j / Nh, jj = j - nh * Nh, h2 = Nh >> 1;
+  return jj < h2 ? nh * h2 + jj : Nh2 + nh * h2 + (jj - h2);
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TM_THREADS, 1)
+mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant__ CUtensorMap tb_l,
+                const __grid_constant__ CUtensorMap ty_h, const __grid_constant__ CUtensorMap ty_l,
+                TmParams P, const float2* __restrict__ wt32, double* __restrict__ part,
+                int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_b_full[TM_STAGES], bar_b_empty[TM_STAGES],
+      bar_y_full[TM_STAGES], bar_y_empty[TM_STAGES], bar_w_full[TM_WSTAGES],
+      bar_w_empty[TM_WSTAGES], bar_a_full[TM_ASTAGES], bar_a_empty[TM_ASTAGES], bar_acc_full,
+      bar_acc_empty, bar_done;
+  __shared__ uint32_t s_tmem;
+  __shared__ volatile int s_abort;
+
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint32_t crank;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(crank));
+  const bool leader = crank == 0;
+  const int tile = 2 * (int)(blockIdx.x >> 1) + (int)crank;
+  const bool dummy = tile >= P.n_tiles;      // odd tile count: the last peer only loads B
+  const int tile_e = dummy ? 0 : tile;
+  const int om = tile_e / P.tiles_a;
+  const int a0 = (tile_e % P.tiles_a) * TM_AB;
+  const int split = blockIdx.y;
+  const int kb0 = split * P.kb_per_split;
+  const int nkb = max(0, min(P.nkb_total, kb0 + P.kb_per_split) - kb0);
+  const int nch = (nkb + TM_CHUNK - 1) / TM_CHUNK;
+  const int Nh2 = P.Npad / 2;                // table rows per CTA
+  const int nmma = P.Npad > 256 ? 2 : 1;     // MMAs along N
+  const int Nh = P.Npad / nmma;              // N of each MMA
+  const int SB = tm_stage_bytes(P.Npad), BT = tm_btile(P.Npad);
+  const unsigned long long lim = P.wait_ns;
+
+  // B tile (part 0 hi / 1 lo, sub 0 Re rows / 1 Im rows) and A-source tile
+  auto b_tile = [&](int s, int pt, int sub) {
+    return smem + (size_t)s * SB + (size_t)(2 * pt + sub) * BT;
+  };
+  auto y_tile = [&](int s, int pt, int sub) {
+    return smem + (size_t)s * SB + 4 * (size_t)BT + (size_t)(2 * pt + sub) * TM_YTILE;
+  };
+  uint8_t* wring = smem + (size_t)TM_STAGES * SB;
+
+  if (tid == 0) {
+    s_abort = 0;
+    for (int s = 0; s < TM_STAGES; ++s) {
+      mbar_init(smem_u32(&bar_b_full[s]), 1);
+      mbar_init(smem_u32(&bar_b_empty[s]), 1);
+      mbar_init(smem_u32(&bar_y_full[s]), 1);
+      mbar_init(smem_u32(&bar_y_empty[s]), TM_NPROD);
+    }
+    for (int s = 0; s < TM_WSTAGES; ++s) {
+      mbar_init(smem_u32(&bar_w_full[s]), 1);
+      mbar_init(smem_u32(&bar_w_empty[s]), TM_NPROD);
+    }
+    for (int s = 0; s < TM_ASTAGES; ++s) {
+      mbar_init(smem_u32(&bar_a_full[s]), 2 * TM_NPROD);
+      mbar_init(smem_u32(&bar_a_empty[s]), 1);
+    }
+    mbar_init(smem_u32(&bar_acc_full), 1);
+    mbar_init(smem_u32(&bar_acc_empty), 2 * TM_NDRAIN);
+    mbar_init(smem_u32(&bar_done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2 && nkb > 0) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(TM_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();            // both CTAs' barriers initialised, TMEM allocated
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+
+  if (warp == 0) {
+    // ---------------- TMA: B halves (leader's barrier) + A-source tiles (own)
+    if (lane == 0 && nkb > 0) {
+      int issued = 0;
+      const int yb = (int)crank * Nh2;
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % TM_STAGES, r = i / TM_STAGES;
+        if (!mbar_wait_cl_lim(smem_u32(&bar_b_empty[s]), (r & 1) ^ 1, &s_abort, err, 1, lim)) break;
+        if (!mbar_wait_lim(smem_u32(&bar_y_empty[s]), (r & 1) ^ 1, &s_abort, err, 11, lim)) break;
+        const int kx = (kb0 + i) * TM_KB;
+        if (leader) mbar_arrive_tx(smem_u32(&bar_b_full[s]), 2 * 4 * BT);
+        const uint32_t fb = mapa_u32(smem_u32(&bar_b_full[s]), 0);
+        tma_load_2d_pair(smem_u32(b_tile(s, 0, 0)), &tb_h, kx, yb, fb);
+        tma_load_2d_pair(smem_u32(b_tile(s, 0, 1)), &tb_h, kx, P.Npad + yb, fb);
+        tma_load_2d_pair(smem_u32(b_tile(s, 1, 0)), &tb_l, kx, yb, fb);
+        tma_load_2d_pair(smem_u32(b_tile(s, 1, 1)), &tb_l, kx, P.Npad + yb, fb);
+        const uint32_t yf = smem_u32(&bar_y_full[s]);
+        mbar_arrive_tx(yf, 4 * TM_YTILE);
+        tma_load_2d(smem_u32(y_tile(s, 0, 0)), &ty_h, kx, a0, yf);
+        tma_load_2d(smem_u32(y_tile(s, 0, 1)), &ty_h, kx, P.Npad + a0, yf);
+        tma_load_2d(smem_u32(y_tile(s, 1, 0)), &ty_l, kx, a0, yf);
+        tma_load_2d(smem_u32(y_tile(s, 1, 1)), &ty_l, kx, P.Npad + a0, yf);
+        issued = i + 1;
+      }
+      // the last copies into this CTA's shared memory land before it may exit
+      // (the peer's B copies complete on the leader's barrier, which the
+      // leader checks; the final cluster barrier orders the peer's exit)
+      for (int i = max(0, issued - TM_STAGES); i < issued; ++i) {
+        mbar_wait_lim(smem_u32(&bar_y_full[i % TM_STAGES]), (i / TM_STAGES) & 1, nullptr, err, 6,
+                      lim);
+        if (leader)
+          mbar_wait_cl_lim(smem_u32(&bar_b_full[i % TM_STAGES]), (i / TM_STAGES) & 1, nullptr,
+                           err, 6, lim);
+      }
+    }
+  } else if (warp == 3) {
+    // ---------------- weights ring
+    if (lane == 0 && nkb > 0) {
+      int issued = 0;
+      const float2* wz = wt32 + (size_t)om * P.K_pad;
+      for (int i = 0; i < nkb; ++i) {
+        const int ws = i % TM_WSTAGES, r = i / TM_WSTAGES;
+        if (!mbar_wait_lim(smem_u32(&bar_w_empty[ws]), (r & 1) ^ 1, &s_abort, err, 10, lim)) break;
+        const uint32_t wb = smem_u32(&bar_w_full[ws]);
+        mbar_arrive_tx(wb, TM_WBYTES);
+        bulk_load(smem_u32(wring + ws * TM_WBYTES), wz + (size_t)(kb0 + i) * TM_KB, TM_WBYTES, wb);
+        issued = i + 1;
+      }
+      for (int i = max(0, issued - TM_WSTAGES); i < issued; ++i)
+        mbar_wait_lim(smem_u32(&bar_w_full[i % TM_WSTAGES]), (i / TM_WSTAGES) & 1, nullptr, err,
+                      6, lim);
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer (leader)
+    if (leader && lane == 0 && nkb > 0) {
+      const uint32_t idesc = idesc_bf16(256, Nh);
+      for (int i = 0; i < nkb; ++i) {
+        const int s = i % TM_STAGES, as = i % TM_ASTAGES;
+        const int ci = i % TM_CHUNK, ch = i / TM_CHUNK;
+        const bool first = ci == 0;
+        const bool last = ci == TM_CHUNK - 1 || i == nkb - 1;
+        if (first && ch > 0 &&
+            !mbar_wait_cl_lim(smem_u32(&bar_acc_empty), (ch - 1) & 1, &s_abort, err, 7, lim))
+          break;
+        if (!mbar_wait_cl_lim(smem_u32(&bar_b_full[s]), (i / TM_STAGES) & 1, &s_abort, err, 2, lim))
+          break;
+        if (!mbar_wait_cl_lim(smem_u32(&bar_a_full[as]), (i / TM_ASTAGES) & 1, &s_abort, err, 3,
+                              lim))
+          break;
+        tc_fence_after();
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const int sub = kk >> 1;                       // Re rows, then Im rows
+          const uint32_t kb = (uint32_t)(kk & 1) * 32;   // bytes: k 0..15 / 16..31
+          const uint32_t a_hi = tmem + TM_ACOL + (uint32_t)(as * 64 + kk * 8);
+          const uint32_t a_lo = a_hi + 32;
+          for (int nh = 0; nh < nmma; ++nh) {
+            const uint32_t d = tmem + (uint32_t)(nh * Nh);
+            const uint32_t boff = (uint32_t)(nh * (Nh >> 1) * 64) + kb;
+            const uint64_t bh = sw64_desc(smem_u32(b_tile(s, 0, sub)) + boff);
+            const uint64_t bl = sw64_desc(smem_u32(b_tile(s, 1, sub)) + boff);
+            umma_pair_ts(d, a_hi, bh, idesc, (first && kk == 0) ? 0u : 1u);
+            umma_pair_ts(d, a_lo, bh, idesc, 1u);
+            umma_pair_ts(d, a_hi, bl, idesc, 1u);
+          }
+        }
+        umma_pair_commit(smem_u32(&bar_b_empty[s]));
+        umma_pair_commit(smem_u32(&bar_a_empty[as]));
+        if (last) umma_pair_commit(smem_u32(&bar_acc_full));
+      }
+      // completion of every issued MMA (also on the abort path)
+      umma_pair_commit(smem_u32(&bar_done));
+    }
+  } else if (warp >= 4 && warp < 4 + TM_NPROD) {
+    // ---------------- producers: A rows of this CTA's 64 alphas into TMEM
+    const int pw = warp - 4, q = pw & 3, h = pw >> 2;
+    const int l = 32 * q + lane;               // TMEM lane = A row
+    const int al = l >> 1, p = l & 1;          // alpha (local), row (a, r) / (a, i)
+    // half 0 (Re W columns): (a, r) <- Re U, (a, i) <- Im U;
+    // half 1 (Im W columns): (a, r) <- -Im U, (a, i) <- Re U
+    const bool use_re = h == p;
+    const float sgn = (h == 1 && p == 0) ? -1.f : 1.f;
+    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16) + TM_ACOL + (uint32_t)(h * 16);
+    const bool skip_one = P.fault_skip && leader && blockIdx.x == 0 && blockIdx.y == 0 && pw == 0;
+    for (int i = 0; i < nkb; ++i) {
+      const int s = i % TM_STAGES, as = i % TM_ASTAGES, ws = i % TM_WSTAGES;
+      bool ok = mbar_wait_lim(smem_u32(&bar_y_full[s]), (i / TM_STAGES) & 1, &s_abort, err, 4, lim);
+      if (ok) ok = mbar_wait_lim(smem_u32(&bar_w_full[ws]), (i / TM_WSTAGES) & 1, &s_abort, err, 8,
+                                 lim);
+      if (ok) ok = mbar_wait_cl_lim(smem_u32(&bar_a_empty[as]), ((i / TM_ASTAGES) & 1) ^ 1,
+                                    &s_abort, err, 12, lim);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      tc_fence_after();
+      const float4* wz = reinterpret_cast<const float4*>(wring + ws * TM_WBYTES);
+      uint32_t hi[16], lo[16];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        // 16-byte chunk c of the alpha's table rows: k = 8c .. 8c + 7
+        const uint32_t off = sw64_off(al, c);
+        const uint4 Rh = *reinterpret_cast<const uint4*>(y_tile(s, 0, 0) + off);
+        const uint4 Ih = *reinterpret_cast<const uint4*>(y_tile(s, 0, 1) + off);
+        const uint4 Rl = *reinterpret_cast<const uint4*>(y_tile(s, 1, 0) + off);
+        const uint4 Il = *reinterpret_cast<const uint4*>(y_tile(s, 1, 1) + off);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int j = 4 * c + e;               // k = 2j, 2j + 1
+          const uint32_t rh = (&Rh.x)[e], rl = (&Rl.x)[e], ih = (&Ih.x)[e], il = (&Il.x)[e];
+          const float wr0 = bf_lo(rh) + bf_lo(rl), wr1 = bf_hi(rh) + bf_hi(rl);
+          const float wi0 = bf_lo(ih) + bf_lo(il), wi1 = bf_hi(ih) + bf_hi(il);
+          const float4 w = wz[j];                // (w_2j, w_2j+1)
+          // U = w conj(W): Re U = wr Wr + wi Wi, Im U = wi Wr - wr Wi
+          const float v0 = use_re ? __fmaf_rn(w.x, wr0, __fmul_rn(w.y, wi0))
+                                  : __fmaf_rn(w.y, wr0, -__fmul_rn(w.x, wi0));
+          const float v1 = use_re ? __fmaf_rn(w.z, wr1, __fmul_rn(w.w, wi1))
+                                  : __fmaf_rn(w.w, wr1, -__fmul_rn(w.z, wi1));
+          hi[j] = pack_split(sgn * v0, sgn * v1, lo[j]);
+        }
+      }
+      TMEM_ST16(tl + (uint32_t)(as * 64), hi);
+      TMEM_ST16(tl + (uint32_t)(as * 64 + 32), lo);
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(smem_u32(&bar_y_empty[s]));
+        mbar_arrive(smem_u32(&bar_w_empty[ws]));
+        if (!(skip_one && i == 0)) {
+          if (leader) mbar_arrive(smem_u32(&bar_a_full[as]));
+          else mbar_arrive_remote(mapa_u32(smem_u32(&bar_a_full[as]), 0));
+        }
+      }
+    }
+  } else if (warp >= 4 + TM_NPROD) {
+    // ---------------- drain: D chunk -> FP64 partial [tile][split][b][A row]
+    const int dw = warp - 4 - TM_NPROD, q = dw & 3, half = dw >> 2;
+    const int l = 32 * q + lane;
+    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16);
+    double* out = part + ((size_t)tile_e * P.splits + split) * (size_t)P.Npad * 128 + l;
+    const int c0 = half * Nh2;
+    for (int ch = 0; ch < nch; ++ch) {
+      const bool ok =
+          mbar_wait_cl_lim(smem_u32(&bar_acc_full), ch & 1, &s_abort, err, 9, lim);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      tc_fence_after();
+      for (int cb = 0; cb < Nh2 / 16; ++cb) {
+        const int j0 = c0 + 16 * cb;
+        uint32_t v[16];
+        TMEM_LD16(tl + (uint32_t)j0, v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (dummy) continue;
+        // the 16 columns map to at most two runs of consecutive table rows
+        double old[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+          old[t] = ch > 0 ? out[(size_t)tm_brow(j0 + t, Nh, Nh2) * 128] : 0.0;
+#pragma unroll
+        for (int t = 0; t < 16; ++t)
+          out[(size_t)tm_brow(j0 + t, Nh, Nh2) * 128] = old[t] + (double)__uint_as_float(v[t]);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        if (leader) mbar_arrive(smem_u32(&bar_acc_empty));
+        else mbar_arrive_remote(mapa_u32(smem_u32(&bar_acc_empty), 0));
+      }
+    }
+  }
+  __syncwarp();
+  tc_fence_before();
+  __syncthreads();
+  // every role has finished; all MMAs complete before TMEM is released
+  if (warp == 2 && nkb > 0) mbar_wait_cl_lim(smem_u32(&bar_done), 0, nullptr, err, 5, lim);
+  cluster_sync_all();            // no CTA leaves while its peer may still touch it
+  if (warp == 2 && nkb > 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TM_TMEM_COLS));
+  }
+}
+
+// FP32 copy of the weights, plain [omega][K_pad] order
+__global__ void tm_weights32_kernel(int64_t total, const double2* __restrict__ wt,
+                                    float2* __restrict__ wt32) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = wt[i];
+    wt32[i] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+// split sum, * G * N(a), I - M: partial [tile][split][b][2 a_local + (0 r | 1 i)]
+__global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, double G,
+                                 const double* __restrict__ Nk, const double* __restrict__ part,
+                                 double2* __restrict__ A, double2* __restrict__ Mout) {
+  const int z = blockIdx.y;
+  const size_t plane = (size_t)Npad * 128;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
+    const int b = e / Na, a = e % Na;
+    const int at = a / TM_AB, l2 = 2 * (a % TM_AB);
+    const double* src = part + (size_t)(z * tiles_a + at) * splits * plane + (size_t)b * 128 + l2;
+    double sr = 0.0, si = 0.0;
+    for (int s = 0; s < splits; ++s) {
+      sr += src[(size_t)s * plane];
+      si += src[(size_t)s * plane + 1];
+    }
+    const double n = Nk[a];
+    const double mr = __dmul_rn(__dmul_rn(sr, G), n), mi = __dmul_rn(__dmul_rn(si, G), n);
+    A[(size_t)z * Na * Na + e] = make_double2((a == b ? 1.0 : 0.0) - mr, -mi);
+    if (Mout && z == 0) Mout[e] = make_double2(mr, mi);
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+}  // namespace
+
+struct kls_mixed_tm {
+  CUtensorMap tb_h, tb_l, ty_h, ty_l;
+  int splits = 1;
+  double* part = nullptr;       // [n tiles][splits][Npad][128]
+  size_t part_elems = 0;
+  float2* wt32 = nullptr;       // [n][K_pad]
+  size_t wt32_elems = 0;
+};
+
+bool kls_tm_supported(const kls_ctx* c) {
+  return c->Na_pad % TM_AB == 0 && c->Na_pad <= 384 && c->K_pad % TM_KB == 0;
+}
+
+// K splits of the form: fixed per context (determinants do not depend on the
+// batch), chosen so that a Newton triple's tile pairs fill whole waves of
+// CTA pairs twice over
+int kls_tm_default_splits(const kls_ctx* c) {
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  const int tiles_a = c->Na_pad / TM_AB;
+  const int pairs3 = (3 * tiles_a + 1) / 2;
+  const int nkb = (int)(c->K_pad / TM_KB);
+  return std::max(1, std::min(nkb, 2 * std::max(1, (sms / 2) / pairs3)));
+}
+
+int kls_tm_create(kls_ctx* c, const void* Xh, const void* Xl, kls_mixed_tm** out) {
+  *out = nullptr;
+  if (!kls_tm_supported(c)) return kls_fail(c, KLS_ERR_UNSUPPORTED, "N_alpha_pad > 384");
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  KLS_CK(c, cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (!fn || q != cudaDriverEntryPointSuccess)
+    return kls_fail(c, KLS_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  EncodeTiledFn encode = (EncodeTiledFn)fn;
+  kls_mixed_tm* t = new kls_mixed_tm();
+  const cuuint64_t dims[2] = {(cuuint64_t)c->K_pad, (cuuint64_t)(2 * c->Na_pad)};
+  const cuuint64_t strides[1] = {(cuuint64_t)c->K_pad * sizeof(__nv_bfloat16)};
+  const cuuint32_t estr[2] = {1, 1};
+  const cuuint32_t box_b[2] = {TM_KB, (cuuint32_t)(c->Na_pad / 2)};
+  const cuuint32_t box_y[2] = {TM_KB, TM_AB};
+  struct { CUtensorMap* m; const void* base; const cuuint32_t* box; } maps[4] = {
+      {&t->tb_h, Xh, box_b}, {&t->tb_l, Xl, box_b}, {&t->ty_h, Xh, box_y}, {&t->ty_l, Xl, box_y}};
+  for (auto& mm : maps) {
+    CUresult r = encode(mm.m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(mm.base),
+                        dims, strides, mm.box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      delete t;
+      return kls_fail(c, KLS_ERR_CUDA, "cuTensorMapEncodeTiled failed (TMEM-operand form)");
+    }
+  }
+  t->splits = kls_tm_default_splits(c);
+  cudaError_t e = cudaFuncSetAttribute(mixed_tm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)tm_smem(c->Na_pad));
+  if (e != cudaSuccess) {
+    delete t;
+    return kls_cuda_fail(c, e, "cudaFuncSetAttribute (TMEM-operand form)");
+  }
+  *out = t;
+  return KLS_OK;
+}
+
+void kls_tm_destroy(kls_mixed_tm* t) {
+  if (!t) return;
+  cudaFree(t->part);
+  cudaFree(t->wt32);
+  delete t;
+}
+
+int kls_tm_splits(const kls_mixed_tm* t) { return t->splits; }
+
+void kls_tm_set_splits(const kls_ctx* c, kls_mixed_tm* t, int s) {
+  t->splits = std::max(1, std::min(s, (int)(c->K_pad / TM_KB)));
+}
+
+int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned long long wait_ns,
+                    int fault_skip) {
+  const int tiles_a = c->Na_pad / TM_AB;
+  const int nkb_total = (int)(c->K_pad / TM_KB);
+  const int kbs = (nkb_total + t->splits - 1) / t->splits;
+  const int splits = (nkb_total + kbs - 1) / kbs;          // no empty split
+  const int n_tiles = n * tiles_a;
+  const size_t need = (size_t)n_tiles * splits * c->Na_pad * 128;
+  if (need > t->part_elems) {
+    cudaFree(t->part);
+    t->part = nullptr;
+    t->part_elems = 0;
+    KLS_CK(c, cudaMalloc(&t->part, need * sizeof(double)));
+    t->part_elems = need;
+  }
+  const size_t nw = (size_t)n * c->K_pad;
+  if (nw > t->wt32_elems) {
+    cudaFree(t->wt32);
+    t->wt32 = nullptr;
+    t->wt32_elems = 0;
+    KLS_CK(c, cudaMalloc(&t->wt32, nw * sizeof(float2)));
+    t->wt32_elems = nw;
+  }
+  tm_weights32_kernel<<<(unsigned)std::min<size_t>((nw + 255) / 256, 4096), 256, 0, c->stream>>>(
+      (int64_t)nw, c->d_wt, t->wt32);
+  KLS_LAUNCHED(c);
+  TmParams P{};
+  P.Npad = c->Na_pad;
+  P.tiles_a = tiles_a;
+  P.n_tiles = n_tiles;
+  P.splits = splits;
+  P.kb_per_split = kbs;
+  P.nkb_total = nkb_total;
+  P.K_pad = c->K_pad;
+  P.wait_ns = wait_ns;
+  P.fault_skip = fault_skip;
+  const int pairs = (n_tiles + 1) / 2;
+  dim3 grid((unsigned)(2 * pairs), (unsigned)splits);
+  mixed_tm_kernel<<<grid, TM_THREADS, tm_smem(c->Na_pad), c->stream>>>(
+      t->tb_h, t->tb_l, t->ty_h, t->ty_l, P, t->wt32, t->part, d_err);
+  KLS_LAUNCHED(c);
+  return KLS_OK;
+}
+
+int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M) {
+  const int nkb_total = (int)(c->K_pad / TM_KB);
+  const int kbs = (nkb_total + t->splits - 1) / t->splits;
+  const int splits = (nkb_total + kbs - 1) / kbs;
+  int blocks = std::min((c->Na * c->Na + 255) / 256, 1024);
+  tm_reduce_kernel<<<dim3(blocks, n), 256, 0, c->stream>>>(
+      c->Na, c->Na_pad, c->Na_pad / TM_AB, splits, c->cfg.G, c->d_N, t->part, c->d_A,
+      export_M ? c->d_M : nullptr);
+  KLS_LAUNCHED(c);
+  return KLS_OK;
+}

@@ -402,7 +402,7 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
       d.tmap_h = dm;
       d.tmap_l = dm + sizeof(CUtensorMap);
       d.nkb_total = (int)(c->K_pad / MIX_BK);
-      const int s = kls_mixed_splits_of(c);
+      const int s = kls_mixed_legacy_splits(c);
       d.kb_per_split = (d.nkb_total + s - 1) / s;
       d.msplits = (d.nkb_total + d.kb_per_split - 1) / d.kb_per_split;   // non-empty splits
       d.om_per_item = 2;

@@ -60,11 +60,25 @@ function check(h, code)
     error("libkls status $code: $msg")
 end
 
+const QUAD_CODES = Dict('t' => Int32(1), 's' => Int32(2), 'b' => Int32(3))
+
+"""Quadrature rules of the alpha, ln Rc and v grids: the `quadrature` field of
+the grid config when it has one (three letters of t/s/b, the --quad option of
+NL_julia_boole.jl:14-16), else the package's rules ("tts")."""
+function quad_codes(g)
+    q = hasproperty(g, :quadrature) ? String(getproperty(g, :quadrature)) : "tts"
+    (length(q) == 3 && all(c -> haskey(QUAD_CODES, c), q)) ||
+        error("grid quadrature must be 3 letters of t/s/b (alpha, Rc, v), got $q")
+    q == "tts" && return (Int32(0), Int32(0), Int32(0))
+    return (QUAD_CODES[q[1]], QUAD_CODES[q[2]], QUAD_CODES[q[3]])
+end
+
 function kls_config(config, model)
     g = config.grid
+    qa, qr, qv = quad_codes(g)
     KlsConfig(config.physics.m, config.physics.G, config.model.L0, config.model.n_zang,
               Float64(config.model.q1), g.NR, g.Ne, g.Rc_min, g.Rc_max, g.v_min, g.N_alpha,
-              g.alpha_max, g.l_min, g.l_max, g.nw, g.nwa, 0, 0, 0)
+              g.alpha_max, g.l_min, g.l_max, g.nw, g.nwa, qa, qr, qv)
 end
 
 "precompute_all (BasisFunctions.jl:73): grids, orbits, W_l, N_m on the GPU."

@@ -59,3 +59,10 @@ def test_julia_ccalls_name_declared_symbols():
     used = set(re.findall(r"ccall\(\(:(kls_\w+), LIBKLS\)", JULIA))
     declared = set(re.findall(r"\b(kls_\w+)\(", HEADER))
     assert used and used <= declared, used - declared
+
+
+def test_julia_passes_the_grid_quadrature():
+    codes = dict(re.findall(r"'(\w)' => Int32\((\d)\)", JULIA))
+    hdr = {k: v for k, v in re.findall(r"#define KLS_QUAD_(\w+)\s+(\d)", HEADER)}
+    assert codes == {"t": hdr["TRAPEZOID"], "s": hdr["SIMPSON"], "b": hdr["BOOLE"]}
+    assert "g.nw, g.nwa, qa, qr, qv)" in JULIA
