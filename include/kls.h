@@ -167,7 +167,8 @@ int kls_export_W(kls_ctx* ctx, int il0, int nl, double* W_ri);
 /* ---- hot path ----------------------------------------------------------- */
 /* compute_determinant for n omegas (interleaved re,im), one batched launch
  * sequence; det_ri interleaved re,im; log_abs = log|det| (may be NULL).
- * Host buffers in, host buffers out (MatrixBuilder.jl:197-239).            */
+ * Host buffers in, host buffers out (MatrixBuilder.jl:197-239).  A NaN
+ * determinant (a non-finite table row or weight) returns KLS_ERR_NONFINITE. */
 int kls_det_batch(kls_ctx* ctx, const double* omega_ri, int n, int mode,
                   double* det_ri, double* log_abs);
 /* Same with device buffers on the context's stream; no host synchronisation.*/
@@ -352,11 +353,18 @@ int kls_set_mixed_form(kls_ctx* ctx, int form);
  * fixed 2 s).  A wait that runs out makes the call return KLS_ERR_TIMEOUT
  * instead of hanging the GPU; the context stays usable.                     */
 int kls_set_wait_limit(kls_ctx* ctx, double seconds);
-/* Test hook for that path: mode 1 makes the next KLS_MIXED_TMEM contraction
- * skip one producer warp's "operand ready" arrival in its first CTA pair, so
- * the MMA warp's bounded wait runs out and the call returns KLS_ERR_TIMEOUT
- * (no trap, no fault, no unbounded wait); the mode clears itself after that
- * launch.  mode 0 clears it.                                               */
+/* Test hooks for the failure paths (no trap, no fault, no unbounded wait):
+ * KLS_FAULT_SKIP_ARRIVAL makes the next KLS_MIXED_TMEM contraction skip one
+ * producer warp's "operand ready" arrival in its first CTA pair, so the MMA
+ * warp's bounded wait runs out and the call returns KLS_ERR_TIMEOUT; it
+ * clears itself after that launch.  KLS_FAULT_NAN_ROW writes NaN into the
+ * device weight numerator G_k = DJ F0l of the first table row, so every
+ * determinant is NaN and host-buffer calls (kls_det_batch, kls_scan,
+ * kls_newton, ...) return KLS_ERR_NONFINITE.  KLS_FAULT_NONE clears both and
+ * restores the row.                                                        */
+#define KLS_FAULT_NONE          0
+#define KLS_FAULT_SKIP_ARRIVAL  1
+#define KLS_FAULT_NAN_ROW       2
 int kls_set_fault_injection(kls_ctx* ctx, int mode);
 
 /* ---- instrumentation ----------------------------------------------------- */

@@ -35,6 +35,10 @@ KLS_MIXED_ONE_CTA = 1
 KLS_MIXED_PAIR = 2
 KLS_MIXED_TMEM = 3
 
+KLS_FAULT_NONE = 0
+KLS_FAULT_SKIP_ARRIVAL = 1
+KLS_FAULT_NAN_ROW = 2
+
 KLS_LU_AUTO = 0
 KLS_LU_CTA = 1
 KLS_LU_CLUSTER = 2

@@ -172,6 +172,14 @@ int det_batch_host(kls_ctx* c, const double* omega_ri, int n, int mode, double* 
     KLS_CK(c, cudaStreamSynchronize(c->stream));
     if (mode == KLS_MODE_MIXED && (r = kls_mixed_check(c))) return r;
     if ((r = collect_timing(c))) return r;
+    for (int i = 0; i < nb; ++i)
+      if (std::isnan(det_ri[2 * (b + i)]) || std::isnan(det_ri[2 * (b + i) + 1])) {
+        char buf[200];
+        snprintf(buf, sizeof buf,
+                 "NaN determinant at omega = %.17g%+.17gi (a non-finite table row, weight "
+                 "or model value)", omega_ri[2 * (b + i)], omega_ri[2 * (b + i) + 1]);
+        return kls_fail(c, KLS_ERR_NONFINITE, buf);
+      }
   }
   return KLS_OK;
 }
@@ -901,7 +909,25 @@ int kls_set_wait_limit(kls_ctx* c, double seconds) {
 int kls_set_fault_injection(kls_ctx* c, int mode) {
   int r = check_ready(c);
   if (r) return r;
-  if (mode != 0 && mode != 1) return kls_fail(c, KLS_ERR_CONFIG, "fault injection mode is 0 or 1");
+  if (mode < KLS_FAULT_NONE || mode > KLS_FAULT_NAN_ROW)
+    return kls_fail(c, KLS_ERR_CONFIG, "unknown fault injection mode");
+  KLS_CK(c, cudaStreamSynchronize(c->stream));
+  if (mode == KLS_FAULT_NAN_ROW) {
+    if (!c->gk0_poisoned) {
+      KLS_CK(c, cudaMemcpy(&c->gk0_saved, c->d_Gk, sizeof(double), cudaMemcpyDeviceToHost));
+      const double nan = NAN;
+      KLS_CK(c, cudaMemcpy(c->d_Gk, &nan, sizeof(double), cudaMemcpyHostToDevice));
+      c->gk0_poisoned = true;
+    }
+    return KLS_OK;
+  }
+  if (mode == KLS_FAULT_NONE) {
+    if (c->gk0_poisoned) {
+      KLS_CK(c, cudaMemcpy(c->d_Gk, &c->gk0_saved, sizeof(double), cudaMemcpyHostToDevice));
+      c->gk0_poisoned = false;
+    }
+    return c->mixed ? kls_mixed_set_wait(c, 0, KLS_FAULT_NONE) : KLS_OK;
+  }
   if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
   return kls_mixed_set_wait(c, 0, mode);
 }

@@ -105,6 +105,10 @@ struct kls_ctx {
 
   kls_mixed* mixed = nullptr;
 
+  // test hook of the non-finite path: G_k[0] overwritten with NaN, original kept
+  bool gk0_poisoned = false;
+  double gk0_saved = 0.0;
+
   // determinant stage: KLS_LU_* form and the cluster size it uses (-1: not
   // chosen yet, 0: the cluster form does not fit)
   int lu_mode = 0;

@@ -95,7 +95,7 @@ def test_tmem_timeout_returns_error_and_context_recovers(lib_path):
     p.ctx.call("kls_set_mixed_form", _lib.KLS_MIXED_TMEM)
     good = K.compute_determinant_batched(OMEGAS[:3], p, dev)
     p.ctx.call("kls_set_wait_limit", 0.05)
-    p.ctx.call("kls_set_fault_injection", 1)
+    p.ctx.call("kls_set_fault_injection", _lib.KLS_FAULT_SKIP_ARRIVAL)
     with pytest.raises(K.KlsError) as e:
         K.compute_determinant_batched(OMEGAS[:3], p, dev)
     assert e.value.code == _lib.KLS_ERR_TIMEOUT, str(e.value)
@@ -108,7 +108,7 @@ def test_tmem_timeout_returns_error_and_context_recovers(lib_path):
 def test_wait_limit_and_injection_reject_bad_arguments(lib_path):
     p = K.precompute_all(kconfig(**BASE, N_alpha=41))
     for fn, arg in [("kls_set_wait_limit", 0.0), ("kls_set_wait_limit", 100.0),
-                    ("kls_set_fault_injection", 2)]:
+                    ("kls_set_fault_injection", 3)]:
         with pytest.raises(K.KlsError) as e:
             p.ctx.call(fn, arg)
         assert e.value.code == _lib.KLS_ERR_CONFIG
