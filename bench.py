@@ -857,6 +857,21 @@ def ours(args):
                                         _lib.KLS_MODE_MIXED, _lib.dptr(dmx.view(np.float64)),
                                         C.cast(None, C.POINTER(C.c_double))))
         rel = np.abs(dmx - d64) / np.abs(d64)
+        # accumulation chunk of the TMEM-operand form: time and accuracy
+        chunk_sweep = []
+        if tunes["mixed"].form == _lib.KLS_MIXED_TMEM:
+            for ch in (32, 64, 128, 256):
+                _lib.check(h, lib.kls_set_mixed_chunk(h, ch))
+                ms_c, _, _ = time_device(_lib.KLS_MODE_MIXED)
+                dc = np.empty_like(d64[:40])
+                _lib.check(h, lib.kls_det_batch(h, _lib.dptr(om[:40].view(np.float64)), 40,
+                                                _lib.KLS_MODE_MIXED, _lib.dptr(dc.view(np.float64)),
+                                                C.cast(None, C.POINTER(C.c_double))))
+                rc = np.abs(dc - d64[:40]) / np.abs(d64[:40])
+                chunk_sweep.append({"k_blocks": ch, "ms_per_step": ms_c / args.steps,
+                                    "rel_det_err_median": float(np.median(rc)),
+                                    "rel_det_err_max": float(rc.max())})
+            _lib.check(h, lib.kls_set_mixed_chunk(h, 128))
         mixed = {"det_evals_per_s": world * nb * args.steps / (ms_mx * 1e-3),
                  "ms_per_step": ms_mx / args.steps, "gpu_launches": int(launches_mx),
                  "split_table_s": t_split,
@@ -868,6 +883,7 @@ def ours(args):
                               "traffic_scaled": read_traffic(mixed_kernel)[1],
                               "stage_ms": {"weights": stage_mx[0], "contract": stage_mx[1],
                                            "reduce": stage_mx[2], "lu": stage_mx[3]}},
+                 "chunk_sweep": chunk_sweep,
                  "rel_det_err_vs_fp64": {"points": int(len(om)), "seed": 0,
                                          "median": float(np.median(rel)),
                                          "p90": float(np.quantile(rel, 0.9)),

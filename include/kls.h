@@ -347,6 +347,13 @@ int kls_set_lu_mode(kls_ctx* ctx, int mode);
 #define KLS_MIXED_TMEM       3
 int kls_set_mixed_form(kls_ctx* ctx, int form);
 
+/* Accumulation chunk of the KLS_MIXED_TMEM form (no reference counterpart):
+ * the FP32 tensor-memory accumulator is flushed into FP64 every k_blocks
+ * blocks of 32 complex k (default 128, i.e. 4096 terms per FP32 chain).
+ * Shorter chunks bound the FP32 accumulation error more tightly; each flush
+ * pauses the MMA while the accumulator is drained.                          */
+int kls_set_mixed_chunk(kls_ctx* ctx, int k_blocks);
+
 /* ---- failure handling of the device pipeline (no reference counterpart) --- *
  * Every wait of the KLS_MIXED_TMEM contraction (on a copy, an MMA or another
  * warp) is bounded by this limit (default 2 s; the older mixed forms keep a

@@ -155,6 +155,7 @@ SIGNATURES = {
     "kls_set_splits": (C.c_int, [_P, C.c_int, C.c_int]),
     "kls_set_lu_mode": (C.c_int, [_P, C.c_int]),
     "kls_set_mixed_form": (C.c_int, [_P, C.c_int]),
+    "kls_set_mixed_chunk": (C.c_int, [_P, C.c_int]),
     "kls_set_wait_limit": (C.c_int, [_P, C.c_double]),
     "kls_set_fault_injection": (C.c_int, [_P, C.c_int]),
     "kls_enable_timing": (C.c_int, [_P, C.c_int]),

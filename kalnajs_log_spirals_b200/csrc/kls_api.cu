@@ -897,6 +897,15 @@ int kls_set_mixed_form(kls_ctx* c, int form) {
   return kls_mixed_set_form(c, form);
 }
 
+int kls_set_mixed_chunk(kls_ctx* c, int k_blocks) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (k_blocks < 1 || k_blocks > 1 << 20)
+    return kls_fail(c, KLS_ERR_CONFIG, "chunk must be in [1, 2^20] k-blocks");
+  if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
+  return kls_mixed_set_chunk(c, k_blocks);
+}
+
 int kls_set_wait_limit(kls_ctx* c, double seconds) {
   int r = check_ready(c);
   if (r) return r;

@@ -201,6 +201,8 @@ int kls_tm_create(kls_ctx* c, const void* Xh, const void* Xl, kls_mixed_tm** out
 void kls_tm_destroy(kls_mixed_tm* t);
 int kls_tm_splits(const kls_mixed_tm* t);
 void kls_tm_set_splits(const kls_ctx* c, kls_mixed_tm* t, int s);
+void kls_tm_set_chunk(kls_mixed_tm* t, int stages);
+int kls_mixed_set_chunk(kls_ctx* c, int stages);
 int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned long long wait_ns,
                     int fault_skip);
 int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M);

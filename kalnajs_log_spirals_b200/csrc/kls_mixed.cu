@@ -1366,6 +1366,13 @@ int kls_mixed_set_form(kls_ctx* c, int form) {
   return KLS_OK;
 }
 
+int kls_mixed_set_chunk(kls_ctx* c, int stages) {
+  if (!c->mixed) return KLS_ERR_STATE;
+  if (!c->mixed->tm) return kls_fail(c, KLS_ERR_UNSUPPORTED, "KLS_MIXED_TMEM needs N_alpha_pad <= 384");
+  kls_tm_set_chunk(c->mixed->tm, stages);
+  return KLS_OK;
+}
+
 int kls_mixed_set_wait(kls_ctx* c, unsigned long long ns, int fault_mode) {
   if (!c->mixed) return KLS_ERR_STATE;
   if (ns) c->mixed->wait_ns = ns;

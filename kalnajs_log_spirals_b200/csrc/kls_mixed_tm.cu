@@ -21,8 +21,8 @@
 // of it (64-byte swizzled TMA tiles of the split table Xh / Xl, Re rows a and
 // Im rows Npad + a), so each SM reads Npad / 2 table rows per stage.  The
 // accumulator (128 lanes x Npad FP32 columns per CTA) holds every output row
-// b and is flushed every TM_CHUNK stages into an FP64 partial per (tile, K
-// split) in deterministic order; the split sum, G N(a) scaling, I - M, the
+// b and is flushed every `chunk` stages (default TM_CHUNK) into an FP64
+// partial per (tile, K split) in deterministic order; the split sum, G N(a) scaling, I - M, the
 // weights and the LU are FP64.  Products hi*hi + lo*hi + hi*lo (the lo*lo
 // term, ~2^-18 relative, is dropped).
 //
@@ -52,7 +52,7 @@ constexpr int TM_KB = 32;              // complex k per stage
 constexpr int TM_STAGES = 3;           // shared-memory stages (B halves + A sources)
 constexpr int TM_ASTAGES = 2;          // TMEM stages of A
 constexpr int TM_WSTAGES = 8;          // weights ring
-constexpr int TM_CHUNK = 128;          // stages per FP32 accumulation chunk (4096 complex k)
+constexpr int TM_CHUNK = 128;          // default stages per FP32 accumulation chunk (4096 k)
 constexpr int TM_THREADS = 640;
 constexpr int TM_NPROD = 8;            // producer warps 4..11
 constexpr int TM_NDRAIN = 8;           // drain warps 12..19
@@ -77,6 +77,7 @@ struct TmParams {
   int64_t K_pad;
   unsigned long long wait_ns;
   int fault_skip;           // test hook: one producer arrival is skipped
+  int chunk;                // stages per FP32 accumulation chunk
 };
 
 // output row b of the table for accumulator column j (the pair splits each
@@ -113,7 +114,8 @@ mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant_
   const int split = blockIdx.y;
   const int kb0 = split * P.kb_per_split;
   const int nkb = max(0, min(P.nkb_total, kb0 + P.kb_per_split) - kb0);
-  const int nch = (nkb + TM_CHUNK - 1) / TM_CHUNK;
+  const int CH = P.chunk;
+  const int nch = (nkb + CH - 1) / CH;
   const int Nh2 = P.Npad / 2;                // table rows per CTA
   const int nmma = P.Npad > 256 ? 2 : 1;     // MMAs along N
   const int Nh = P.Npad / nmma;              // N of each MMA
@@ -220,9 +222,9 @@ mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant_
       const uint32_t idesc = idesc_bf16(256, Nh);
       for (int i = 0; i < nkb; ++i) {
         const int s = i % TM_STAGES, as = i % TM_ASTAGES;
-        const int ci = i % TM_CHUNK, ch = i / TM_CHUNK;
+        const int ci = i % CH, ch = i / CH;
         const bool first = ci == 0;
-        const bool last = ci == TM_CHUNK - 1 || i == nkb - 1;
+        const bool last = ci == CH - 1 || i == nkb - 1;
         if (first && ch > 0 &&
             !mbar_wait_cl_lim(smem_u32(&bar_acc_empty), (ch - 1) & 1, &s_abort, err, 7, lim))
           break;
@@ -404,6 +406,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 struct kls_mixed_tm {
   CUtensorMap tb_h, tb_l, ty_h, ty_l;
   int splits = 1;
+  int chunk = TM_CHUNK;         // stages per FP32 accumulation chunk
   double* part = nullptr;       // [n tiles][splits][Npad][128]
   size_t part_elems = 0;
   float2* wt32 = nullptr;       // [n][K_pad]
@@ -477,6 +480,8 @@ void kls_tm_set_splits(const kls_ctx* c, kls_mixed_tm* t, int s) {
   t->splits = std::max(1, std::min(s, (int)(c->K_pad / TM_KB)));
 }
 
+void kls_tm_set_chunk(kls_mixed_tm* t, int stages) { t->chunk = std::max(1, stages); }
+
 int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned long long wait_ns,
                     int fault_skip) {
   const int tiles_a = c->Na_pad / TM_AB;
@@ -513,6 +518,7 @@ int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned lon
   P.K_pad = c->K_pad;
   P.wait_ns = wait_ns;
   P.fault_skip = fault_skip;
+  P.chunk = t->chunk;
   const int pairs = (n_tiles + 1) / 2;
   dim3 grid((unsigned)(2 * pairs), (unsigned)splits);
   mixed_tm_kernel<<<grid, TM_THREADS, tm_smem(c->Na_pad), c->stream>>>(
