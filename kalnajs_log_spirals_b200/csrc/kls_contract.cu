@@ -18,6 +18,7 @@
 //   reduce_kernel  : deterministic sum over splits, * G * N(a), I - M
 #include "kls_internal.cuh"
 #include <algorithm>
+#include <cmath>
 
 namespace {
 
@@ -298,9 +299,11 @@ __global__ void multi_reduce_kernel(const kls_mdesc* __restrict__ md,
 
 // The split count depends on the table and the device only, never on the
 // batch size, so a determinant is bitwise identical whichever batch it is
-// evaluated in.  It is chosen so that tiles * splits fills just under a
-// whole number q of waves (q the smallest giving >= 16 splits): then n
-// omegas take n * q rounds with every round nearly full.
+// evaluated in.  It is chosen so that tiles * splits fills a whole number q
+// of waves as closely as possible (q in 1..8, at least 16 splits where the
+// table allows, at least 8 slabs per split): then n omegas take n * q nearly
+// full waves for every n.  At N_alpha_pad = 320 (25 tiles) on 296 slots
+// that is 71 splits: 1775 CTAs per omega = 99.9% of 6 waves.
 int kls_choose_splits(const kls_ctx* c) {
   const int tiles = (c->Na_pad / KLS_TILE) * (c->Na_pad / KLS_TILE);
   int sms = 148, per_sm = 2;
@@ -310,13 +313,23 @@ int kls_choose_splits(const kls_ctx* c) {
                                                     CT_SMEM) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   const int slots = sms * per_sm;
-  int q = std::max(1, (16 * tiles + slots - 1) / slots);
-  int s = (q * slots) / tiles;
   int64_t max_s = c->K_pad / (CT_BK * 8);            // at least 8 slabs per split
-  if (s > max_s) s = (int)max_s;
-  if (s < 1) s = 1;
-  if (s > 256) s = 256;
-  return s;
+  if (max_s > 512) max_s = 512;
+  if (max_s < 1) max_s = 1;
+  int best = (int)std::min<int64_t>(max_s, std::max(1, slots / std::max(1, tiles)));
+  double best_fill = -1.0;
+  for (int q = 1; q <= 8; ++q) {
+    const int s = (int)std::min<int64_t>(max_s, (int64_t)q * slots / tiles);
+    if (s < 1) continue;
+    if (s < 16 && (int64_t)(q + 1) * slots / tiles <= max_s) continue;   // prefer >= 16 splits
+    const double work = (double)tiles * s;
+    const double fill = work / (std::ceil(work / slots) * slots);
+    if (fill > best_fill + 1e-3) {
+      best_fill = fill;
+      best = s;
+    }
+  }
+  return best;
 }
 
 int kls_run_weights(kls_ctx* c, int n) {

@@ -418,15 +418,27 @@ bool kls_tm_supported(const kls_ctx* c) {
 }
 
 // K splits of the form: fixed per context (determinants do not depend on the
-// batch), chosen so that a Newton triple's tile pairs fill whole waves of
-// CTA pairs twice over
+// batch).  With as many splits as CTA pairs can be resident at once, every
+// batch fills whole waves: (tile pairs of the batch) x splits is a multiple
+// of the resident pairs for any number of omegas.
 int kls_tm_default_splits(const kls_ctx* c) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-  const int tiles_a = c->Na_pad / TM_AB;
-  const int pairs3 = (3 * tiles_a + 1) / 2;
+  int pairs = sms / 2;
+  cudaFuncSetAttribute(mixed_tm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)tm_smem(c->Na_pad));
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(2 * pairs, 1, 1);
+  lc.blockDim = dim3(TM_THREADS, 1, 1);
+  lc.dynamicSmemBytes = tm_smem(c->Na_pad);
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, (void*)mixed_tm_kernel, &lc) == cudaSuccess &&
+      clusters > 0)
+    pairs = clusters;
+  else
+    cudaGetLastError();
   const int nkb = (int)(c->K_pad / TM_KB);
-  return std::max(1, std::min(nkb, 2 * std::max(1, (sms / 2) / pairs3)));
+  return std::max(1, std::min(nkb, pairs));
 }
 
 int kls_tm_create(kls_ctx* c, const void* Xh, const void* Xl, kls_mixed_tm** out) {
