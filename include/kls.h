@@ -189,18 +189,23 @@ int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cf
 
 /* Mixed-precision Newton with an FP64 finish (no reference counterpart; it
  * returns the point at which the reference's own stopping rule,
- * |det| < nc->tol on the plain FP64 determinant, holds):
- *   phase 1: Newton on split-BF16 determinants, the finite-difference triple
- *            (omega, omega + m*mixed_delta, omega + i*mixed_delta) evaluated
- *            as one batch, until a step is shorter than mixed_step_tol or
- *            |det| has not halved for 3 steps (the split form's noise floor;
- *            its det error is ~5e-5 relative, so mixed_delta ~1e-3 keeps
- *            the finite-difference Jacobian well above that noise);
- *   phase 2: FP64 determinant at the current point; if |det| < tol, one
- *            more chord step when it exceeds 1e-12 (kept if it lowers |det|),
- *            then stop; else a chord step with the last Jacobian; the
- *            Jacobian is recomputed in FP64 (step nc->delta) when |det| falls
- *            by less than 10x per step.                                      */
+ * |det| < nc->tol on the plain FP64 determinant, holds).  det(I - M(omega))
+ * is holomorphic in omega = m Omega_p + i gamma, so one complex slope S gives
+ * the reference's whole 2x2 finite-difference Jacobian (dF/dOmega_p = m S,
+ * dF/dgamma = i S) and the step is delta omega = -det / S:
+ *   phase 1: Newton on split-BF16 determinants, S by central difference of
+ *            the triple (omega - h, omega, omega + h), h = m*mixed_delta,
+ *            evaluated as one batch, until a step is shorter than
+ *            mixed_step_tol or |det| has not halved for 3 steps (the split
+ *            form's noise floor; mixed_delta ~1e-3 keeps the difference well
+ *            above its ~5e-5 relative det error);
+ *   phase 2: FP64 determinants, one per step: a chord step with the last
+ *            split-BF16 slope, then secant slopes from the FP64 values; when
+ *            a step does not lower |det| the slope is recomputed as an FP64
+ *            forward difference (step nc->delta).  Once |det| < tol, one more
+ *            step is taken (and kept if it lowers |det|) when the predicted
+ *            correction exceeds 1e-11, since |det| < tol fixes the root only
+ *            to tol / |det'|.                                               */
 typedef struct kls_hybrid_cfg {
     double  mixed_delta;
     double  mixed_step_tol;

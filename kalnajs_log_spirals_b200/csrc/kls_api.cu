@@ -9,6 +9,7 @@
 #include "kls_internal.cuh"
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -589,34 +590,50 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
   if (r) return r;
   if (!nc || !hc || !res || hc->mixed_max_iter < 0 || hc->fp64_max_iter < 1)
     return kls_fail(c, KLS_ERR_CONFIG, "bad hybrid Newton arguments");
+  using cplx = std::complex<double>;
   const double m = (double)c->cfg.m, tol = nc->tol;
-  double Op = Op_init, g = g_init;
+  // omega = m Omega_p + i gamma, with the reference's clamps on (Omega_p, gamma)
+  auto clamp = [&](cplx w) {
+    const double Op = std::min(std::max(w.real() / m, 0.0), 1.0);
+    return cplx(m * Op, std::max(w.imag(), 1e-4));
+  };
+  cplx w = clamp(cplx(m * Op_init, g_init));
   int n_mixed = 0, n_fp64 = 0, it_total = 0;
   std::memset(res, 0, sizeof *res);
-  auto clamp = [&]() {
-    g = std::max(g, 1e-4);
-    Op = std::min(std::max(Op, 0.0), 1.0);
-  };
-  auto hist = [&](double a) {
+  auto hist = [&](cplx at, double a) {
     if (history && it_total < nc->max_iter) {
-      history[3 * it_total] = Op;
-      history[3 * it_total + 1] = g;
+      history[3 * it_total] = at.real() / m;
+      history[3 * it_total + 1] = at.imag();
       history[3 * it_total + 2] = a;
     }
     ++it_total;
   };
-  // ---- phase 1: split-BF16 Newton, FD triple in one batch
-  double J[2][2] = {{0, 0}, {0, 0}};
-  bool haveJ = false;
-  const double dm = hc->mixed_delta;
+  auto det = [&](const cplx* ws, int n, int mode, cplx* out) -> int {
+    double in[6], o[6];
+    for (int i = 0; i < n; ++i) { in[2 * i] = ws[i].real(); in[2 * i + 1] = ws[i].imag(); }
+    int q = det_batch_host(c, in, n, mode, o, nullptr);
+    if (q) return q;
+    for (int i = 0; i < n; ++i) out[i] = cplx(o[2 * i], o[2 * i + 1]);
+    (mode == KLS_MODE_MIXED ? n_mixed : n_fp64) += n;
+    return KLS_OK;
+  };
+  // det(I - M(omega)) is holomorphic in omega, so one complex slope S =
+  // d det / d omega gives the whole 2x2 finite-difference Jacobian of the
+  // reference (dF/dOmega_p = m S, dF/dgamma = i S) and the Newton step is
+  // delta omega = -det / S.
+  // ---- phase 1: split-BF16 Newton, slope by central difference of the
+  //      triple (omega - h, omega, omega + h) evaluated as one batch
+  const double h = m * hc->mixed_delta;
+  cplx S(0.0, 0.0);
+  bool haveS = false;
   double best = INFINITY;
   int stall = 0;
   for (int it = 0; it < hc->mixed_max_iter; ++it) {
-    double w[6] = {m * Op, g, m * (Op + dm), g, m * Op, g + dm}, d[6];
-    if ((r = det_batch_host(c, w, 3, KLS_MODE_MIXED, d, nullptr))) return r;
-    n_mixed += 3;
-    const double a = std::hypot(d[0], d[1]);
-    hist(a);
+    const cplx ws[3] = {w - h, w, w + h};
+    cplx d[3];
+    if ((r = det(ws, 3, KLS_MODE_MIXED, d))) return r;
+    const double a = std::abs(d[1]);
+    hist(w, a);
     // |det| no longer halving for 3 steps: the split form's noise floor
     if (a < 0.5 * best) {
       best = a;
@@ -624,76 +641,66 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
     } else if (++stall >= 3) {
       break;
     }
-    J[0][0] = (d[2] - d[0]) / dm; J[0][1] = (d[4] - d[0]) / dm;
-    J[1][0] = (d[3] - d[1]) / dm; J[1][1] = (d[5] - d[1]) / dm;
-    haveJ = true;
-    double F[2] = {d[0], d[1]}, x[2];
-    if (!solve2(J, F, x)) break;
-    Op -= x[0];
-    g -= x[1];
-    clamp();
-    if (std::hypot(x[0], x[1]) < hc->mixed_step_tol) break;
+    const cplx Sn = (d[2] - d[0]) / (2.0 * h);
+    if (!(std::abs(Sn) > 0.0) || !std::isfinite(std::abs(Sn))) break;
+    S = Sn;
+    haveS = true;
+    const cplx wn = clamp(w - d[1] / S);
+    const double step = std::abs(wn - w);
+    w = wn;
+    if (step < hc->mixed_step_tol) break;
   }
-  // ---- phase 2: FP64 determinant, chord steps with the last Jacobian
+  // ---- phase 2: FP64 determinants, one per step: a chord step with the
+  //      split form's slope, then secant slopes from the FP64 values; an FP64
+  //      forward-difference slope (step nc->delta) when a step does not lower
+  //      |det|
   bool converged = false;
-  double dl[2] = {NAN, NAN}, prev = INFINITY;
-  for (int it = 0; it < hc->fp64_max_iter; ++it) {
-    double w[2] = {m * Op, g};
-    if ((r = det_batch_host(c, w, 1, KLS_MODE_FP64, dl, nullptr))) return r;
-    ++n_fp64;
-    const double a = std::hypot(dl[0], dl[1]);
-    hist(a);
-    if (a < tol) {
-      converged = true;
-      // |det| < tol fixes the root only to tol / |det'|: quadratically
-      // converging FP64 Newton lands far below tol, a chord iteration just
-      // below it.  One more chord step when it is not negligible (> 1e-12),
-      // kept if it lowers |det|.
-      double F[2] = {dl[0], dl[1]}, x[2];
-      if (haveJ && solve2(J, F, x) && std::hypot(x[0], x[1]) > 1e-12) {
-        const double Op2 = std::min(std::max(Op - x[0], 0.0), 1.0);
-        const double g2 = std::max(g - x[1], 1e-4);
-        double w2[2] = {m * Op2, g2}, d2[2];
-        if ((r = det_batch_host(c, w2, 1, KLS_MODE_FP64, d2, nullptr))) return r;
-        ++n_fp64;
-        if (std::hypot(d2[0], d2[1]) < a) {
-          Op = Op2;
-          g = g2;
-          dl[0] = d2[0];
-          dl[1] = d2[1];
-        }
-      }
-      break;
+  cplx dw;
+  if ((r = det(&w, 1, KLS_MODE_FP64, &dw))) return r;
+  hist(w, std::abs(dw));
+  for (int it = 0; it < hc->fp64_max_iter && !(std::abs(dw) < tol); ++it) {
+    if (!haveS) {
+      const cplx wd = w + m * nc->delta;
+      cplx dd;
+      if ((r = det(&wd, 1, KLS_MODE_FP64, &dd))) return r;
+      S = (dd - dw) / (m * nc->delta);
+      haveS = true;
     }
-    if (!haveJ || a > 0.1 * prev) {
-      // Jacobian in FP64 (NewtonSolver.jl:98-109), FD pair in one batch
-      double w2[4] = {m * (Op + nc->delta), g, m * Op, g + nc->delta}, d2[4];
-      if ((r = det_batch_host(c, w2, 2, KLS_MODE_FP64, d2, nullptr))) return r;
-      n_fp64 += 2;
-      J[0][0] = (d2[0] - dl[0]) / nc->delta; J[0][1] = (d2[2] - dl[0]) / nc->delta;
-      J[1][0] = (d2[1] - dl[1]) / nc->delta; J[1][1] = (d2[3] - dl[1]) / nc->delta;
-      haveJ = true;
-    }
-    prev = a;
-    double F[2] = {dl[0], dl[1]}, x[2];
-    if (!solve2(J, F, x)) {
-      res->Omega_p = Op; res->gamma = g; res->iterations = it_total;
+    if (!(std::abs(S) > 0.0)) {
+      res->Omega_p = w.real() / m; res->gamma = w.imag(); res->iterations = it_total;
       res->det_evals = n_mixed + n_fp64;
       return kls_fail(c, KLS_ERR_SINGULAR, "singular Jacobian in the FP64 phase");
     }
-    Op -= x[0];
-    g -= x[1];
-    clamp();
+    const cplx wn = clamp(w - dw / S);
+    cplx dn;
+    if ((r = det(&wn, 1, KLS_MODE_FP64, &dn))) return r;
+    hist(wn, std::abs(dn));
+    if (std::abs(dn) < std::abs(dw)) {
+      if (wn != w) S = (dn - dw) / (wn - w);      // secant slope
+      w = wn;
+      dw = dn;
+    } else {
+      haveS = false;                              // FP64 slope at w next
+    }
   }
-  res->Omega_p = Op; res->gamma = g; res->omega_re = m * Op; res->omega_im = g;
-  if (converged) {
-    res->det_re = dl[0]; res->det_im = dl[1];
-  } else {
-    double w[2] = {m * Op, g};
-    if ((r = det_batch_host(c, w, 1, KLS_MODE_FP64, dl, nullptr))) return r;
-    ++n_fp64;
-    res->det_re = dl[0]; res->det_im = dl[1];
+  if (std::abs(dw) < tol) {
+    converged = true;
+    // |det| < tol fixes the root only to tol / |det'|; a secant iteration
+    // stops just below tol.  One more step when the predicted correction is
+    // not negligible (> 1e-11), kept if it lowers |det|.
+    if (haveS && std::abs(S) > 0.0 && std::abs(dw / S) > 1e-11) {
+      const cplx wn = clamp(w - dw / S);
+      cplx dn;
+      if ((r = det(&wn, 1, KLS_MODE_FP64, &dn))) return r;
+      if (std::abs(dn) < std::abs(dw)) {
+        w = wn;
+        dw = dn;
+      }
+    }
   }
+  res->Omega_p = w.real() / m; res->gamma = w.imag();
+  res->omega_re = w.real(); res->omega_im = w.imag();
+  res->det_re = dw.real(); res->det_im = dw.imag();
   res->iterations = it_total;
   res->converged = converged ? 1 : 0;
   res->det_evals = n_mixed + n_fp64;
