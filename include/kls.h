@@ -262,8 +262,9 @@ int kls_mlp_train(kls_mlp* mlp, const float* X, const float* T, int n, int epoch
  * result download) is one CUDA graph replay.  Each model keeps its
  * context's K split count (tune with kls_autotune before creating the
  * batch), so every determinant is bitwise what kls_det_batch returns for
- * that context (split-BF16: in the KLS_MIXED_ONE_CTA form, whose kernel body
- * the batch runs; the KLS_MIXED_TMEM form sums in another order).  The contexts must outlive the batch and are not modified;
+ * that context: the batch runs the KLS_MIXED_TMEM kernel body (one CTA pair
+ * per model, tile pair and K split, from per-model descriptors) when that is
+ * every model's split-BF16 form, else the KLS_MIXED_ONE_CTA body.  The contexts must outlive the batch and are not modified;
  * a batch is not re-entrant.  Errors: kls_multi_last_error (NULL handle:
  * errors of kls_multi_create).                                              */
 typedef struct kls_multi kls_multi;
@@ -276,7 +277,7 @@ typedef struct kls_multi_info {
     int64_t replays;              /* passes so far                            */
     double  last_ms;              /* device time of the last pass (ms)        */
     int32_t schedule;             /* mixed form: 0 persistent round robin,
-                                     1 one CTA per item (the faster of the two
+                                     1 one CTA (pair) per item (the faster of the two
                                      passes timed at creation)                */
     double  schedule_ms[2];       /* those two passes (ms)                    */
 } kls_multi_info;

@@ -1,5 +1,6 @@
 // Internal declarations shared by the libkls.so translation units.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -48,6 +49,18 @@ struct kls_mdesc {
   void* wt32;                 // [batch][K_pad] float2, permuted per 64-block
   double* mpart;              // [batch][msplits][2 Na_pad][2 Na_pad] column-major planes
   int msplits, kb_per_split, nkb_total, om_per_item;
+};
+
+// One model of an uneven batch in the TMEM-operand split-BF16 form (device
+// descriptor): the model context's tensor maps and split parameters and the
+// batch's buffers.
+struct alignas(64) kls_tm_model {
+  CUtensorMap tb_h, tb_l, ty_h, ty_l;
+  const float2* wt32;          // [batch][K_pad] FP32 weights
+  double* part;                // [batch * tiles_a][splits][Npad][128] FP64 partials
+  int64_t K_pad;
+  unsigned long long wait_ns;
+  int Npad, tiles_a, n_tiles, splits, kb_per_split, nkb_total, chunk, pad;
 };
 
 // One work item of the persistent contraction: FP64 form (model, omega z,
@@ -206,3 +219,10 @@ int kls_mixed_set_chunk(kls_ctx* c, int stages);
 int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned long long wait_ns,
                     int fault_skip);
 int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M);
+// the context's TMEM-operand state when that is its split-BF16 form (else null)
+kls_mixed_tm* kls_mixed_tm_state(const kls_ctx* c, unsigned long long* wait_ns);
+void kls_tm_describe(const kls_ctx* c, const kls_mixed_tm* t, unsigned long long wait_ns,
+                     int batch, kls_tm_model* out);
+int kls_tm_multi_launch(cudaStream_t st, const kls_mdesc* d_md, const kls_tm_model* d_tm,
+                        const int2* d_pairs, int n_pairs, const int4* d_items, int n_items,
+                        int64_t max_K_pad, int max_Npad, int* d_err);

@@ -1353,6 +1353,12 @@ int kls_mixed_splits_of(const kls_ctx* c) {
 
 int kls_mixed_legacy_splits(const kls_ctx* c) { return c->mixed ? c->mixed->splits : 0; }
 
+kls_mixed_tm* kls_mixed_tm_state(const kls_ctx* c, unsigned long long* wait_ns) {
+  if (!c->mixed || c->mixed->form != KLS_MIXED_TMEM) return nullptr;
+  if (wait_ns) *wait_ns = c->mixed->wait_ns;
+  return c->mixed->tm;
+}
+
 int kls_mixed_default_splits(const kls_ctx* c) {
   if (c->mixed && c->mixed->form == KLS_MIXED_TMEM) return kls_tm_default_splits(c);
   return mixed_splits(c);

@@ -88,11 +88,12 @@ __device__ __forceinline__ int tm_brow(int j, int Nh, int Nh2) {
   return jj < h2 ? nh * h2 + jj : Nh2 + nh * h2 + (jj - h2);
 }
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TM_THREADS, 1)
-mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant__ CUtensorMap tb_l,
-                const __grid_constant__ CUtensorMap ty_h, const __grid_constant__ CUtensorMap ty_l,
-                TmParams P, const float2* __restrict__ wt32, double* __restrict__ part,
-                int* __restrict__ err) {
+// One CTA of a pair: tile `tile_pair` x 2 + its cluster rank, K split `split`.
+__device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMap* tbl,
+                                        const CUtensorMap* tyh, const CUtensorMap* tyl,
+                                        const TmParams& P, int tile_pair, int split,
+                                        const float2* __restrict__ wt32,
+                                        double* __restrict__ part, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_b_full[TM_STAGES], bar_b_empty[TM_STAGES],
       bar_y_full[TM_STAGES], bar_y_empty[TM_STAGES], bar_w_full[TM_WSTAGES],
@@ -106,12 +107,11 @@ mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant_
   uint32_t crank;
   asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(crank));
   const bool leader = crank == 0;
-  const int tile = 2 * (int)(blockIdx.x >> 1) + (int)crank;
+  const int tile = 2 * tile_pair + (int)crank;
   const bool dummy = tile >= P.n_tiles;      // odd tile count: the last peer only loads B
   const int tile_e = dummy ? 0 : tile;
   const int om = tile_e / P.tiles_a;
   const int a0 = (tile_e % P.tiles_a) * TM_AB;
-  const int split = blockIdx.y;
   const int kb0 = split * P.kb_per_split;
   const int nkb = max(0, min(P.nkb_total, kb0 + P.kb_per_split) - kb0);
   const int CH = P.chunk;
@@ -176,16 +176,16 @@ mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant_
         const int kx = (kb0 + i) * TM_KB;
         if (leader) mbar_arrive_tx(smem_u32(&bar_b_full[s]), 2 * 4 * BT);
         const uint32_t fb = mapa_u32(smem_u32(&bar_b_full[s]), 0);
-        tma_load_2d_pair(smem_u32(b_tile(s, 0, 0)), &tb_h, kx, yb, fb);
-        tma_load_2d_pair(smem_u32(b_tile(s, 0, 1)), &tb_h, kx, P.Npad + yb, fb);
-        tma_load_2d_pair(smem_u32(b_tile(s, 1, 0)), &tb_l, kx, yb, fb);
-        tma_load_2d_pair(smem_u32(b_tile(s, 1, 1)), &tb_l, kx, P.Npad + yb, fb);
+        tma_load_2d_pair(smem_u32(b_tile(s, 0, 0)), tbh, kx, yb, fb);
+        tma_load_2d_pair(smem_u32(b_tile(s, 0, 1)), tbh, kx, P.Npad + yb, fb);
+        tma_load_2d_pair(smem_u32(b_tile(s, 1, 0)), tbl, kx, yb, fb);
+        tma_load_2d_pair(smem_u32(b_tile(s, 1, 1)), tbl, kx, P.Npad + yb, fb);
         const uint32_t yf = smem_u32(&bar_y_full[s]);
         mbar_arrive_tx(yf, 4 * TM_YTILE);
-        tma_load_2d(smem_u32(y_tile(s, 0, 0)), &ty_h, kx, a0, yf);
-        tma_load_2d(smem_u32(y_tile(s, 0, 1)), &ty_h, kx, P.Npad + a0, yf);
-        tma_load_2d(smem_u32(y_tile(s, 1, 0)), &ty_l, kx, a0, yf);
-        tma_load_2d(smem_u32(y_tile(s, 1, 1)), &ty_l, kx, P.Npad + a0, yf);
+        tma_load_2d(smem_u32(y_tile(s, 0, 0)), tyh, kx, a0, yf);
+        tma_load_2d(smem_u32(y_tile(s, 0, 1)), tyh, kx, P.Npad + a0, yf);
+        tma_load_2d(smem_u32(y_tile(s, 1, 0)), tyl, kx, a0, yf);
+        tma_load_2d(smem_u32(y_tile(s, 1, 1)), tyl, kx, P.Npad + a0, yf);
         issued = i + 1;
       }
       // the last copies into this CTA's shared memory land before it may exit
@@ -267,7 +267,7 @@ mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant_
     const bool use_re = h == p;
     const float sgn = (h == 1 && p == 0) ? -1.f : 1.f;
     const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16) + TM_ACOL + (uint32_t)(h * 16);
-    const bool skip_one = P.fault_skip && leader && blockIdx.x == 0 && blockIdx.y == 0 && pw == 0;
+    const bool skip_one = P.fault_skip && leader && tile_pair == 0 && split == 0 && pw == 0;
     for (int i = 0; i < nkb; ++i) {
       const int s = i % TM_STAGES, as = i % TM_ASTAGES, ws = i % TM_WSTAGES;
       bool ok = mbar_wait_lim(smem_u32(&bar_y_full[s]), (i / TM_STAGES) & 1, &s_abort, err, 4, lim);
@@ -361,6 +361,79 @@ mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant_
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                  "r"(TM_TMEM_COLS));
+  }
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TM_THREADS, 1)
+mixed_tm_kernel(const __grid_constant__ CUtensorMap tb_h, const __grid_constant__ CUtensorMap tb_l,
+                const __grid_constant__ CUtensorMap ty_h, const __grid_constant__ CUtensorMap ty_l,
+                TmParams P, const float2* __restrict__ wt32, double* __restrict__ part,
+                int* __restrict__ err) {
+  tm_body(&tb_h, &tb_l, &ty_h, &ty_l, P, (int)(blockIdx.x >> 1), (int)blockIdx.y, wt32, part, err);
+}
+
+// Uneven batch: one cluster per work item (model, tile pair, K split); the
+// model's tensor maps and parameters come from device descriptors.  Each
+// item runs exactly the one-model kernel's body, so a determinant is bitwise
+// what the model's own context returns in this form.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TM_THREADS, 1)
+mixed_tm_multi_kernel(const kls_tm_model* __restrict__ md, const int4* __restrict__ items,
+                      int* __restrict__ err) {
+  const int4 it = items[blockIdx.x >> 1];
+  const kls_tm_model& d = md[it.x];
+  tensormap_acquire(&d.tb_h);
+  tensormap_acquire(&d.tb_l);
+  tensormap_acquire(&d.ty_h);
+  tensormap_acquire(&d.ty_l);
+  TmParams P;
+  P.Npad = d.Npad;
+  P.tiles_a = d.tiles_a;
+  P.n_tiles = d.n_tiles;
+  P.splits = d.splits;
+  P.kb_per_split = d.kb_per_split;
+  P.nkb_total = d.nkb_total;
+  P.K_pad = d.K_pad;
+  P.wait_ns = d.wait_ns;
+  P.fault_skip = 0;
+  P.chunk = d.chunk;
+  tm_body(&d.tb_h, &d.tb_l, &d.ty_h, &d.ty_l, P, it.y, it.z, d.wt32, d.part, err);
+}
+
+// uneven batch: FP32 weights of every (model, omega) pair, plain order
+__global__ void tm_multi_weights32_kernel(const kls_mdesc* __restrict__ md,
+                                          const int2* __restrict__ pairs) {
+  const int2 pz = pairs[blockIdx.y];
+  const kls_mdesc& d = md[pz.x];
+  const double2* wt = d.wt + (size_t)pz.y * d.K_pad;
+  float2* w32 = reinterpret_cast<float2*>(d.wt32) + (size_t)pz.y * d.K_pad;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.K_pad;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = wt[i];
+    w32[i] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+// uneven batch: split sum, * G * N(a), I - M per (model, omega) pair; mpart is
+// the model's TMEM-form partial [batch * tiles_a][splits][Npad][128]
+__global__ void tm_multi_reduce_kernel(const kls_mdesc* __restrict__ md,
+                                       const int2* __restrict__ pairs) {
+  const int2 pz = pairs[blockIdx.y];
+  const kls_mdesc& d = md[pz.x];
+  const int Na = d.Na, tiles_a = d.Na_pad / TM_AB;
+  const size_t plane = (size_t)d.Na_pad * 128;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
+    const int b = e / Na, a = e % Na;
+    const int at = a / TM_AB, l2 = 2 * (a % TM_AB);
+    const double* src =
+        d.mpart + (size_t)(pz.y * tiles_a + at) * d.msplits * plane + (size_t)b * 128 + l2;
+    double sr = 0.0, si = 0.0;
+    for (int s = 0; s < d.msplits; ++s) {
+      sr += src[(size_t)s * plane];
+      si += src[(size_t)s * plane + 1];
+    }
+    const double n = d.Nk[a];
+    const double mr = __dmul_rn(__dmul_rn(sr, d.G), n), mi = __dmul_rn(__dmul_rn(si, d.G), n);
+    d.A[(size_t)pz.y * Na * Na + e] = make_double2((a == b ? 1.0 : 0.0) - mr, -mi);
   }
 }
 
@@ -537,6 +610,42 @@ int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned lon
       t->tb_h, t->tb_l, t->ty_h, t->ty_l, P, t->wt32, t->part, d_err);
   KLS_LAUNCHED(c);
   return KLS_OK;
+}
+
+void kls_tm_describe(const kls_ctx* c, const kls_mixed_tm* t, unsigned long long wait_ns,
+                     int batch, kls_tm_model* d) {
+  d->tb_h = t->tb_h;
+  d->tb_l = t->tb_l;
+  d->ty_h = t->ty_h;
+  d->ty_l = t->ty_l;
+  d->Npad = c->Na_pad;
+  d->tiles_a = c->Na_pad / TM_AB;
+  d->n_tiles = batch * d->tiles_a;
+  d->nkb_total = (int)(c->K_pad / TM_KB);
+  d->kb_per_split = (d->nkb_total + t->splits - 1) / t->splits;
+  d->splits = (d->nkb_total + d->kb_per_split - 1) / d->kb_per_split;
+  d->chunk = t->chunk;
+  d->K_pad = c->K_pad;
+  d->wait_ns = wait_ns;
+  d->wt32 = nullptr;
+  d->part = nullptr;
+  d->pad = 0;
+}
+
+int kls_tm_multi_launch(cudaStream_t st, const kls_mdesc* d_md, const kls_tm_model* d_tm,
+                        const int2* d_pairs, int n_pairs, const int4* d_items, int n_items,
+                        int64_t max_K_pad, int max_Npad, int* d_err) {
+  cudaError_t e;
+  const int wblocks = (int)std::min<int64_t>((max_K_pad + 255) / 256, 1024);
+  tm_multi_weights32_kernel<<<dim3(wblocks, n_pairs), 256, 0, st>>>(d_md, d_pairs);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  if ((e = cudaFuncSetAttribute(mixed_tm_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tm_smem(max_Npad))) != cudaSuccess)
+    return (int)e;
+  mixed_tm_multi_kernel<<<2 * n_items, TM_THREADS, tm_smem(max_Npad), st>>>(d_tm, d_items, d_err);
+  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  tm_multi_reduce_kernel<<<dim3(256, n_pairs), 256, 0, st>>>(d_md, d_pairs);
+  return (int)cudaGetLastError();
 }
 
 int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M) {

@@ -16,7 +16,10 @@
 // the mixed one the batch times one pass with each of two schedules of the
 // same list (a persistent round robin, one CTA per item) and keeps the faster.  Each model's K split count is its context's own
 // (kls_autotune chooses it), so a determinant from the batch is bitwise the
-// one kls_det_batch returns for the same context.
+// one kls_det_batch returns for the same context.  When every model's
+// split-BF16 form is the TMEM-operand one, the contraction is that form's
+// kernel body driven by per-model descriptors, one CTA pair per (model, tile
+// pair, K split); otherwise the one-CTA form's body.
 #include "kls_internal.cuh"
 #include <cuda.h>
 #include <algorithm>
@@ -37,6 +40,12 @@ struct kls_multi {
   std::vector<kls_item> list;       // mixed: items in locality order
   std::vector<int> starts;          // mixed: per-CTA item ranges
   int schedule = 0;                 // mixed: 0 persistent round robin, 1 one CTA per item
+  bool tm = false;                  // mixed: every model in the TMEM-operand form
+  std::vector<kls_tm_model> tmd;    // its per-model descriptors
+  std::vector<int4> tm_items;       // (model, tile pair, split): one CTA pair each
+  kls_tm_model* d_tm = nullptr;
+  int4* d_tm_items = nullptr;
+  int max_Npad = 0;
   double schedule_ms[2] = {0, 0};   // mixed: eager-pass time of each schedule
   std::vector<int2> pairs;          // (model, omega) pairs
   int grid = 0, max_Na = 0;
@@ -108,6 +117,7 @@ int build_items(kls_multi* m) {
   m->pairs.clear();
   for (int i = 0; i < m->n_models; ++i)
     for (int z = 0; z < m->batch; ++z) m->pairs.push_back(make_int2(i, z));
+  if (m->tm) return KLS_OK;               // items built by build_tm_items
   std::vector<int> order(m->n_models);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -145,6 +155,27 @@ int build_items(kls_multi* m) {
     }
   }
   return KLS_OK;
+}
+
+// TMEM-operand form: one CTA pair per (model, tile pair, K split), model by
+// model with the largest first, split-major so that pairs running together
+// read the same k-range of one table.
+void build_tm_items(kls_multi* m) {
+  m->tm_items.clear();
+  std::vector<int> order(m->n_models);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    const kls_tm_model &x = m->tmd[a], &y = m->tmd[b];
+    return (double)x.K_pad * x.Npad * x.Npad > (double)y.K_pad * y.Npad * y.Npad;
+  });
+  for (int i : order) {
+    const kls_tm_model& d = m->tmd[i];
+    const int pairs = (d.n_tiles + 1) / 2;
+    for (int s = 0; s < d.splits; ++s)
+      for (int p = 0; p < pairs; ++p) m->tm_items.push_back(make_int4(i, p, s, 0));
+  }
+  m->grid = 2 * (int)m->tm_items.size();
+  m->schedule = 1;
 }
 
 // Mixed form: per-CTA item ranges of the ordered list.  Schedule 0: a
@@ -187,7 +218,10 @@ int launch_batch(kls_multi* m) {
   } else {
     // the mixed weights are converted from the FP64 weights of the same pass
     r = kls_multi_launch_f64_weights(m->stream, m->d_md, m->d_pairs, np, m->max_K_pad);
-    if (!r)
+    if (!r && m->tm)
+      r = kls_tm_multi_launch(m->stream, m->d_md, m->d_tm, m->d_pairs, np, m->d_tm_items,
+                              (int)m->tm_items.size(), m->max_K_pad, m->max_Npad, m->d_err);
+    else if (!r)
       r = kls_multi_launch_mixed(m->stream, m->d_md, m->d_pairs, np, m->d_items, m->d_starts,
                                  m->grid, m->max_K_pad, m->d_err);
   }
@@ -366,6 +400,16 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
     return bail(mcuda(m, cudaGetLastError(), "cudaMemset"));
 
   m->md.resize(n_models);
+  if (mode == KLS_MODE_MIXED) {
+    // one kernel for the whole batch: the TMEM-operand form when it is every
+    // model's form, else the one-CTA kernel body
+    m->tm = true;
+    for (int i = 0; i < n_models; ++i) {
+      if (!models[i]->mixed && (r = kls_mixed_prepare(models[i])))
+        return bail(mfail(m, r, models[i]->err));
+      if (!kls_mixed_tm_state(models[i], nullptr)) m->tm = false;
+    }
+  }
   for (int i = 0; i < n_models; ++i) {
     kls_ctx* c = models[i];
     kls_mdesc d{};
@@ -391,6 +435,29 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
         return bail(r);
     } else {
       if (!c->mixed && (r = kls_mixed_prepare(c))) return bail(mfail(m, r, c->err));
+      if (m->tm) {
+        // TMEM-operand form: plain FP32 weights and this form's partials
+        unsigned long long wns = 0;
+        kls_mixed_tm* t = kls_mixed_tm_state(c, &wns);
+        kls_tm_model td;
+        kls_tm_describe(c, t, wns, batch, &td);
+        float2* w32 = nullptr;
+        double* mp = nullptr;
+        if ((r = malloc_buf(m, &w32, (size_t)batch * c->K_pad)) ||
+            (r = malloc_buf(m, &mp, (size_t)td.n_tiles * td.splits * c->Na_pad * 128)))
+          return bail(r);
+        td.wt32 = w32;
+        td.part = mp;
+        m->tmd.push_back(td);
+        d.wt32 = w32;
+        d.mpart = mp;
+        d.msplits = td.splits;
+        m->md[i] = d;
+        m->max_Na = std::max(m->max_Na, c->Na);
+        m->max_K_pad = std::max(m->max_K_pad, c->K_pad);
+        m->max_Npad = std::max(m->max_Npad, c->Na_pad);
+        continue;
+      }
       const void *xl = nullptr, *th = nullptr, *tl = nullptr;
       d.Xh = kls_mixed_tables(c, &xl, &th, &tl);
       d.Xl = xl;
@@ -419,6 +486,17 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
     m->max_Na = std::max(m->max_Na, c->Na);
     m->max_K_pad = std::max(m->max_K_pad, c->K_pad);
   }
+  if (m->tm) {
+    build_tm_items(m);
+    if ((r = malloc_buf(m, &m->d_tm, m->tmd.size())) ||
+        (r = malloc_buf(m, &m->d_tm_items, m->tm_items.size())))
+      return bail(r);
+    if (cudaMemcpy(m->d_tm, m->tmd.data(), m->tmd.size() * sizeof(kls_tm_model),
+                   cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->d_tm_items, m->tm_items.data(), m->tm_items.size() * sizeof(int4),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (TMEM-form descriptors)"));
+  }
   if ((r = build_items(m))) return bail(r);
   const size_t n_it = std::max(m->items.size(), m->list.size());
   if ((r = malloc_buf(m, &m->d_md, m->md.size())) || (r = malloc_buf(m, &m->d_items, n_it)) ||
@@ -434,6 +512,10 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
                    cudaMemcpyHostToDevice) != cudaSuccess)
       return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (items)"));
     if ((r = eager_pass(m, nullptr))) return bail(r);
+  } else if (m->tm) {
+    float ms = 0.f;
+    if ((r = eager_pass(m, nullptr)) || (r = eager_pass(m, &ms))) return bail(r);
+    m->schedule_ms[0] = m->schedule_ms[1] = ms;     // one schedule: a CTA pair per item
   } else {
     // schedule tuning: one warm-up pass, then one timed pass per schedule
     if ((r = schedule_items(m, 0)) || (r = eager_pass(m, nullptr))) return bail(r);
@@ -510,7 +592,7 @@ int kls_multi_get_info(const kls_multi* m, kls_multi_info* out) {
   out->n_models = m->n_models;
   out->batch = m->batch;
   out->mode = m->mode;
-  out->n_items = (int32_t)m->items.size();
+  out->n_items = (int32_t)(m->tm ? m->tm_items.size() : m->items.size());
   out->grid = m->grid;
   out->graph = m->exec ? 1 : 0;
   out->replays = m->replays;

@@ -43,16 +43,17 @@ def pcs(lib_path):
         x.close()
 
 
-@pytest.mark.parametrize("Tgpu", ["Float64", "Float32"])
-def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu):
+@pytest.mark.parametrize("Tgpu,form", [("Float64", None), ("Float32", _lib.KLS_MIXED_ONE_CTA),
+                                       ("Float32", _lib.KLS_MIXED_TMEM)])
+def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu, form):
     n = 7                                  # passes of 3: 3 + 3 + 1
     om = np.stack([omegas(n, 10 + i) * (m / 2) for i, (m, *_) in enumerate(MODELS)])
     singles = []
     for pc, o in zip(pcs, om):
         dev = K.to_device(pc, K.GPUType.NVIDIA, Tgpu)
-        if Tgpu == "Float32":
-            # the batch runs the one-CTA kernel body: compare with that form
-            pc.ctx.call("kls_set_mixed_form", _lib.KLS_MIXED_ONE_CTA)
+        if form is not None:
+            # the batch runs this form's kernel body when it is every model's form
+            pc.ctx.call("kls_set_mixed_form", form)
         singles.append(K.compute_determinant_batched(o, pc, dev, batch_size=16, log_abs=True))
     mb = K.ModelBatch(pcs, Tgpu, batch=3)
     d, la = mb.det(om)
@@ -198,3 +199,35 @@ def test_ksharded_lu_batch_larger_than_one_chunk(lib_path):
         dist.destroy_process_group()
     ref = np.linalg.det(np.eye(N)[None] - mats)
     assert np.max(np.abs(d - ref) / np.abs(ref)) < 1e-11
+
+
+def test_batched_m3_real_q1_model_matches_oracle(pcs):
+    """Model 1 of the batch (m = 3, n_zang = 3, q1 = 9.5, NR = 31, Ne = 9,
+    N_alpha = 97, l = +-6) evaluated inside the uneven batch against the
+    oracle directly: FP64 within 1e-11 relative + 4x the oracle's own 2-ulp-ln
+    sensitivity, split-BF16 within 1e-3 relative."""
+    from oracle import np_oracle as O
+    m, nz, q, nr, ne, na, lm = MODELS[1]
+    over = dict(BASE, m=m, n_zang=nz, q1=q, NR=nr, Ne=ne, N_alpha=na, l_min=-lm, l_max=lm)
+    om = np.stack([omegas(5, 40 + i) * (mm / 2) for i, (mm, *_) in enumerate(MODELS)])
+    mb64 = K.ModelBatch(pcs, "Float64", batch=5)
+    d64, _ = mb64.det(om)
+    mb64.close()
+    mb32 = K.ModelBatch(pcs, "Float32", batch=5)
+    d32, _ = mb32.det(om)
+    mb32.close()
+
+    def oracle_dets():
+        pc = O.precompute_all(O.OracleConfig(**over))
+        return np.array([O.compute_det(pc, w) for w in om[1]])
+
+    ref = oracle_dets()
+    orig = O.orbit_log
+    O.orbit_log = lambda x: orig(x) * (1.0 + 4.440892098500626e-16)
+    try:
+        sens = np.abs(oracle_dets() - ref)
+    finally:
+        O.orbit_log = orig
+    assert np.all(np.abs(d64[1] - ref) <= 1e-11 * np.abs(ref) + 4 * sens), \
+        np.abs(d64[1] - ref) / np.abs(ref)
+    assert np.max(np.abs(d32[1] - ref) / np.abs(ref)) < 1e-3
