@@ -61,8 +61,9 @@ def parse():
     ap.add_argument("--accuracy-points", type=int, default=200)
     ap.add_argument("--no-proposer", action="store_true",
                     help="skip the learned-proposal time-to-root block")
-    ap.add_argument("--full-scan", action="store_true",
-                    help="time the whole FP64 41x20 scan instead of two of its columns")
+    ap.add_argument("--scan-columns", type=int, default=0,
+                    help="time only this many columns of the FP64 41x20 scan and scale "
+                         "(0: the whole scan, measured)")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the 16-model uneven batched scan block")
     ap.add_argument("--no-refgpu", action="store_true",
@@ -73,8 +74,11 @@ def parse():
                     help="save the held-out network's parameters (.npy) after training")
     ap.add_argument("--heldout-params", default="",
                     help="load the held-out network's parameters (.npy) instead of training")
-    ap.add_argument("--uneven-passes", type=int, default=3)
-    ap.add_argument("--uneven-batch", type=int, default=4)
+    ap.add_argument("--uneven-columns", type=int, default=1,
+                    help="whole Omega_p columns (128 gammas) of the 256 x 128 grid per model")
+    ap.add_argument("--uneven-batch", type=int, default=16)
+    ap.add_argument("--uneven-out", default="",
+                    help="save the evaluated log|det| / arg det maps of the 16 models (.npz)")
     return ap.parse_args()
 
 
@@ -478,17 +482,16 @@ def time_to_root(args, K, P, cfg, pc, local, sync):
     t0 = time.perf_counter()
     dgm, Op_m, g_m = K.grid_scan(cfg, pc, devmx)
     t_scan_mx = time.perf_counter() - t0
-    if args.full_scan:
+    if args.scan_columns <= 0:
         t0 = time.perf_counter()
         dg64, Op64, g64 = K.grid_scan(cfg, pc, None)
         t_scan64 = time.perf_counter() - t0
         scan_note = "measured: whole 41 x 20 FP64 scan"
     else:
-        # two whole columns of the FP64 scan (the mixed argmin's and its
-        # neighbour), the same batches of 16 the scan launches; every point
-        # costs the same, so the scan time is the column time x n_Op / 2
+        # whole columns of the FP64 scan (the mixed argmin's and its
+        # neighbours), the same batches of 16 the scan launches, scaled
         j = int(np.argmin(np.abs(Op_grid - Op_m)))
-        cols = [j, j + 1 if j + 1 < s.n_Op else j - 1]
+        cols = sorted({min(max(j + d, 0), s.n_Op - 1) for d in range(args.scan_columns)})
         om = np.array([m * Op_grid[c] + 1j * g for c in cols for g in g_grid])
         t0 = time.perf_counter()
         d64 = K.compute_determinant_batched(om, pc, None, batch_size=16)
@@ -497,8 +500,7 @@ def time_to_root(args, K, P, cfg, pc, local, sync):
         q = int(np.argmin(np.abs(d64)))
         Op64, g64 = float(Op_grid[cols[q // s.n_gamma]]), float(g_grid[q % s.n_gamma])
         scan_note = (f"extrapolated: columns {cols} of {s.n_Op} ({len(om)} FP64 dets in "
-                     f"{t_cols:.2f} s) x {s.n_Op}/{len(cols)}; FP64 argmin of those columns "
-                     f"{'equals' if (Op64, g64) == (Op_m, g_m) else 'differs from'} the mixed scan's")
+                     f"{t_cols:.2f} s) x {s.n_Op}/{len(cols)}")
     sync()
     t0 = time.perf_counter()
     r64 = K.newton_search(cfg, pc, None, K.GPUType.NVIDIA, "Float64", Op64, g64)
@@ -526,6 +528,8 @@ def time_to_root(args, K, P, cfg, pc, local, sync):
         "same_root_within_1e-10": bool(rh.converged and r64.converged and dOp <= 1e-10
                                        and dg <= 1e-10),
         "speedup_learned_vs_plain": plain_total / learned_total,
+        "learned_total_with_training_s": learned_total + t_gen + t_train,
+        "speedup_learned_with_training_vs_plain": plain_total / (learned_total + t_gen + t_train),
         "timing": "host wall clock around synchronous library calls"})
     return out
 
@@ -634,6 +638,12 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
 # per pass, split-BF16 form, autotuned K splits
 # ---------------------------------------------------------------------------
 def uneven_batch(args, K, P, local, sync):
+    """Config [3]: 16 seeded models of three sizes on the 256 x 128 grid over
+    Omega_p [0.2, 0.8], gamma [0.01, 0.30], split-BF16; the first
+    `--uneven-columns` whole Omega_p columns (128 gammas each) of every model
+    are evaluated (one graph replay per pass of `--uneven-batch` omegas per
+    model) and the full grid's time is projected from them.  With
+    `--uneven-out` the log|det| and arg det maps are saved (.npz)."""
     import numpy as np
     base = K.load_model(K.load_config(args.config), args.model)
     specs = P.random_models(16, seed=0, sizes=P.SIZES)
@@ -647,51 +657,64 @@ def uneven_batch(args, K, P, local, sync):
         pcs.append(pc)
     sync()
     t_setup = time.perf_counter() - t0
-    B, npass = args.uneven_batch, args.uneven_passes
+    B, cols = args.uneven_batch, args.uneven_columns
     nO, nG = 256, 128
     Op = np.linspace(0.2, 0.8, nO)
     gm = np.linspace(0.01, 0.30, nG)
-    q = np.arange((npass + 1) * B)                  # first grid points, column-major
+    n_pts = cols * nG                                   # column-major: whole columns
+    q = np.arange(n_pts)
     pts = Op[q // nG], gm[q % nG]
     om = np.stack([sp.m * pts[0] + 1j * pts[1] for sp in specs])
     mb = K.ModelBatch(pcs, "Float32", batch=B)
-    mb.det(om[:, :B])                                 # warm-up pass
+    mb.det(om[:, :B])                                   # warm-up pass
     sync()
+    dets = np.empty(om.shape, dtype=np.complex128)
+    la = np.empty(om.shape)
     t0 = time.perf_counter()
     dev_ms = 0.0
-    for p in range(1, npass + 1):
-        mb.det(om[:, p * B:(p + 1) * B])
+    npass = 0
+    for p0 in range(0, n_pts, B):
+        d, l = mb.det(om[:, p0:p0 + B])
+        dets[:, p0:p0 + B], la[:, p0:p0 + B] = d, l
         dev_ms += mb.info()["last_ms"]
+        npass += 1
     t_wall = time.perf_counter() - t0
     info = mb.info()
     mb.close()
-    n_det = len(specs) * B * npass
-    # the same omegas model by model through each context's own batch call
+    n_det = len(specs) * n_pts
+    # one column model by model through each context's own batch call
     sync()
     t0 = time.perf_counter()
     for pc, o in zip(pcs, om):
         dev = K.to_device(pc, K.GPUType.NVIDIA, "Float32")
-        for p in range(1, npass + 1):
-            K.compute_determinant_batched(o[p * B:(p + 1) * B], pc, dev, batch_size=B)
+        K.compute_determinant_batched(o[:nG], pc, dev, batch_size=B)
     t_seq = time.perf_counter() - t0
     for pc in pcs:
         pc.close()
     rate = n_det / (dev_ms * 1e-3)
+    if args.uneven_out:
+        np.savez_compressed(args.uneven_out, log_abs=la.reshape(len(specs), cols, nG),
+                            arg=np.angle(dets).reshape(len(specs), cols, nG),
+                            Omega_p=Op[:cols], gamma=gm,
+                            models=np.array([[sp.n_zang, sp.q1, sp.m, *sp.size] for sp in specs]))
     sizes = [sp.size for sp in specs]
     return {
         "models": len(specs), "model_seed": 0, "sizes": {str(sz): sizes.count(sz) for sz in P.SIZES},
         "grid": "256 x 128 over Omega_p [0.2, 0.8], gamma [0.01, 0.30]",
-        "omegas_per_model_per_pass": B, "passes_timed": npass,
+        "evaluated": f"{cols} whole Omega_p column(s) x 128 gammas per model ({n_det} dets)",
+        "omegas_per_model_per_pass": B, "passes": npass,
         "det_evals_per_s": rate, "ms_per_pass_device": dev_ms / npass,
         "wall_det_evals_per_s": n_det / t_wall,
-        "one_model_at_a_time_det_evals_per_s": n_det / t_seq,
+        "one_model_at_a_time_det_evals_per_s": len(specs) * nG / t_seq,
         "projected_full_grid_s": len(specs) * nO * nG / rate,
+        "maps_saved": args.uneven_out or None,
         "batch_launch": {"items": info["n_items"], "ctas": info["grid"],
-                         "schedule": ["persistent round robin", "one CTA per item"][info["schedule"]],
+                         "schedule": ["persistent round robin", "one CTA (pair) per item"][
+                             info["schedule"]],
                          "schedule_pass_ms": info["schedule_ms"],
                          "graph_replay": bool(info["graph"]),
                          "kernels_per_pass": info["launches_per_replay"]},
-        "autotune": [{"splits": t.splits, "default": t.default_splits,
+        "autotune": [{"splits": t.splits, "default": t.default_splits, "form": t.form,
                       "ms_per_omega": t.ms_per_omega,
                       "default_ms_per_omega": t.default_ms_per_omega} for t in tunes],
         "setup_s": t_setup,
