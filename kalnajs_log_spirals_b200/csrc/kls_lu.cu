@@ -352,6 +352,11 @@ static int lu_cluster_size(int device, int n) {
 
 static int run_lu_cluster(kls_ctx* c, int n, int C) {
   const size_t bytes = luc_smem_bytes(c->Na, C);
+  // the limit is a property of the kernel shared by all contexts: set it for
+  // this context's N right before its launch (another context may have set
+  // a smaller one)
+  KLS_CK(c, cudaFuncSetAttribute(lu_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)bytes));
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;

@@ -469,6 +469,18 @@ __global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, doub
   }
 }
 
+// The dynamic shared-memory limit is a property of the kernel, shared by
+// every context in the process: set it once to the largest stage layout
+// (N_alpha_pad = 384), so that contexts of any size can launch.
+cudaError_t tm_set_smem_limits() {
+  cudaError_t e = cudaFuncSetAttribute(mixed_tm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)tm_smem(384));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(mixed_tm_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tm_smem(384));
+  return e;
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -498,8 +510,7 @@ int kls_tm_default_splits(const kls_ctx* c) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
   int pairs = sms / 2;
-  cudaFuncSetAttribute(mixed_tm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)tm_smem(c->Na_pad));
+  tm_set_smem_limits();
   cudaLaunchConfig_t lc = {};
   lc.gridDim = dim3(2 * pairs, 1, 1);
   lc.blockDim = dim3(TM_THREADS, 1, 1);
@@ -542,8 +553,7 @@ int kls_tm_create(kls_ctx* c, const void* Xh, const void* Xl, kls_mixed_tm** out
     }
   }
   t->splits = kls_tm_default_splits(c);
-  cudaError_t e = cudaFuncSetAttribute(mixed_tm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)tm_smem(c->Na_pad));
+  cudaError_t e = tm_set_smem_limits();
   if (e != cudaSuccess) {
     delete t;
     return kls_cuda_fail(c, e, "cudaFuncSetAttribute (TMEM-operand form)");
@@ -639,9 +649,7 @@ int kls_tm_multi_launch(cudaStream_t st, const kls_mdesc* d_md, const kls_tm_mod
   const int wblocks = (int)std::min<int64_t>((max_K_pad + 255) / 256, 1024);
   tm_multi_weights32_kernel<<<dim3(wblocks, n_pairs), 256, 0, st>>>(d_md, d_pairs);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
-  if ((e = cudaFuncSetAttribute(mixed_tm_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tm_smem(max_Npad))) != cudaSuccess)
-    return (int)e;
+  if ((e = tm_set_smem_limits()) != cudaSuccess) return (int)e;
   mixed_tm_multi_kernel<<<2 * n_items, TM_THREADS, tm_smem(max_Npad), st>>>(d_tm, d_items, d_err);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   tm_multi_reduce_kernel<<<dim3(256, n_pairs), 256, 0, st>>>(d_md, d_pairs);
