@@ -53,3 +53,23 @@ def test_lu_mode_rejects_unknown(lib_path):
     lib = pc.ctx.lib
     assert lib.kls_set_lu_mode(pc.ctx.h, 7) == _lib.KLS_ERR_CONFIG
     pc.close()
+
+
+def test_contexts_of_different_sizes_interleave(lib_path):
+    """Kernel launch limits (dynamic shared memory) are per kernel, shared by
+    all contexts: a larger context created first and used after a smaller one
+    still launches, in the cluster LU and the TMEM-operand contraction."""
+    big = K.precompute_all(kconfig(**BASE, N_alpha=301))
+    small = K.precompute_all(kconfig(**BASE, N_alpha=161))
+    om = np.array([0.88 + 0.12j, 0.7 + 0.05j])
+    devs = [K.to_device(p, K.GPUType.NVIDIA, "Float32") for p in (big, small)]
+    for p in (big, small):
+        p.ctx.call("kls_set_mixed_form", _lib.KLS_MIXED_TMEM)
+    first = [dets(p, om, _lib.KLS_LU_CLUSTER)[0] for p in (big, small)]
+    mixed = [K.compute_determinant_batched(om, p, d) for p, d in zip((big, small), devs)]
+    again = [dets(p, om, _lib.KLS_LU_CLUSTER)[0] for p in (big, small)]
+    mixed2 = [K.compute_determinant_batched(om, p, d) for p, d in zip((big, small), devs)]
+    big.close()
+    small.close()
+    for a, b in zip(first + mixed, again + mixed2):
+        assert np.array_equal(a, b)
