@@ -63,7 +63,11 @@ def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu, form):
         assert np.array_equal(d[i], ds), (i, np.max(np.abs(d[i] - ds) / np.abs(ds)))
         assert np.array_equal(la[i], ls), i
     assert info["graph"] == 1 and info["replays"] == 3 and info["n_models"] == len(MODELS)
-    assert info["launches_per_replay"] >= 4 and info["n_items"] >= info["grid"] > 0
+    assert info["launches_per_replay"] >= 4 and info["n_items"] > 0 and info["grid"] > 0
+    if form == _lib.KLS_MIXED_TMEM:
+        assert info["grid"] == 2 * info["n_items"]            # one CTA pair per item
+    else:
+        assert info["n_items"] >= info["grid"]
     if Tgpu == "Float32":
         assert info["schedule"] in (0, 1) and min(info["schedule_ms"]) > 0
 
