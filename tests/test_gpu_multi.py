@@ -110,7 +110,10 @@ def test_autotune(lib_path, Tgpu):
     assert t.candidates >= 2 and t.splits >= 1 and t.default_splits >= 1
     assert 0 < t.ms_per_omega <= t.default_ms_per_omega * 1.0001
     after = K.compute_determinant_batched(om, pc, dev)
-    tol = 1e-12 if Tgpu == "Float64" else 1e-5
+    # FP64: a split count only regroups the FP64 sum; split-BF16: tuning may
+    # also change the kernel, whose summation orders differ by their FP32
+    # accumulation error (~2e-5 of the scale at this size)
+    tol = 1e-12 if Tgpu == "Float64" else 1e-4
     assert np.max(np.abs(after - before) / np.abs(before)) < tol
     again = K.autotune(pc, Tgpu, batch=2)          # process cache
     assert again.candidates == 0 and again.splits == t.splits
