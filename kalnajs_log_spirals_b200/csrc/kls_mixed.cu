@@ -15,7 +15,10 @@
 // an FP64 partial in global memory (deterministic order); the split-K
 // reduction, the weights w(omega), the LU and the determinant are FP64.
 //
-// Table: Xh/Xl [2 Npad][K_pad] BF16, built once by split_table_kernel from
+// Table: Xh/Xl BF16 in 64-k blocks, element (row r, k) at
+// (k / 64) * (2 Npad * 64) + r * 64 + k % 64 (each block of 64 k over all
+// rows contiguous, so that one stage reads a few pages rather than one page
+// per table row), built once by split_table_kernel from
 // the FP64 table.  Contraction CTA (one per SM, 16 warps):
 //   warp 0       TMA: X tile 128 rows x 64 k (hi, lo; 128B swizzle)
 //   warp 3       bulk copies of the FP32 weights into their own 8-deep ring,
@@ -89,10 +92,13 @@ __device__ __forceinline__ void split2(double v, __nv_bfloat16& hi, __nv_bfloat1
   lo = __float2bfloat16_rn((float)(v - (double)__bfloat162float(hi)));
 }
 
-// [K_pad][Npad] FP64 planes -> X{h,l}[2 Npad][K_pad] (row a: Re, row Npad + a: Im)
+// [K_pad][Npad] FP64 planes -> X{h,l}, rows a (Re) and Npad + a (Im), in
+// 64-k blocks: element (r, k) at (k / 64) * (2 Npad * 64) + r * 64 + k % 64
 __global__ void split_table_kernel(const double* __restrict__ Wre, const double* __restrict__ Wim,
                                    int Npad, int64_t K_pad, __nv_bfloat16* __restrict__ Xh,
                                    __nv_bfloat16* __restrict__ Xl) {
+  (void)K_pad;
+  const size_t blk = (size_t)2 * Npad * MX_BK;      // elements of one 64-k block
   __shared__ double tr[32][33], ti[32][33];
   const int64_t k0 = (int64_t)blockIdx.x * 32;
   const int a0 = blockIdx.y * 32;
@@ -105,11 +111,12 @@ __global__ void split_table_kernel(const double* __restrict__ Wre, const double*
   for (int i = ty; i < 32; i += 8) {
     __nv_bfloat16 h, l;
     split2(tr[tx][i], h, l);
-    size_t o = (size_t)(a0 + i) * K_pad + k0 + tx;
+    const int64_t k = k0 + tx;
+    size_t o = (size_t)(k >> 6) * blk + (size_t)(a0 + i) * MX_BK + (k & 63);
     Xh[o] = h;
     Xl[o] = l;
     split2(ti[tx][i], h, l);
-    o = (size_t)(Npad + a0 + i) * K_pad + k0 + tx;
+    o = (size_t)(k >> 6) * blk + (size_t)(Npad + a0 + i) * MX_BK + (k & 63);
     Xh[o] = h;
     Xl[o] = l;
   }
@@ -205,11 +212,10 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
       for (int i = 0; i < nkb; ++i) {
         const int s = i % MX_STAGES, r = i / MX_STAGES;
         if (!mbar_wait(smem_u32(&bar_empty[s]), (r & 1) ^ 1, &s_abort, err, 1)) break;
-        const int64_t kx = (int64_t)(kb0 + i) * MX_BK;
         const uint32_t fb = smem_u32(&bar_full_x[s]);
         mbar_arrive_tx(fb, 2 * MX_TILE_X);
-        tma_load_2d(smem_u32(xh_s(s)), &tm_h, (int)kx, m0, fb);
-        tma_load_2d(smem_u32(xl_s(s)), &tm_l, (int)kx, m0, fb);
+        tma_load_3d(smem_u32(xh_s(s)), &tm_h, 0, m0, kb0 + i, fb);
+        tma_load_3d(smem_u32(xl_s(s)), &tm_l, 0, m0, kb0 + i, fb);
         issued = i + 1;
       }
       // the last copies into each stage land before the CTA may exit
@@ -281,14 +287,14 @@ mixed_contract_kernel(const __grid_constant__ CUtensorMap tm_h,
       al_u[u] = (pt >> 3) + 32 * u;
       c_u[u] = pt & 7;
       const size_t a = (size_t)(a0 + al_u[u]);
-      rows_u[u][0] = Xh + a * P.K_pad;
-      rows_u[u][1] = Xl + a * P.K_pad;
-      rows_u[u][2] = Xh + (P.Npad + a) * P.K_pad;
-      rows_u[u][3] = Xl + (P.Npad + a) * P.K_pad;
+      rows_u[u][0] = Xh + a * MX_BK;
+      rows_u[u][1] = Xl + a * MX_BK;
+      rows_u[u][2] = Xh + (P.Npad + a) * MX_BK;
+      rows_u[u][3] = Xl + (P.Npad + a) * MX_BK;
     }
     uint4 pre[2][4];
     auto prefetch = [&](int i) {
-      const int64_t kb = (int64_t)(kb0 + i) * MX_BK;
+      const int64_t kb = (int64_t)(kb0 + i) * P.rows * MX_BK;    // 64-k block
 #pragma unroll
       for (int u = 0; u < 2; ++u)
 #pragma unroll
@@ -544,9 +550,8 @@ mixed_pair_kernel(const __grid_constant__ CUtensorMap tm_h, const __grid_constan
         const uint32_t fb = mapa_u32(smem_u32(&bar_full_x[s]), 0);
         if (leader) mbar_arrive_tx(smem_u32(&bar_full_x[s]), (peer_rows ? 2 : 1) * 2 * MX_TILE_X);
         if (has_rows) {
-          const int64_t kx = (int64_t)(kb0 + i) * MX_BK;
-          tma_load_2d_pair(smem_u32(xh_s(s)), &tm_h, (int)kx, m0, fb);
-          tma_load_2d_pair(smem_u32(xl_s(s)), &tm_l, (int)kx, m0, fb);
+          tma_load_3d_pair(smem_u32(xh_s(s)), &tm_h, 0, m0, kb0 + i, fb);
+          tma_load_3d_pair(smem_u32(xl_s(s)), &tm_l, 0, m0, kb0 + i, fb);
         }
       }
     }
@@ -604,11 +609,11 @@ mixed_pair_kernel(const __grid_constant__ CUtensorMap tm_h, const __grid_constan
     const int pt = tid - 128;
     const int al = pt >> 3, c = pt & 7;
     const size_t a = (size_t)(ah0 + al);
-    const __nv_bfloat16* rows_u[4] = {Xh + a * P.K_pad, Xl + a * P.K_pad,
-                                      Xh + (P.Npad + a) * P.K_pad, Xl + (P.Npad + a) * P.K_pad};
+    const __nv_bfloat16* rows_u[4] = {Xh + a * MX_BK, Xl + a * MX_BK,
+                                      Xh + (P.Npad + a) * MX_BK, Xl + (P.Npad + a) * MX_BK};
     uint4 pre[4];
     auto prefetch = [&](int i) {
-      const int64_t kb = (int64_t)(kb0 + i) * MX_BK;
+      const int64_t kb = (int64_t)(kb0 + i) * R * MX_BK;         // 64-k block
 #pragma unroll
       for (int q = 0; q < 4; ++q)
         pre[q] = __ldg(reinterpret_cast<const uint4*>(rows_u[q] + kb + c * 8));
@@ -882,11 +887,10 @@ mixed_multi_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict_
             ok = false;
             break;
           }
-          const int64_t kx = (int64_t)(it.kb0 + i) * MX_BK;
           const uint32_t fb = smem_u32(&bar_full_x[s]);
           mbar_arrive_tx(fb, 2 * MX_TILE_X);
-          tma_load_2d(smem_u32(xh_s(s)), mh, (int)kx, m0, fb);
-          tma_load_2d(smem_u32(xl_s(s)), ml, (int)kx, m0, fb);
+          tma_load_3d(smem_u32(xh_s(s)), mh, 0, m0, it.kb0 + i, fb);
+          tma_load_3d(smem_u32(xl_s(s)), ml, 0, m0, it.kb0 + i, fb);
           ++g;
         }
       }
@@ -983,14 +987,14 @@ mixed_multi_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict_
       for (int u = 0; u < 2; ++u) {
         al_u[u] = (pt >> 3) + 32 * u;
         const size_t a = (size_t)(a0 + al_u[u]);
-        rows_u[u][0] = Xh + a * d.K_pad;
-        rows_u[u][1] = Xl + a * d.K_pad;
-        rows_u[u][2] = Xh + (d.Na_pad + a) * d.K_pad;
-        rows_u[u][3] = Xl + (d.Na_pad + a) * d.K_pad;
+        rows_u[u][0] = Xh + a * MX_BK;
+        rows_u[u][1] = Xl + a * MX_BK;
+        rows_u[u][2] = Xh + (d.Na_pad + a) * MX_BK;
+        rows_u[u][3] = Xl + (d.Na_pad + a) * MX_BK;
       }
       uint4 pre[2][4];
       auto prefetch = [&](int i) {
-        const int64_t kb = (int64_t)(it.kb0 + i) * MX_BK;
+        const int64_t kb = (int64_t)(it.kb0 + i) * 2 * d.Na_pad * MX_BK;   // 64-k block
 #pragma unroll
         for (int u = 0; u < 2; ++u)
 #pragma unroll
@@ -1191,19 +1195,21 @@ int kls_mixed_prepare(kls_ctx* c) {
   split_table_kernel<<<grid, dim3(32, 8), 0, c->stream>>>(c->d_Wre, c->d_Wim, c->Na_pad, c->K_pad,
                                                           m->Xh, m->Xl);
   KLS_LAUNCHED(c);
-  // TMA descriptors over X{h,l}: dims {K_pad, rows}, box {64 k, 128 rows}, 128B swizzle
+  // TMA descriptors over X{h,l}: box {64 k, 128 rows, 1 block}, 128B swizzle
   void* fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   KLS_CK(c, cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
   if (!fn || q != cudaDriverEntryPointSuccess)
     return kls_fail(c, KLS_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   EncodeTiledFn encode = (EncodeTiledFn)fn;
-  cuuint64_t dims[2] = {(cuuint64_t)c->K_pad, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)c->K_pad * sizeof(__nv_bfloat16)};
-  cuuint32_t box[2] = {MX_BK, MX_BM};
-  cuuint32_t estr[2] = {1, 1};
+  // 3-D view of the blocked table: {64 k, rows, 64-k blocks}
+  cuuint64_t dims[3] = {(cuuint64_t)MX_BK, (cuuint64_t)rows, (cuuint64_t)(c->K_pad / MX_BK)};
+  cuuint64_t strides[2] = {(cuuint64_t)MX_BK * sizeof(__nv_bfloat16),
+                           (cuuint64_t)rows * MX_BK * sizeof(__nv_bfloat16)};
+  cuuint32_t box[3] = {MX_BK, MX_BM, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
   for (int t = 0; t < 2; ++t) {
-    CUresult r = encode(t == 0 ? &m->tm_h : &m->tm_l, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+    CUresult r = encode(t == 0 ? &m->tm_h : &m->tm_l, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
                         t == 0 ? (void*)m->Xh : (void*)m->Xl, dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

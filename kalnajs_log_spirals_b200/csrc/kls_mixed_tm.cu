@@ -173,19 +173,20 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
         const int s = i % TM_STAGES, r = i / TM_STAGES;
         if (!mbar_wait_cl_lim(smem_u32(&bar_b_empty[s]), (r & 1) ^ 1, &s_abort, err, 1, lim)) break;
         if (!mbar_wait_lim(smem_u32(&bar_y_empty[s]), (r & 1) ^ 1, &s_abort, err, 11, lim)) break;
-        const int kx = (kb0 + i) * TM_KB;
+        // stage g of 32 k: half (g & 1) of the table's 64-k block g >> 1
+        const int g = kb0 + i, kx = (g & 1) * TM_KB, kz = g >> 1;
         if (leader) mbar_arrive_tx(smem_u32(&bar_b_full[s]), 2 * 4 * BT);
         const uint32_t fb = mapa_u32(smem_u32(&bar_b_full[s]), 0);
-        tma_load_2d_pair(smem_u32(b_tile(s, 0, 0)), tbh, kx, yb, fb);
-        tma_load_2d_pair(smem_u32(b_tile(s, 0, 1)), tbh, kx, P.Npad + yb, fb);
-        tma_load_2d_pair(smem_u32(b_tile(s, 1, 0)), tbl, kx, yb, fb);
-        tma_load_2d_pair(smem_u32(b_tile(s, 1, 1)), tbl, kx, P.Npad + yb, fb);
+        tma_load_3d_pair(smem_u32(b_tile(s, 0, 0)), tbh, kx, yb, kz, fb);
+        tma_load_3d_pair(smem_u32(b_tile(s, 0, 1)), tbh, kx, P.Npad + yb, kz, fb);
+        tma_load_3d_pair(smem_u32(b_tile(s, 1, 0)), tbl, kx, yb, kz, fb);
+        tma_load_3d_pair(smem_u32(b_tile(s, 1, 1)), tbl, kx, P.Npad + yb, kz, fb);
         const uint32_t yf = smem_u32(&bar_y_full[s]);
         mbar_arrive_tx(yf, 4 * TM_YTILE);
-        tma_load_2d(smem_u32(y_tile(s, 0, 0)), tyh, kx, a0, yf);
-        tma_load_2d(smem_u32(y_tile(s, 0, 1)), tyh, kx, P.Npad + a0, yf);
-        tma_load_2d(smem_u32(y_tile(s, 1, 0)), tyl, kx, a0, yf);
-        tma_load_2d(smem_u32(y_tile(s, 1, 1)), tyl, kx, P.Npad + a0, yf);
+        tma_load_3d(smem_u32(y_tile(s, 0, 0)), tyh, kx, a0, kz, yf);
+        tma_load_3d(smem_u32(y_tile(s, 0, 1)), tyh, kx, P.Npad + a0, kz, yf);
+        tma_load_3d(smem_u32(y_tile(s, 1, 0)), tyl, kx, a0, kz, yf);
+        tma_load_3d(smem_u32(y_tile(s, 1, 1)), tyl, kx, P.Npad + a0, kz, yf);
         issued = i + 1;
       }
       // the last copies into this CTA's shared memory land before it may exit
@@ -499,7 +500,7 @@ struct kls_mixed_tm {
 };
 
 bool kls_tm_supported(const kls_ctx* c) {
-  return c->Na_pad % TM_AB == 0 && c->Na_pad <= 384 && c->K_pad % TM_KB == 0;
+  return c->Na_pad % TM_AB == 0 && c->Na_pad <= 384 && c->K_pad % 64 == 0;
 }
 
 // K splits of the form: fixed per context (determinants do not depend on the
@@ -535,15 +536,17 @@ int kls_tm_create(kls_ctx* c, const void* Xh, const void* Xl, kls_mixed_tm** out
     return kls_fail(c, KLS_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   EncodeTiledFn encode = (EncodeTiledFn)fn;
   kls_mixed_tm* t = new kls_mixed_tm();
-  const cuuint64_t dims[2] = {(cuuint64_t)c->K_pad, (cuuint64_t)(2 * c->Na_pad)};
-  const cuuint64_t strides[1] = {(cuuint64_t)c->K_pad * sizeof(__nv_bfloat16)};
-  const cuuint32_t estr[2] = {1, 1};
-  const cuuint32_t box_b[2] = {TM_KB, (cuuint32_t)(c->Na_pad / 2)};
-  const cuuint32_t box_y[2] = {TM_KB, TM_AB};
+  // the split table in 64-k blocks: {64 k, 2 Na_pad rows, K_pad / 64 blocks}
+  const cuuint64_t rows = (cuuint64_t)(2 * c->Na_pad);
+  const cuuint64_t dims[3] = {64, rows, (cuuint64_t)(c->K_pad / 64)};
+  const cuuint64_t strides[2] = {64 * sizeof(__nv_bfloat16), rows * 64 * sizeof(__nv_bfloat16)};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const cuuint32_t box_b[3] = {TM_KB, (cuuint32_t)(c->Na_pad / 2), 1};
+  const cuuint32_t box_y[3] = {TM_KB, TM_AB, 1};
   struct { CUtensorMap* m; const void* base; const cuuint32_t* box; } maps[4] = {
       {&t->tb_h, Xh, box_b}, {&t->tb_l, Xl, box_b}, {&t->ty_h, Xh, box_y}, {&t->ty_l, Xl, box_y}};
   for (auto& mm : maps) {
-    CUresult r = encode(mm.m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(mm.base),
+    CUresult r = encode(mm.m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(mm.base),
                         dims, strides, mm.box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                         CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
