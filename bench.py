@@ -941,10 +941,14 @@ def ours(args):
             t0 = time.perf_counter()
             rh = newton_search_hybrid(cfg, pc)
             t_h = time.perf_counter() - t0
+            d64_h = K.compute_determinant(rh.omega, pc, None)     # outside the timed region
             newton["mixed_fp64_finish"] = {
                 "time_to_root_s": t_h, "Omega_p": rh.Omega_p, "gamma": rh.gamma,
-                "abs_det": abs(rh.det_val), "converged": rh.converged,
+                "abs_det": abs(rh.det_val), "abs_det_plain_fp64_at_result": abs(d64_h),
+                "converged": rh.converged,
                 "mixed_evals": rh.mixed_evals, "fp64_evals": rh.fp64_evals,
+                "anchored_evals": rh.anchored_evals,
+                "history": [[float(x) for x in row] for row in rh.history],
                 "abs_dOmega_p_vs_plain": abs(rh.Omega_p - r.Omega_p),
                 "abs_dgamma_vs_plain": abs(rh.gamma - r.gamma)}
             newton["speedup_hybrid_vs_plain"] = t_plain / t_h
@@ -955,8 +959,23 @@ def ours(args):
             d_pair = K.compute_determinant_batched(np.array([w_r, w_r + 1e-7]), pc, None)
             dprime = abs((d_pair[1] - d_pair[0]) / 1e-7)
             d_mx = K.compute_determinant(w_r, pc, K.to_device(pc, K.GPUType.NVIDIA, "Float32"))
+            # anchored form 1e-6 and 1e-5 from the root: M error against the
+            # FP64 M there, and its determinant residual at the root
+            M64 = K.build_M_matrix(w_r, pc, None)
+            dev_an = K.api.DevicePrecomputed(pc.m, pc.G, pc.N_alpha, pc.n_l, pc.NPh,
+                                             K.KLS_MODE_ANCHORED, pc)
+            anch = {}
+            for dist in (1e-6, 1e-5):
+                K.set_anchor(pc, w_r + dist * np.exp(0.7j))
+                Man = K.build_M_matrix(w_r, pc, dev_an)
+                d_an = K.compute_determinant(w_r, pc, dev_an)
+                anch[f"{dist:.0e}"] = {
+                    "M_err_over_max": float(np.abs(Man - M64).max() / np.abs(M64).max()),
+                    "abs_det_at_fp64_root": abs(d_an),
+                    "root_error_estimate": abs(d_an) / dprime}
             newton["at_fp64_root"] = {"abs_det_prime": dprime, "abs_mixed_det": abs(d_mx),
-                                      "mixed_root_error_estimate": abs(d_mx) / dprime}
+                                      "mixed_root_error_estimate": abs(d_mx) / dprime,
+                                      "anchored_at_distance": anch}
 
     # ---- parity against the oracle's default-size fixture ----------------------
     parity = None

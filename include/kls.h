@@ -47,6 +47,15 @@ extern "C" {
 #define KLS_MODE_FP64        0  /* plain FP64 (the oracle form)               */
 #define KLS_MODE_MIXED       1  /* split-BF16 tensor-core contraction, FP32
                                    accumulation; FP64 weights/LU              */
+#define KLS_MODE_ANCHORED    2  /* M(omega) = M(omega_a) + dM: the FP64 M at
+                                   the anchor set by kls_set_anchor plus the
+                                   split-BF16 contraction of the weight
+                                   differences w_k(omega) - w_k(omega_a).
+                                   dM is ~|omega - omega_a| / gamma of M, so
+                                   near the anchor its split-BF16 error is that
+                                   fraction of the split form's (1e-6 of omega
+                                   away: ~1e-11 of max|M|) at the cost of a
+                                   KLS_MODE_MIXED evaluation                  */
 
 /* ---- configuration: the [physics] [model] [grid] TOML sections ---------- *
  * Mirrors PhysicsConfig / ModelConfig / GridConfig
@@ -176,6 +185,12 @@ int kls_det_batch_device(kls_ctx* ctx, const double* d_omega_ri, int n, int mode
                          double* d_det_ri, double* d_log_abs);
 /* M(omega) [N_alpha, N_alpha] complex column-major (MatrixBuilder.jl:242).  */
 int kls_build_M(kls_ctx* ctx, double omega_re, double omega_im, int mode, double* M_ri);
+/* Anchor of KLS_MODE_ANCHORED (no reference counterpart): one FP64
+ * evaluation at omega_a that keeps M(omega_a) on the device (N_alpha^2
+ * complex) and returns det(I - M(omega_a)) in det_ri (may be NULL).  Needs
+ * the FP64 table (KLS_ERR_STATE after kls_release_fp64) and builds the
+ * split-BF16 table if it is missing.  A later call moves the anchor.       */
+int kls_set_anchor(kls_ctx* ctx, double omega_re, double omega_im, double* det_ri);
 
 /* grid_scan (GridScan.jl:25-88): det_grid [n_gamma, n_Op] column-major
  * complex; argmin of |det| in column-major order (GridScan.jl:234-246).   */
@@ -187,32 +202,41 @@ int kls_scan(kls_ctx* ctx, const kls_scan_cfg* sc, double* det_grid_ri,
 int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cfg* nc,
                kls_newton_result* res, double* history);
 
-/* Mixed-precision Newton with an FP64 finish (no reference counterpart; it
- * returns the point at which the reference's own stopping rule,
- * |det| < nc->tol on the plain FP64 determinant, holds).  det(I - M(omega))
+/* Mixed-precision Newton with an FP64-anchored finish (no reference
+ * counterpart; it returns a point at which the reference's stopping rule
+ * |det| < nc->tol holds on a determinant of FP64 accuracy).  det(I - M(omega))
  * is holomorphic in omega = m Omega_p + i gamma, so one complex slope S gives
  * the reference's whole 2x2 finite-difference Jacobian (dF/dOmega_p = m S,
  * dF/dgamma = i S) and the step is delta omega = -det / S:
- *   phase 1: Newton on split-BF16 determinants, S by central difference of
- *            the triple (omega - h, omega, omega + h), h = m*mixed_delta,
- *            evaluated as one batch, until a step is shorter than
- *            mixed_step_tol or |det| has not halved for 3 steps (the split
- *            form's noise floor; mixed_delta ~1e-3 keeps the difference well
- *            above its ~5e-5 relative det error);
- *   phase 2: FP64 determinants, one per step: a chord step with the last
- *            split-BF16 slope, then secant slopes from the FP64 values; when
- *            a step does not lower |det| the slope is recomputed as an FP64
- *            forward difference (step nc->delta).  Once |det| < tol, one more
- *            step is taken (and kept if it lowers |det|) when the predicted
- *            correction exceeds 1e-11, since |det| < tol fixes the root only
- *            to tol / |det'|.                                               */
+ *   phase 1: secant iteration on split-BF16 determinants.  The first slope
+ *            is the forward difference of the pair (omega, omega + h),
+ *            h = m*mixed_delta, evaluated as one batch; each later step's
+ *            determinant gives the next secant slope.  It stops when the
+ *            next step is shorter than mixed_step_tol (that step is taken
+ *            without an evaluation), when |det| does not fall (the split
+ *            form's noise floor) or after mixed_max_iter steps.
+ *   phase 2: kls_set_anchor at the last point (one FP64 determinant), then
+ *            KLS_MODE_ANCHORED determinants, secant steps from those values
+ *            (FP64 accuracy near the anchor), starting with the phase-1
+ *            slope.  A step that lands farther than anchor_radius from the
+ *            anchor moves the anchor there (another FP64 determinant).  A
+ *            step that does not lower |det| is retried once with a slope by
+ *            forward difference (step nc->delta); the phase ends when |det|
+ *            < tol and the next step is below 1e-11 (|det| < tol alone fixes
+ *            the root only to tol / |det'|), when |det| < tol and |det|
+ *            stops falling, or after fp64_max_iter steps.  final_fp64 != 0
+ *            adds one plain FP64 determinant at the result, which then
+ *            decides `converged` and is the returned det.                 */
 typedef struct kls_hybrid_cfg {
     double  mixed_delta;
     double  mixed_step_tol;
     int32_t mixed_max_iter;
     int32_t fp64_max_iter;
+    double  anchor_radius;
+    int32_t final_fp64;
 } kls_hybrid_cfg;
-/* evals[0], evals[1] (may be NULL): mixed and FP64 determinant evaluations. */
+/* evals[0..2] (may be NULL): split-BF16, plain FP64 (anchors included) and
+ * anchored determinant evaluations.                                        */
 int kls_newton_hybrid(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cfg* nc,
                       const kls_hybrid_cfg* hc, kls_newton_result* res, int32_t* evals,
                       double* history);

@@ -13,8 +13,8 @@ from .api import (DevicePrecomputed, GPUType, NewtonResult, OrbitData, Precomput
                   compute_determinant_batched, create_toomre_zang_model, detect_gpu_type,
                   compute_determinant_ksharded, find_minimum, grid_scan, grid_scan_distributed,
                   harmonic_ranges, precompute_ksharded, newton_search, precompute_all, release_fp64,
-                  to_device)
-from ._lib import KLS_MODE_FP64, KLS_MODE_MIXED, KlsError
+                  set_anchor, to_device)
+from ._lib import KLS_MODE_ANCHORED, KLS_MODE_FP64, KLS_MODE_MIXED, KlsError
 
 __all__ = [
     "KalnajsConfig", "PhysicsConfig", "ModelConfig", "GridConfig", "ScanConfig", "NewtonConfig",
@@ -24,6 +24,7 @@ __all__ = [
     "create_toomre_zang_model", "PrecomputedData", "OrbitData", "precompute_all",
     "DevicePrecomputed", "to_device", "compute_determinant", "compute_determinant_batched",
     "build_M_matrix", "grid_scan", "find_minimum", "newton_search", "NewtonResult", "KlsError",
-    "KLS_MODE_FP64", "KLS_MODE_MIXED", "ModelBatch", "autotune", "TuneResult", "release_fp64", "grid_scan_distributed",
+    "KLS_MODE_FP64", "KLS_MODE_MIXED", "KLS_MODE_ANCHORED", "set_anchor", "ModelBatch",
+    "autotune", "TuneResult", "release_fp64", "grid_scan_distributed",
     "harmonic_ranges", "precompute_ksharded", "compute_determinant_ksharded",
 ]

@@ -23,6 +23,7 @@ KLS_ERR_TIMEOUT = 8
 
 KLS_MODE_FP64 = 0
 KLS_MODE_MIXED = 1
+KLS_MODE_ANCHORED = 2
 
 KLS_QUAD_DEFAULT = 0
 KLS_QUAD_TRAPEZOID = 1
@@ -83,7 +84,8 @@ class kls_newton_result(C.Structure):
 
 class kls_hybrid_cfg(C.Structure):
     _fields_ = [("mixed_delta", C.c_double), ("mixed_step_tol", C.c_double),
-                ("mixed_max_iter", C.c_int32), ("fp64_max_iter", C.c_int32)]
+                ("mixed_max_iter", C.c_int32), ("fp64_max_iter", C.c_int32),
+                ("anchor_radius", C.c_double), ("final_fp64", C.c_int32)]
 
 
 class kls_scan_cfg(C.Structure):
@@ -128,6 +130,7 @@ SIGNATURES = {
     "kls_det_batch": (C.c_int, [_P, _D, C.c_int, C.c_int, _D, _D]),
     "kls_det_batch_device": (C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
     "kls_build_M": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _D]),
+    "kls_set_anchor": (C.c_int, [_P, C.c_double, C.c_double, _D]),
     "kls_scan": (C.c_int, [_P, C.POINTER(kls_scan_cfg), _D, _D, _D, _D]),
     "kls_newton": (C.c_int, [_P, C.c_double, C.c_double, C.POINTER(kls_newton_cfg),
                              C.POINTER(kls_newton_result), _D]),

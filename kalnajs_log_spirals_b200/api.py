@@ -629,28 +629,42 @@ def newton_search(config: KalnajsConfig, precomputed: PrecomputedData,
 
 @dataclass
 class HybridConfig:
-    """Mixed-precision phase parameters of newton_search_hybrid.
+    """Parameters of newton_search_hybrid (kls_hybrid_cfg in include/kls.h).
 
-    The split-BF16 determinant carries a ~5e-5 relative error, so the
-    finite-difference step of the mixed phase is 1e-3 (a Jacobian error of
-    ~5e-2 x the distance to the root, truncation ~1e-3); the FP64 phase may
-    take as many steps as the reference's Newton (max_iter 50)."""
+    The split-BF16 determinant carries a ~5e-5 relative error, so the first
+    finite-difference slope of the mixed phase uses a step of 1e-3; the mixed
+    phase hands over once its next step is below 1e-5 (its root error is
+    ~1e-6).  Anchored determinants stay within FP64 accuracy for ~1e-5 around
+    the anchor; a step beyond anchor_radius re-anchors (one FP64
+    determinant)."""
     mixed_delta: float = 1e-3
-    mixed_step_tol: float = 1e-7
+    mixed_step_tol: float = 1e-5
     mixed_max_iter: int = 30
     fp64_max_iter: int = 50
+    anchor_radius: float = 1e-5
+    final_fp64: bool = False
+
+
+def set_anchor(precomputed: PrecomputedData, omega: complex) -> complex:
+    """FP64 M(omega_a) kept on the device for KLS_MODE_ANCHORED; returns
+    det(I - M(omega_a)) (no reference counterpart)."""
+    out = np.zeros(2)
+    precomputed.ctx.call("kls_set_anchor", float(np.real(omega)), float(np.imag(omega)),
+                         dptr(out))
+    return complex(out[0], out[1])
 
 
 def newton_search_hybrid(config: KalnajsConfig, precomputed: PrecomputedData,
                          Omega_p_init: Optional[float] = None,
                          gamma_init: Optional[float] = None,
                          hybrid: Optional[HybridConfig] = None) -> NewtonResult:
-    """Split-BF16 Newton, then FP64 chord steps to the reference's stopping rule.
+    """Split-BF16 secant phase, then an FP64 anchor and anchored steps to the
+    reference's stopping rule (kls_newton_hybrid).
 
-    No reference counterpart: the result satisfies |det(I - M)| < config.newton.tol
-    on the plain FP64 determinant, the same test newton_search applies
-    (NewtonSolver.jl:89); ``det_evals`` counts both precisions and
-    ``history`` has one row per determinant batch.
+    No reference counterpart: the result satisfies |det(I - M)| <
+    config.newton.tol (NewtonSolver.jl:89) on an FP64-accurate determinant
+    (the anchored form, or plain FP64 with ``final_fp64``); ``det_evals``
+    counts every evaluation and ``history`` has one row per evaluation.
     """
     n = config.newton
     hc = hybrid or HybridConfig()
@@ -662,16 +676,17 @@ def newton_search_hybrid(config: KalnajsConfig, precomputed: PrecomputedData,
     nc = _lib.kls_newton_cfg(int(n.max_iter), float(n.tol), float(n.delta),
                              int(bool(n.use_line_search)), int(n.max_line_search), KLS_MODE_FP64)
     h = _lib.kls_hybrid_cfg(float(hc.mixed_delta), float(hc.mixed_step_tol),
-                            int(hc.mixed_max_iter), int(hc.fp64_max_iter))
+                            int(hc.mixed_max_iter), int(hc.fp64_max_iter),
+                            float(hc.anchor_radius), int(bool(hc.final_fp64)))
     res = _lib.kls_newton_result()
-    ev = (C.c_int32 * 2)()
+    ev = (C.c_int32 * 3)()
     hist = np.zeros((int(n.max_iter), 3))
     precomputed.ctx.call("kls_newton_hybrid", float(Omega_p_init), float(gamma_init), C.byref(nc),
                          C.byref(h), C.byref(res), ev, dptr(hist))
     r = NewtonResult(res.Omega_p, res.gamma, complex(res.omega_re, res.omega_im),
                      complex(res.det_re, res.det_im), int(res.iterations), bool(res.converged),
                      hist[:min(res.iterations, int(n.max_iter))].copy(), int(res.det_evals))
-    r.mixed_evals, r.fp64_evals = int(ev[0]), int(ev[1])
+    r.mixed_evals, r.fp64_evals, r.anchored_evals = int(ev[0]), int(ev[1]), int(ev[2])
     return r
 
 

@@ -109,21 +109,24 @@ int ensure_ws(kls_ctx* c, int n) {
 int run_batch(kls_ctx* c, int n, int mode, bool export_M) {
   int r;
   const int splits = c->splits;
+  if (mode != KLS_MODE_FP64 && mode != KLS_MODE_MIXED && mode != KLS_MODE_ANCHORED)
+    return kls_fail(c, KLS_ERR_CONFIG, "unknown precision mode");
+  const bool anchored = mode == KLS_MODE_ANCHORED;
+  if (anchored && !c->anchor_set)
+    return kls_fail(c, KLS_ERR_STATE, "KLS_MODE_ANCHORED needs kls_set_anchor first");
   if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[0], c->stream));
-  if ((r = kls_run_weights(c, n))) return r;
+  if ((r = kls_run_weights(c, n, anchored ? c->anchor_w : nullptr))) return r;
   if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[1], c->stream));
   if (mode == KLS_MODE_FP64) {
     if (!c->d_Wre) return kls_fail(c, KLS_ERR_STATE, "the FP64 table was released (kls_release_fp64)");
     if ((r = kls_run_contract_f64(c, n, splits))) return r;
-  } else if (mode == KLS_MODE_MIXED) {
+  } else {
     if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
     if ((r = kls_mixed_contract(c, n, splits))) return r;
-  } else {
-    return kls_fail(c, KLS_ERR_CONFIG, "unknown precision mode");
   }
   if (c->timing) KLS_CK(c, cudaEventRecord(c->ev[2], c->stream));
-  if (mode == KLS_MODE_MIXED) {
-    if ((r = kls_mixed_reduce(c, n, export_M))) return r;
+  if (mode != KLS_MODE_FP64) {
+    if ((r = kls_mixed_reduce(c, n, export_M, anchored ? c->d_anchorM : nullptr))) return r;
   } else if ((r = kls_run_reduce(c, n, splits, export_M))) {
     return r;
   }
@@ -171,7 +174,7 @@ int det_batch_host(kls_ctx* c, const double* omega_ri, int n, int mode, double* 
       KLS_CK(c, cudaMemcpyAsync(log_abs + b, c->d_logabs, nb * sizeof(double),
                                 cudaMemcpyDeviceToHost, c->stream));
     KLS_CK(c, cudaStreamSynchronize(c->stream));
-    if (mode == KLS_MODE_MIXED && (r = kls_mixed_check(c))) return r;
+    if (mode != KLS_MODE_FP64 && (r = kls_mixed_check(c))) return r;
     if ((r = collect_timing(c))) return r;
     for (int i = 0; i < nb; ++i)
       if (std::isnan(det_ri[2 * (b + i)]) || std::isnan(det_ri[2 * (b + i) + 1])) {
@@ -284,7 +287,7 @@ int kls_destroy(kls_ctx* c) {
   void* ptrs[] = {c->d_cosw, c->d_sinw, c->d_of, c->d_SRC, c->d_rc, c->d_valid, c->d_w1, c->d_ra,
                   c->d_pha, c->d_alpha, c->d_dalpha, c->d_N, c->d_Gk, c->d_Ok, c->d_F0l,
                   c->d_Wre, c->d_Wim, c->d_omega, c->d_wt, c->d_part, c->d_A, c->d_M,
-                  c->d_det, c->d_logabs};
+                  c->d_anchorM, c->d_det, c->d_logabs};
   for (void* p : ptrs) dfree(p);
   for (auto& ev : c->ev) if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->pev) if (ev) cudaEventDestroy(ev);
@@ -462,13 +465,41 @@ int kls_build_M(kls_ctx* c, double wr, double wi, int mode, double* M) {
   KLS_CK(c, cudaMemcpyAsync(h.data(), c->d_M, h.size() * sizeof(double2), cudaMemcpyDeviceToHost,
                             c->stream));
   KLS_CK(c, cudaStreamSynchronize(c->stream));
-  if (mode == KLS_MODE_MIXED && (r = kls_mixed_check(c))) return r;
+  if (mode != KLS_MODE_FP64 && (r = kls_mixed_check(c))) return r;
   const int N = c->Na;
   for (int b = 0; b < N; ++b)
     for (int a = 0; a < N; ++a) {   // device [b][a] -> host column-major (b + N a)
       M[2 * (b + (size_t)N * a)] = h[(size_t)b * N + a].x;
       M[2 * (b + (size_t)N * a) + 1] = h[(size_t)b * N + a].y;
     }
+  return KLS_OK;
+}
+
+int kls_set_anchor(kls_ctx* c, double wr, double wi, double* det_ri) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (!std::isfinite(wr) || !std::isfinite(wi))
+    return kls_fail(c, KLS_ERR_NONFINITE, "non-finite anchor omega");
+  if (!c->d_Wre) return kls_fail(c, KLS_ERR_STATE, "the FP64 table was released (kls_release_fp64)");
+  if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
+  if (!c->d_anchorM && (r = dalloc(c, &c->d_anchorM, (size_t)c->Na * c->Na))) return r;
+  if ((r = ensure_ws(c, 1))) return r;
+  c->anchor_set = false;
+  const double om[2] = {wr, wi};
+  KLS_CK(c, cudaMemcpyAsync(c->d_omega, om, sizeof om, cudaMemcpyHostToDevice, c->stream));
+  if ((r = run_batch(c, 1, KLS_MODE_FP64, true))) return r;
+  KLS_CK(c, cudaMemcpyAsync(c->d_anchorM, c->d_M, (size_t)c->Na * c->Na * sizeof(double2),
+                            cudaMemcpyDeviceToDevice, c->stream));
+  double2 d;
+  KLS_CK(c, cudaMemcpyAsync(&d, c->d_det, sizeof d, cudaMemcpyDeviceToHost, c->stream));
+  KLS_CK(c, cudaStreamSynchronize(c->stream));
+  if ((r = collect_timing(c))) return r;
+  if (std::isnan(d.x) || std::isnan(d.y))
+    return kls_fail(c, KLS_ERR_NONFINITE, "NaN determinant at the anchor");
+  c->anchor_w[0] = wr;
+  c->anchor_w[1] = wi;
+  c->anchor_set = true;
+  if (det_ri) { det_ri[0] = d.x; det_ri[1] = d.y; }
   return KLS_OK;
 }
 
@@ -588,7 +619,8 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
                       double* history) {
   int r = check_ready(c);
   if (r) return r;
-  if (!nc || !hc || !res || hc->mixed_max_iter < 0 || hc->fp64_max_iter < 1)
+  if (!nc || !hc || !res || hc->mixed_max_iter < 0 || hc->fp64_max_iter < 1 ||
+      !(hc->mixed_delta > 0.0) || !(hc->anchor_radius > 0.0))
     return kls_fail(c, KLS_ERR_CONFIG, "bad hybrid Newton arguments");
   using cplx = std::complex<double>;
   const double m = (double)c->cfg.m, tol = nc->tol;
@@ -597,8 +629,9 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
     const double Op = std::min(std::max(w.real() / m, 0.0), 1.0);
     return cplx(m * Op, std::max(w.imag(), 1e-4));
   };
+  auto usable = [](cplx s) { return std::isfinite(std::abs(s)) && std::abs(s) > 0.0; };
   cplx w = clamp(cplx(m * Op_init, g_init));
-  int n_mixed = 0, n_fp64 = 0, it_total = 0;
+  int n_mixed = 0, n_fp64 = 0, n_anch = 0, it_total = 0;
   std::memset(res, 0, sizeof *res);
   auto hist = [&](cplx at, double a) {
     if (history && it_total < nc->max_iter) {
@@ -609,102 +642,114 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
     ++it_total;
   };
   auto det = [&](const cplx* ws, int n, int mode, cplx* out) -> int {
-    double in[6], o[6];
+    double in[4], o[4];
     for (int i = 0; i < n; ++i) { in[2 * i] = ws[i].real(); in[2 * i + 1] = ws[i].imag(); }
     int q = det_batch_host(c, in, n, mode, o, nullptr);
     if (q) return q;
     for (int i = 0; i < n; ++i) out[i] = cplx(o[2 * i], o[2 * i + 1]);
-    (mode == KLS_MODE_MIXED ? n_mixed : n_fp64) += n;
+    (mode == KLS_MODE_MIXED ? n_mixed : mode == KLS_MODE_FP64 ? n_fp64 : n_anch) += n;
     return KLS_OK;
+  };
+  auto finish = [&](cplx at, cplx d, bool conv) {
+    res->Omega_p = at.real() / m; res->gamma = at.imag();
+    res->omega_re = at.real(); res->omega_im = at.imag();
+    res->det_re = d.real(); res->det_im = d.imag();
+    res->iterations = it_total;
+    res->converged = conv ? 1 : 0;
+    res->det_evals = n_mixed + n_fp64 + n_anch;
+    if (evals) { evals[0] = n_mixed; evals[1] = n_fp64; evals[2] = n_anch; }
   };
   // det(I - M(omega)) is holomorphic in omega, so one complex slope S =
   // d det / d omega gives the whole 2x2 finite-difference Jacobian of the
   // reference (dF/dOmega_p = m S, dF/dgamma = i S) and the Newton step is
   // delta omega = -det / S.
-  // ---- phase 1: split-BF16 Newton, slope by central difference of the
-  //      triple (omega - h, omega, omega + h) evaluated as one batch
+  // ---- phase 1: split-BF16 secant iteration
   const double h = m * hc->mixed_delta;
-  cplx S(0.0, 0.0);
-  bool haveS = false;
-  double best = INFINITY;
-  int stall = 0;
-  for (int it = 0; it < hc->mixed_max_iter; ++it) {
-    const cplx ws[3] = {w - h, w, w + h};
-    cplx d[3];
-    if ((r = det(ws, 3, KLS_MODE_MIXED, d))) return r;
-    const double a = std::abs(d[1]);
-    hist(w, a);
-    // |det| no longer halving for 3 steps: the split form's noise floor
-    if (a < 0.5 * best) {
-      best = a;
-      stall = 0;
-    } else if (++stall >= 3) {
+  cplx S, f;
+  {
+    const cplx ws[2] = {w, w + h};
+    cplx d[2];
+    if ((r = det(ws, 2, KLS_MODE_MIXED, d))) return r;
+    hist(w, std::abs(d[0]));
+    f = d[0];
+    S = (d[1] - d[0]) / h;
+  }
+  bool haveS = usable(S);
+  for (int it = 0; haveS && it < hc->mixed_max_iter; ++it) {
+    const cplx wn = clamp(w - f / S);
+    if (std::abs(wn - w) < hc->mixed_step_tol) {   // below the split form's resolution
+      w = wn;
       break;
     }
-    const cplx Sn = (d[2] - d[0]) / (2.0 * h);
-    if (!(std::abs(Sn) > 0.0) || !std::isfinite(std::abs(Sn))) break;
-    S = Sn;
-    haveS = true;
-    const cplx wn = clamp(w - d[1] / S);
-    const double step = std::abs(wn - w);
+    cplx fn;
+    if ((r = det(&wn, 1, KLS_MODE_MIXED, &fn))) return r;
+    hist(wn, std::abs(fn));
+    if (!(std::abs(fn) < std::abs(f))) break;      // noise floor (or a bad slope): stop here
+    const cplx Sn = (fn - f) / (wn - w);
     w = wn;
-    if (step < hc->mixed_step_tol) break;
+    f = fn;
+    if (usable(Sn)) S = Sn;
   }
-  // ---- phase 2: FP64 determinants, one per step: a chord step with the
-  //      split form's slope, then secant slopes from the FP64 values; an FP64
-  //      forward-difference slope (step nc->delta) when a step does not lower
-  //      |det|
-  bool converged = false;
-  cplx dw;
-  if ((r = det(&w, 1, KLS_MODE_FP64, &dw))) return r;
-  hist(w, std::abs(dw));
-  for (int it = 0; it < hc->fp64_max_iter && !(std::abs(dw) < tol); ++it) {
-    if (!haveS) {
+  // ---- phase 2: FP64 anchor, then anchored determinants
+  cplx wa = w, fa;
+  {
+    double d2[2];
+    if ((r = kls_set_anchor(c, w.real(), w.imag(), d2))) return r;
+    ++n_fp64;
+    fa = cplx(d2[0], d2[1]);
+  }
+  f = fa;
+  hist(w, std::abs(f));
+  // a determinant of FP64 accuracy at wn: anchored near the anchor, else a
+  // new anchor there
+  auto eval2 = [&](cplx wn, cplx* out) -> int {
+    if (std::abs(wn - wa) > hc->anchor_radius) {
+      double d2[2];
+      int q = kls_set_anchor(c, wn.real(), wn.imag(), d2);
+      if (q) return q;
+      ++n_fp64;
+      wa = wn;
+      *out = cplx(d2[0], d2[1]);
+      return KLS_OK;
+    }
+    return det(&wn, 1, KLS_MODE_ANCHORED, out);
+  };
+  bool converged = false, fresh = false;
+  for (int it = 0; it < hc->fp64_max_iter; ++it) {
+    if (!haveS) {                                  // forward-difference slope at w
       const cplx wd = w + m * nc->delta;
-      cplx dd;
-      if ((r = det(&wd, 1, KLS_MODE_FP64, &dd))) return r;
-      S = (dd - dw) / (m * nc->delta);
-      haveS = true;
+      cplx fd;
+      if ((r = eval2(wd, &fd))) return r;
+      S = (fd - f) / (m * nc->delta);
+      haveS = fresh = true;
     }
-    if (!(std::abs(S) > 0.0)) {
-      res->Omega_p = w.real() / m; res->gamma = w.imag(); res->iterations = it_total;
-      res->det_evals = n_mixed + n_fp64;
-      return kls_fail(c, KLS_ERR_SINGULAR, "singular Jacobian in the FP64 phase");
+    if (!usable(S)) {
+      finish(w, f, false);
+      return kls_fail(c, KLS_ERR_SINGULAR, "singular Jacobian in the FP64-anchored phase");
     }
-    const cplx wn = clamp(w - dw / S);
-    cplx dn;
-    if ((r = det(&wn, 1, KLS_MODE_FP64, &dn))) return r;
-    hist(wn, std::abs(dn));
-    if (std::abs(dn) < std::abs(dw)) {
-      if (wn != w) S = (dn - dw) / (wn - w);      // secant slope
+    const cplx wn = clamp(w - f / S);
+    if (std::abs(f) < tol && std::abs(wn - w) <= 1e-11) { converged = true; break; }
+    if (wn == w) break;                            // clamped in place
+    cplx fn;
+    if ((r = eval2(wn, &fn))) return r;
+    hist(wn, std::abs(fn));
+    if (std::abs(fn) < std::abs(f)) {
+      const cplx Sn = (fn - f) / (wn - w);         // secant slope
       w = wn;
-      dw = dn;
-    } else {
-      haveS = false;                              // FP64 slope at w next
+      f = fn;
+      if (usable(Sn)) S = Sn;
+      fresh = false;
+      continue;
     }
+    if (std::abs(f) < tol) { converged = true; break; }   // |det| stopped falling below tol
+    if (fresh) break;                              // a fresh slope did not help either
+    haveS = false;
   }
-  if (std::abs(dw) < tol) {
-    converged = true;
-    // |det| < tol fixes the root only to tol / |det'|; a secant iteration
-    // stops just below tol.  One more step when the predicted correction is
-    // not negligible (> 1e-11), kept if it lowers |det|.
-    if (haveS && std::abs(S) > 0.0 && std::abs(dw / S) > 1e-11) {
-      const cplx wn = clamp(w - dw / S);
-      cplx dn;
-      if ((r = det(&wn, 1, KLS_MODE_FP64, &dn))) return r;
-      if (std::abs(dn) < std::abs(dw)) {
-        w = wn;
-        dw = dn;
-      }
-    }
+  if (hc->final_fp64) {
+    if ((r = det(&w, 1, KLS_MODE_FP64, &f))) return r;
+    converged = std::abs(f) < tol;
   }
-  res->Omega_p = w.real() / m; res->gamma = w.imag();
-  res->omega_re = w.real(); res->omega_im = w.imag();
-  res->det_re = dw.real(); res->det_im = dw.imag();
-  res->iterations = it_total;
-  res->converged = converged ? 1 : 0;
-  res->det_evals = n_mixed + n_fp64;
-  if (evals) { evals[0] = n_mixed; evals[1] = n_fp64; }
+  finish(w, f, converged);
   return KLS_OK;
 }
 

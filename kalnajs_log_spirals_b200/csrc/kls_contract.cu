@@ -58,23 +58,39 @@ __device__ __forceinline__ double2 real_over_complex(double a, double c, double 
   return make_double2(a * p, a * q);
 }
 
+__device__ __forceinline__ double2 weight_at(double g, double ok, double wr, double wi) {
+  double dr = wr - ok, di = wi;
+  if (hypot(dr, di) < 1e-12) { dr = 1e-12; di = 1e-12; }
+  return real_over_complex(g, dr, di);
+}
+
 __device__ __forceinline__ void weights_body(int64_t K_pad, double wr, double wi,
                                              const double* __restrict__ Gk,
                                              const double* __restrict__ Ok,
                                              double2* __restrict__ out) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K_pad;
-       k += (int64_t)gridDim.x * blockDim.x) {
-    double dr = wr - Ok[k], di = wi;
-    if (hypot(dr, di) < 1e-12) { dr = 1e-12; di = 1e-12; }
-    out[k] = real_over_complex(Gk[k], dr, di);
-  }
+       k += (int64_t)gridDim.x * blockDim.x)
+    out[k] = weight_at(Gk[k], Ok[k], wr, wi);
 }
 
+// anchored: w_k(omega) - w_k(omega_a), each with the denominator clamp; the
+// FP64 difference loses ~|w| / |dw| ulps, far below the FP32 rounding the
+// split-BF16 contraction applies next
 __global__ void weights_kernel(int64_t K_pad, const double* __restrict__ omega,
                                const double* __restrict__ Gk, const double* __restrict__ Ok,
-                               double2* __restrict__ wt) {
+                               double2* __restrict__ wt, int anchored, double ar, double ai) {
   const int z = blockIdx.y;
-  weights_body(K_pad, omega[2 * z], omega[2 * z + 1], Gk, Ok, wt + (size_t)z * K_pad);
+  const double wr = omega[2 * z], wi = omega[2 * z + 1];
+  double2* out = wt + (size_t)z * K_pad;
+  if (!anchored) {
+    weights_body(K_pad, wr, wi, Gk, Ok, out);
+    return;
+  }
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K_pad;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const double2 a = weight_at(Gk[k], Ok[k], wr, wi), b = weight_at(Gk[k], Ok[k], ar, ai);
+    out[k] = make_double2(a.x - b.x, a.y - b.y);
+  }
 }
 
 // one (model, omega) pair per grid row
@@ -332,10 +348,11 @@ int kls_choose_splits(const kls_ctx* c) {
   return best;
 }
 
-int kls_run_weights(kls_ctx* c, int n) {
+int kls_run_weights(kls_ctx* c, int n, const double* anchor) {
   int blocks = (int)std::min<int64_t>((c->K_pad + 255) / 256, 2048);
-  weights_kernel<<<dim3(blocks, n), 256, 0, c->stream>>>(c->K_pad, c->d_omega, c->d_Gk, c->d_Ok,
-                                                         c->d_wt);
+  weights_kernel<<<dim3(blocks, n), 256, 0, c->stream>>>(
+      c->K_pad, c->d_omega, c->d_Gk, c->d_Ok, c->d_wt, anchor ? 1 : 0, anchor ? anchor[0] : 0.0,
+      anchor ? anchor[1] : 0.0);
   KLS_LAUNCHED(c);
   return KLS_OK;
 }

@@ -42,7 +42,7 @@ struct kls_mdesc {
   int64_t K_pad, k_per_split;
   int Na, Na_pad, splits, model;
   // mixed form
-  const void* Xh;             // [2 Na_pad][K_pad] BF16 hi / lo
+  const void* Xh;             // BF16 hi / lo, 2 Na_pad rows in 64-k blocks
   const void* Xl;
   const void* tmap_h;         // device copies of the TMA descriptors (64-byte aligned)
   const void* tmap_l;
@@ -111,6 +111,10 @@ struct kls_ctx {
   double2* d_part = nullptr;  // [ws_omega][splits][Na_pad][Na_pad]
   double2* d_A = nullptr;     // [ws_omega][Na][Na]  I - M (row-major), overwritten by LU
   double2* d_M = nullptr;     // [Na][Na] optional M export (row-major beta, alpha)
+  // KLS_MODE_ANCHORED: FP64 M at the anchor omega (row-major beta, alpha)
+  double2* d_anchorM = nullptr;
+  bool anchor_set = false;
+  double anchor_w[2] = {0.0, 0.0};
   double2* d_det = nullptr;   // [ws_omega]
   double* d_logabs = nullptr; // [ws_omega]
   double* h_pinned = nullptr; // pinned staging for omegas/dets
@@ -171,7 +175,7 @@ __host__ __device__ inline double kls_lin(double a, double b, int n, int i) {
 int kls_run_orbits(kls_ctx* c);
 int kls_upload_alpha(kls_ctx* c);
 int kls_run_basis(kls_ctx* c);
-int kls_run_weights(kls_ctx* c, int n);
+int kls_run_weights(kls_ctx* c, int n, const double* anchor = nullptr);
 int kls_run_contract_f64(kls_ctx* c, int n, int splits);
 int kls_run_reduce(kls_ctx* c, int n, int splits, bool export_M);
 int kls_run_lu(kls_ctx* c, int n);
@@ -179,7 +183,7 @@ int kls_choose_splits(const kls_ctx* c);
 // mixed-precision path (kls_mixed.cu)
 int kls_mixed_prepare(kls_ctx* c);
 int kls_mixed_contract(kls_ctx* c, int n, int splits);
-int kls_mixed_reduce(kls_ctx* c, int n, bool export_M);
+int kls_mixed_reduce(kls_ctx* c, int n, bool export_M, const double2* Ma = nullptr);
 int kls_mixed_check(kls_ctx* c);     // pipeline timeout flag of the last launches
 void kls_mixed_free(kls_ctx* c);
 // uneven batch over models (kls_multi.cu drives these)
@@ -218,7 +222,7 @@ void kls_tm_set_chunk(kls_mixed_tm* t, int stages);
 int kls_mixed_set_chunk(kls_ctx* c, int stages);
 int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned long long wait_ns,
                     int fault_skip);
-int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M);
+int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M, const double2* Ma);
 // the context's TMEM-operand state when that is its split-BF16 form (else null)
 kls_mixed_tm* kls_mixed_tm_state(const kls_ctx* c, unsigned long long* wait_ns);
 void kls_tm_describe(const kls_ctx* c, const kls_mixed_tm* t, unsigned long long wait_ns,

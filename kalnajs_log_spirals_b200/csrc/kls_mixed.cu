@@ -745,7 +745,8 @@ __device__ __forceinline__ void mixed_reduce_body(int Na, int Npad, int splits, 
                                                   const double* __restrict__ Nk,
                                                   const double* __restrict__ part,
                                                   double2* __restrict__ A,
-                                                  double2* __restrict__ Mout) {
+                                                  double2* __restrict__ Mout,
+                                                  const double2* __restrict__ Ma) {
   const size_t R = 2 * (size_t)Npad;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
     const int b = e % Na, a = e / Na;          // consecutive threads: consecutive rows b
@@ -761,7 +762,12 @@ __device__ __forceinline__ void mixed_reduce_body(int Na, int Npad, int splits, 
     }
     const double n = Nk[a];
     // unfused products: 1 - Mr must not become an FMA in one kernel only
-    const double Mr = __dmul_rn(__dmul_rn(mr, G), n), Mi = __dmul_rn(__dmul_rn(mi, G), n);
+    double Mr = __dmul_rn(__dmul_rn(mr, G), n), Mi = __dmul_rn(__dmul_rn(mi, G), n);
+    if (Ma) {                                  // anchored: M(omega_a) + delta M
+      const double2 v = Ma[(size_t)b * Na + a];
+      Mr = __dadd_rn(v.x, Mr);
+      Mi = __dadd_rn(v.y, Mi);
+    }
     A[(size_t)b * Na + a] = make_double2((a == b ? 1.0 : 0.0) - Mr, -Mi);
     if (Mout) Mout[(size_t)b * Na + a] = make_double2(Mr, Mi);
   }
@@ -769,11 +775,12 @@ __device__ __forceinline__ void mixed_reduce_body(int Na, int Npad, int splits, 
 
 __global__ void mixed_reduce_kernel(int Na, int Npad, int splits, double G,
                                     const double* __restrict__ Nk, const double* __restrict__ part,
-                                    double2* __restrict__ A, double2* __restrict__ Mout) {
+                                    double2* __restrict__ A, double2* __restrict__ Mout,
+                                    const double2* __restrict__ Ma) {
   const int z = blockIdx.y;
   const size_t R = 2 * (size_t)Npad;
   mixed_reduce_body(Na, Npad, splits, G, Nk, part + (size_t)z * splits * R * R,
-                    A + (size_t)z * Na * Na, z == 0 ? Mout : nullptr);
+                    A + (size_t)z * Na * Na, z == 0 ? Mout : nullptr, Ma);
 }
 
 // ---- uneven batch over models -------------------------------------------------
@@ -799,7 +806,7 @@ __global__ void multi_mixed_reduce_kernel(const kls_mdesc* __restrict__ md,
   const size_t R = 2 * (size_t)d.Na_pad;
   mixed_reduce_body(d.Na, d.Na_pad, d.msplits, d.G, d.Nk,
                     d.mpart + (size_t)pz.y * d.msplits * R * R, d.A + (size_t)pz.y * d.Na * d.Na,
-                    nullptr);
+                    nullptr, nullptr);
 }
 
 
@@ -1289,12 +1296,13 @@ int kls_mixed_contract(kls_ctx* c, int n, int) {
   return KLS_OK;
 }
 
-int kls_mixed_reduce(kls_ctx* c, int n, bool export_M) {
+int kls_mixed_reduce(kls_ctx* c, int n, bool export_M, const double2* Ma) {
   kls_mixed* m = c->mixed;
-  if (m->form == KLS_MIXED_TMEM) return kls_tm_reduce(c, m->tm, n, export_M);
+  if (m->form == KLS_MIXED_TMEM) return kls_tm_reduce(c, m->tm, n, export_M, Ma);
   int blocks = std::min((c->Na * c->Na + 255) / 256, 1024);
   mixed_reduce_kernel<<<dim3(blocks, n), 256, 0, c->stream>>>(
-      c->Na, c->Na_pad, m->splits, c->cfg.G, c->d_N, m->part, c->d_A, export_M ? c->d_M : nullptr);
+      c->Na, c->Na_pad, m->splits, c->cfg.G, c->d_N, m->part, c->d_A, export_M ? c->d_M : nullptr,
+      Ma);
   KLS_LAUNCHED(c);
   return KLS_OK;
 }

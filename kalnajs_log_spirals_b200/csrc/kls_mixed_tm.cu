@@ -451,7 +451,8 @@ __global__ void tm_weights32_kernel(int64_t total, const double2* __restrict__ w
 // split sum, * G * N(a), I - M: partial [tile][split][b][2 a_local + (0 r | 1 i)]
 __global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, double G,
                                  const double* __restrict__ Nk, const double* __restrict__ part,
-                                 double2* __restrict__ A, double2* __restrict__ Mout) {
+                                 double2* __restrict__ A, double2* __restrict__ Mout,
+                                 const double2* __restrict__ Ma) {
   const int z = blockIdx.y;
   const size_t plane = (size_t)Npad * 128;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
@@ -464,7 +465,11 @@ __global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, doub
       si += src[(size_t)s * plane + 1];
     }
     const double n = Nk[a];
-    const double mr = __dmul_rn(__dmul_rn(sr, G), n), mi = __dmul_rn(__dmul_rn(si, G), n);
+    double mr = __dmul_rn(__dmul_rn(sr, G), n), mi = __dmul_rn(__dmul_rn(si, G), n);
+    if (Ma) {                                  // anchored: M(omega_a) + delta M
+      mr = __dadd_rn(Ma[e].x, mr);
+      mi = __dadd_rn(Ma[e].y, mi);
+    }
     A[(size_t)z * Na * Na + e] = make_double2((a == b ? 1.0 : 0.0) - mr, -mi);
     if (Mout && z == 0) Mout[e] = make_double2(mr, mi);
   }
@@ -659,14 +664,14 @@ int kls_tm_multi_launch(cudaStream_t st, const kls_mdesc* d_md, const kls_tm_mod
   return (int)cudaGetLastError();
 }
 
-int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M) {
+int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M, const double2* Ma) {
   const int nkb_total = (int)(c->K_pad / TM_KB);
   const int kbs = (nkb_total + t->splits - 1) / t->splits;
   const int splits = (nkb_total + kbs - 1) / kbs;
   int blocks = std::min((c->Na * c->Na + 255) / 256, 1024);
   tm_reduce_kernel<<<dim3(blocks, n), 256, 0, c->stream>>>(
       c->Na, c->Na_pad, c->Na_pad / TM_AB, splits, c->cfg.G, c->d_N, t->part, c->d_A,
-      export_M ? c->d_M : nullptr);
+      export_M ? c->d_M : nullptr, Ma);
   KLS_LAUNCHED(c);
   return KLS_OK;
 }

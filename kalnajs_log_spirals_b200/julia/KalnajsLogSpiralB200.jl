@@ -12,6 +12,7 @@ const LIBKLS = get(ENV, "LIBKLS", joinpath(@__DIR__, "..", "libkls.so"))
 
 const KLS_MODE_FP64 = Int32(0)
 const KLS_MODE_MIXED = Int32(1)
+const KLS_MODE_ANCHORED = Int32(2)
 
 # kls_config (include/kls.h), field order and C types
 struct KlsConfig
@@ -160,6 +161,7 @@ end
 
 struct KlsHybridCfg
     mixed_delta::Float64; mixed_step_tol::Float64; mixed_max_iter::Int32; fp64_max_iter::Int32
+    anchor_radius::Float64; final_fp64::Int32
 end
 
 struct KlsTuneResult
@@ -168,21 +170,24 @@ struct KlsTuneResult
 end
 
 """
-newton_search_hybrid: split-BF16 Newton, then FP64 chord steps to the
-reference's stopping rule |det| < tol on the plain FP64 determinant
-(kls_newton_hybrid).  Keyword defaults are the library's recommended ones.
+newton_search_hybrid: split-BF16 secant steps, then an FP64 anchor and
+anchored steps to the reference's stopping rule |det| < tol on an
+FP64-accurate determinant (kls_newton_hybrid).  Keyword defaults are the
+library's recommended ones.
 """
 function newton_search_hybrid(config, precomp::PrecomputedData, Omega_p_init::Real,
                               gamma_init::Real; mixed_delta::Real=1e-3,
-                              mixed_step_tol::Real=1e-7, mixed_max_iter::Integer=30,
-                              fp64_max_iter::Integer=50)
+                              mixed_step_tol::Real=1e-5, mixed_max_iter::Integer=30,
+                              fp64_max_iter::Integer=50, anchor_radius::Real=1e-5,
+                              final_fp64::Bool=false)
     n = config.newton
     check(precomp.handle, ccall((:kls_prepare_mixed, LIBKLS), Cint, (Ptr{Cvoid},), precomp.handle))
     nc = Ref(KlsNewtonCfg(n.max_iter, n.tol, n.delta, n.use_line_search, n.max_line_search,
                           KLS_MODE_FP64))
-    hc = Ref(KlsHybridCfg(mixed_delta, mixed_step_tol, mixed_max_iter, fp64_max_iter))
+    hc = Ref(KlsHybridCfg(mixed_delta, mixed_step_tol, mixed_max_iter, fp64_max_iter,
+                          anchor_radius, Int32(final_fp64)))
     res = Ref(KlsNewtonResult())
-    evals = zeros(Int32, 2)
+    evals = zeros(Int32, 3)
     hist = zeros(Float64, 3, n.max_iter)
     check(precomp.handle, ccall((:kls_newton_hybrid, LIBKLS), Cint,
           (Ptr{Cvoid}, Cdouble, Cdouble, Ref{KlsNewtonCfg}, Ref{KlsHybridCfg},

@@ -10,8 +10,9 @@ Tolerances, FP64 (as in tests/test_gpu_parity.py): per element
 under a 2-ulp perturbation of ln along the orbit integrals (stored in the
 fixture); Newton roots 1e-10 absolute plus the oracle root's own 2-ulp shift.
 Split-BF16: the relative det error against the oracle on the seeded accuracy
-points stays below 1e-3, and the hybrid Newton (split-BF16 phase + FP64
-finish) lands within 1e-10 of the oracle's root.
+points stays below 1e-3, and the hybrid Newton (split-BF16 phase, FP64
+anchor, anchored finish) lands within 1e-10 of the oracle's root, where the
+plain FP64 determinant is below tol as well.
 """
 import os
 
@@ -84,6 +85,9 @@ def test_mixed_against_oracle(default_model, ref):
     print(f"split-BF16 det error vs oracle: median {np.median(rel):.2e}, max {rel.max():.2e}")
     assert rel.max() < 1e-3, rel
     rh = newton_search_hybrid(cfg, pc)
-    assert rh.converged
+    d64 = K.compute_determinant(rh.omega, pc, None)
+    print(f"hybrid: {rh.mixed_evals} split-BF16, {rh.fp64_evals} FP64, {rh.anchored_evals} "
+          f"anchored determinants; |det| {abs(rh.det_val):.2e}, plain FP64 there {abs(d64):.2e}")
+    assert rh.converged and abs(d64) < cfg.newton.tol
     assert abs(rh.Omega_p - ref["root"][0]) <= 1e-10 and abs(rh.gamma - ref["root"][1]) <= 1e-10, \
         (rh.Omega_p - ref["root"][0], rh.gamma - ref["root"][1])
