@@ -86,6 +86,12 @@ __global__ void weights_kernel(int64_t K_pad, const double* __restrict__ omega,
     weights_body(K_pad, wr, wi, Gk, Ok, out);
     return;
   }
+  if (wr == ar && wi == ai) {                // at the anchor dM is exactly zero
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K_pad;
+         k += (int64_t)gridDim.x * blockDim.x)
+      out[k] = make_double2(0.0, 0.0);
+    return;
+  }
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K_pad;
        k += (int64_t)gridDim.x * blockDim.x) {
     const double2 a = weight_at(Gk[k], Ok[k], wr, wi), b = weight_at(Gk[k], Ok[k], ar, ai);

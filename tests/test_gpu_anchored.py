@@ -43,7 +43,10 @@ def pc(lib_path):
 def test_anchor_is_bitwise_fp64(pc):
     d_a = K.set_anchor(pc, W_A)
     d64 = K.compute_determinant(W_A, pc, None)
+    M64 = K.build_M_matrix(W_A, pc, None)
+    Man = K.build_M_matrix(W_A, pc, dev(pc, K.KLS_MODE_ANCHORED))
     d_an = K.compute_determinant(W_A, pc, dev(pc, K.KLS_MODE_ANCHORED))
+    assert np.array_equal(Man, M64), relmax(Man, M64)
     assert d_a == d64 and d_an == d64
 
 
