@@ -12,6 +12,8 @@
 // multiple of KLS_TILE so that alpha tiles never need masking.
 constexpr int KLS_TILE = 64;
 constexpr int KLS_KROW_ALIGN = 64;   // K rows padded to a multiple of this
+// TMEM-operand split-BF16 form: FP32 weight variants per k pair (float4 each)
+constexpr int KLS_TM_WVAR = 3;
 
 // Per-orbit scalar fields written by the orbit kernel (struct of arrays,
 // each NPh doubles, orbit index p = iR + NR*ie as in the reference).
@@ -56,7 +58,7 @@ struct kls_mdesc {
 // batch's buffers.
 struct alignas(64) kls_tm_model {
   CUtensorMap tb_h, tb_l, ty_h, ty_l;
-  const float2* wt32;          // [batch][K_pad] FP32 weights
+  const float2* wt32;          // [batch][K_pad / 2][KLS_TM_WVAR] float4 weight variants
   double* part;                // [batch * tiles_a][splits][Npad][128] FP64 partials
   int64_t K_pad;
   unsigned long long wait_ns;

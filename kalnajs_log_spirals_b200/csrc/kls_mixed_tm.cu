@@ -30,12 +30,15 @@
 //   0       TMA: both B half tiles (completing on the leader's barrier) and
 //           this CTA's A-source tiles (its 64 alphas)
 //   1       MMA issuer (leader CTA, one thread)
-//   2       TMEM allocation / release (512 columns: D at [0, Npad), two A
-//           stages at [384, 512))
-//   3       weights ring: bulk copies of the FP32 w(omega) of the CTA's omega
-//   4..11   producers, 2 per TMEM lane quadrant (Re / Im coefficient halves)
+//   2       TMEM allocation / release (512 columns: D at [0, Npad), A stages
+//           of 64 columns at the top: three for Npad <= 320, else two)
+//   3       weights ring: bulk copies of the FP32 w(omega) of the CTA's omega,
+//           three pre-signed coefficient pairs per two k
+//   4..11   producers, 2 per TMEM lane quadrant (Re / Im coefficient halves);
+//           lanes 0..63 hold rows (a, r), lanes 64..127 rows (a, i), so each
+//           warp's formula is uniform, evaluated in packed f32x2 arithmetic
 //   12..19  drain, 2 per lane quadrant (halves of the D columns): TMEM ->
-//           FP64 partial
+//           FP64 partial (stores for the first chunk, L2 reductions after)
 // Every wait is bounded (the context's wait limit, 2 s by default); a wait
 // that runs out records a code in the error flag (KLS_ERR_TIMEOUT on the
 // host) and the CTA pair winds down; TMEM is released after all issued MMAs
@@ -50,16 +53,18 @@ using namespace kls_tc;
 constexpr int TM_AB = 64;              // alphas per CTA (128 A rows)
 constexpr int TM_KB = 32;              // complex k per stage
 constexpr int TM_STAGES = 3;           // shared-memory stages (B halves + A sources)
-constexpr int TM_ASTAGES = 2;          // TMEM stages of A
+constexpr int TM_ASTAGES_MAX = 3;      // TMEM stages of A (3 when Npad <= 320, else 2)
 constexpr int TM_WSTAGES = 8;          // weights ring
 constexpr int TM_CHUNK = 128;          // default stages per FP32 accumulation chunk (4096 k)
 constexpr int TM_THREADS = 640;
 constexpr int TM_NPROD = 8;            // producer warps 4..11
 constexpr int TM_NDRAIN = 8;           // drain warps 12..19
-constexpr uint32_t TM_ACOL = 384;      // TMEM column of A stage 0 (64 columns per stage)
 constexpr int TM_TMEM_COLS = 512;
 constexpr int TM_YTILE = TM_AB * TM_KB * 2;   // 4 KB: 64 rows x 64 B
-constexpr int TM_WBYTES = TM_KB * 8;          // float2 weights of one stage
+constexpr int TM_WVAR = KLS_TM_WVAR;          // coefficient variants per k pair
+constexpr int TM_WBYTES = TM_KB / 2 * TM_WVAR * 16;   // 768 B: weights of one stage
+
+__host__ __device__ constexpr int tm_astages(int Npad) { return Npad <= 320 ? 3 : 2; }
 
 __host__ __device__ constexpr int tm_btile(int Npad) { return (Npad / 2) * TM_KB * 2; }
 __host__ __device__ constexpr int tm_stage_bytes(int Npad) {
@@ -97,7 +102,7 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_b_full[TM_STAGES], bar_b_empty[TM_STAGES],
       bar_y_full[TM_STAGES], bar_y_empty[TM_STAGES], bar_w_full[TM_WSTAGES],
-      bar_w_empty[TM_WSTAGES], bar_a_full[TM_ASTAGES], bar_a_empty[TM_ASTAGES], bar_acc_full,
+      bar_w_empty[TM_WSTAGES], bar_a_full[TM_ASTAGES_MAX], bar_a_empty[TM_ASTAGES_MAX], bar_acc_full,
       bar_acc_empty, bar_done;
   __shared__ uint32_t s_tmem;
   __shared__ volatile int s_abort;
@@ -118,6 +123,8 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
   const int nch = (nkb + CH - 1) / CH;
   const int Nh2 = P.Npad / 2;                // table rows per CTA
   const int nmma = P.Npad > 256 ? 2 : 1;     // MMAs along N
+  const int NA = tm_astages(P.Npad);         // TMEM stages of A
+  const uint32_t acol = (uint32_t)(TM_TMEM_COLS - 64 * NA);
   const int Nh = P.Npad / nmma;              // N of each MMA
   const int SB = tm_stage_bytes(P.Npad), BT = tm_btile(P.Npad);
   const unsigned long long lim = P.wait_ns;
@@ -143,7 +150,7 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
       mbar_init(smem_u32(&bar_w_full[s]), 1);
       mbar_init(smem_u32(&bar_w_empty[s]), TM_NPROD);
     }
-    for (int s = 0; s < TM_ASTAGES; ++s) {
+    for (int s = 0; s < NA; ++s) {
       mbar_init(smem_u32(&bar_a_full[s]), 2 * TM_NPROD);
       mbar_init(smem_u32(&bar_a_empty[s]), 1);
     }
@@ -204,13 +211,15 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
     // ---------------- weights ring
     if (lane == 0 && nkb > 0) {
       int issued = 0;
-      const float2* wz = wt32 + (size_t)om * P.K_pad;
+      // weights of omega om: TM_WVAR float2 per k (the pre-signed variants)
+      const float2* wz = wt32 + (size_t)om * P.K_pad * TM_WVAR;
       for (int i = 0; i < nkb; ++i) {
         const int ws = i % TM_WSTAGES, r = i / TM_WSTAGES;
         if (!mbar_wait_lim(smem_u32(&bar_w_empty[ws]), (r & 1) ^ 1, &s_abort, err, 10, lim)) break;
         const uint32_t wb = smem_u32(&bar_w_full[ws]);
         mbar_arrive_tx(wb, TM_WBYTES);
-        bulk_load(smem_u32(wring + ws * TM_WBYTES), wz + (size_t)(kb0 + i) * TM_KB, TM_WBYTES, wb);
+        bulk_load(smem_u32(wring + ws * TM_WBYTES), wz + (size_t)(kb0 + i) * TM_KB * TM_WVAR,
+                  TM_WBYTES, wb);
         issued = i + 1;
       }
       for (int i = max(0, issued - TM_WSTAGES); i < issued; ++i)
@@ -222,7 +231,7 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
     if (leader && lane == 0 && nkb > 0) {
       const uint32_t idesc = idesc_bf16(256, Nh);
       for (int i = 0; i < nkb; ++i) {
-        const int s = i % TM_STAGES, as = i % TM_ASTAGES;
+        const int s = i % TM_STAGES, as = i % NA;
         const int ci = i % CH, ch = i / CH;
         const bool first = ci == 0;
         const bool last = ci == CH - 1 || i == nkb - 1;
@@ -231,15 +240,14 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
           break;
         if (!mbar_wait_cl_lim(smem_u32(&bar_b_full[s]), (i / TM_STAGES) & 1, &s_abort, err, 2, lim))
           break;
-        if (!mbar_wait_cl_lim(smem_u32(&bar_a_full[as]), (i / TM_ASTAGES) & 1, &s_abort, err, 3,
-                              lim))
+        if (!mbar_wait_cl_lim(smem_u32(&bar_a_full[as]), (i / NA) & 1, &s_abort, err, 3, lim))
           break;
         tc_fence_after();
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
           const int sub = kk >> 1;                       // Re rows, then Im rows
           const uint32_t kb = (uint32_t)(kk & 1) * 32;   // bytes: k 0..15 / 16..31
-          const uint32_t a_hi = tmem + TM_ACOL + (uint32_t)(as * 64 + kk * 8);
+          const uint32_t a_hi = tmem + acol + (uint32_t)(as * 64 + kk * 8);
           const uint32_t a_lo = a_hi + 32;
           for (int nh = 0; nh < nmma; ++nh) {
             const uint32_t d = tmem + (uint32_t)(nh * Nh);
@@ -262,23 +270,25 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
     // ---------------- producers: A rows of this CTA's 64 alphas into TMEM
     const int pw = warp - 4, q = pw & 3, h = pw >> 2;
     const int l = 32 * q + lane;               // TMEM lane = A row
-    const int al = l >> 1, p = l & 1;          // alpha (local), row (a, r) / (a, i)
-    // half 0 (Re W columns): (a, r) <- Re U, (a, i) <- Im U;
-    // half 1 (Im W columns): (a, r) <- -Im U, (a, i) <- Re U
-    const bool use_re = h == p;
-    const float sgn = (h == 1 && p == 0) ? -1.f : 1.f;
-    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16) + TM_ACOL + (uint32_t)(h * 16);
+    const int p = q >> 1, al = l & 63;         // rows (a, r): lanes 0..63, (a, i): 64..127
+    // half 0 (Re W columns): (a, r) <- Re U, (a, i) <- Im U; half 1 (Im W
+    // columns): (a, r) <- -Im U, (a, i) <- Re U; with U = w conj(W) each is
+    // c1 * ReW + c2 * ImW, (c1, c2) = (wr, wi), (wi, -wr) or (-wi, wr): the
+    // weights ring holds the three variants, this warp reads one
+    const int var = h == p ? 0 : (p == 1 ? 1 : 2);
+    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16) + acol + (uint32_t)(h * 16);
     const bool skip_one = P.fault_skip && leader && tile_pair == 0 && split == 0 && pw == 0;
     for (int i = 0; i < nkb; ++i) {
-      const int s = i % TM_STAGES, as = i % TM_ASTAGES, ws = i % TM_WSTAGES;
+      const int s = i % TM_STAGES, as = i % NA, ws = i % TM_WSTAGES;
       bool ok = mbar_wait_lim(smem_u32(&bar_y_full[s]), (i / TM_STAGES) & 1, &s_abort, err, 4, lim);
       if (ok) ok = mbar_wait_lim(smem_u32(&bar_w_full[ws]), (i / TM_WSTAGES) & 1, &s_abort, err, 8,
                                  lim);
-      if (ok) ok = mbar_wait_cl_lim(smem_u32(&bar_a_empty[as]), ((i / TM_ASTAGES) & 1) ^ 1,
-                                    &s_abort, err, 12, lim);
+      if (ok) ok = mbar_wait_cl_lim(smem_u32(&bar_a_empty[as]), ((i / NA) & 1) ^ 1, &s_abort, err,
+                                    12, lim);
       if (!__all_sync(0xffffffffu, ok)) break;
       tc_fence_after();
-      const float4* wz = reinterpret_cast<const float4*>(wring + ws * TM_WBYTES);
+      // (c1 pair, c2 pair) of k = 2j, 2j + 1 at float4 number TM_WVAR j + var
+      const float4* wz = reinterpret_cast<const float4*>(wring + ws * TM_WBYTES) + var;
       uint32_t hi[16], lo[16];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
@@ -291,16 +301,11 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int j = 4 * c + e;               // k = 2j, 2j + 1
-          const uint32_t rh = (&Rh.x)[e], rl = (&Rl.x)[e], ih = (&Ih.x)[e], il = (&Il.x)[e];
-          const float wr0 = bf_lo(rh) + bf_lo(rl), wr1 = bf_hi(rh) + bf_hi(rl);
-          const float wi0 = bf_lo(ih) + bf_lo(il), wi1 = bf_hi(ih) + bf_hi(il);
-          const float4 w = wz[j];                // (w_2j, w_2j+1)
-          // U = w conj(W): Re U = wr Wr + wi Wi, Im U = wi Wr - wr Wi
-          const float v0 = use_re ? __fmaf_rn(w.x, wr0, __fmul_rn(w.y, wi0))
-                                  : __fmaf_rn(w.y, wr0, -__fmul_rn(w.x, wi0));
-          const float v1 = use_re ? __fmaf_rn(w.z, wr1, __fmul_rn(w.w, wi1))
-                                  : __fmaf_rn(w.w, wr1, -__fmul_rn(w.z, wi1));
-          hi[j] = pack_split(sgn * v0, sgn * v1, lo[j]);
+          const uint64_t wr = f2_add(f2_bf16x2((&Rh.x)[e]), f2_bf16x2((&Rl.x)[e]));
+          const uint64_t wi = f2_add(f2_bf16x2((&Ih.x)[e]), f2_bf16x2((&Il.x)[e]));
+          const float4 cw = wz[TM_WVAR * j];
+          const uint64_t v = f2_fma(f2_pack(cw.x, cw.y), wr, f2_mul(f2_pack(cw.z, cw.w), wi));
+          hi[j] = pack_split2(v, lo[j]);
         }
       }
       TMEM_ST16(tl + (uint32_t)(as * 64), hi);
@@ -335,14 +340,18 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
         TMEM_LD16(tl + (uint32_t)j0, v);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (dummy) continue;
-        // the 16 columns map to at most two runs of consecutive table rows
-        double old[16];
+        // first chunk: plain stores; later chunks: FP64 reductions in L2
+        // (fire-and-forget, so the accumulator is free again as soon as it
+        // is read).  Each partial element is written by this one thread, in
+        // chunk order (same-thread, same-address operations are ordered), so
+        // the sums are deterministic: ((c0 + c1) + c2) + ...
 #pragma unroll
-        for (int t = 0; t < 16; ++t)
-          old[t] = ch > 0 ? out[(size_t)tm_brow(j0 + t, Nh, Nh2) * 128] : 0.0;
-#pragma unroll
-        for (int t = 0; t < 16; ++t)
-          out[(size_t)tm_brow(j0 + t, Nh, Nh2) * 128] = old[t] + (double)__uint_as_float(v[t]);
+        for (int t = 0; t < 16; ++t) {
+          double* dst = out + (size_t)tm_brow(j0 + t, Nh, Nh2) * 128;
+          const double x = (double)__uint_as_float(v[t]);
+          if (ch == 0) *dst = x;
+          else asm volatile("red.global.add.f64 [%0], %1;" ::"l"(dst), "d"(x) : "memory");
+        }
       }
       tc_fence_before();
       __syncwarp();
@@ -400,18 +409,28 @@ mixed_tm_multi_kernel(const kls_tm_model* __restrict__ md, const int4* __restric
   tm_body(&d.tb_h, &d.tb_l, &d.ty_h, &d.ty_l, P, it.y, it.z, d.wt32, d.part, err);
 }
 
-// uneven batch: FP32 weights of every (model, omega) pair, plain order
+// FP32 weights as the producers read them: for k = 2j, 2j + 1 three float4
+// (c1 pair, c2 pair) = (wr, wi), (wi, -wr), (-wi, wr); negation is exact, so
+// every variant rounds like the plain FP32 weight
+__device__ __forceinline__ void tm_weight_variants(int64_t K_pad, const double2* __restrict__ wt,
+                                                   float4* __restrict__ out) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < K_pad / 2;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const double2 a = wt[2 * j], b = wt[2 * j + 1];
+    const float r0 = (float)a.x, i0 = (float)a.y, r1 = (float)b.x, i1 = (float)b.y;
+    out[3 * j] = make_float4(r0, r1, i0, i1);
+    out[3 * j + 1] = make_float4(i0, i1, -r0, -r1);
+    out[3 * j + 2] = make_float4(-i0, -i1, r0, r1);
+  }
+}
+
+// uneven batch: FP32 weight variants of every (model, omega) pair
 __global__ void tm_multi_weights32_kernel(const kls_mdesc* __restrict__ md,
                                           const int2* __restrict__ pairs) {
   const int2 pz = pairs[blockIdx.y];
   const kls_mdesc& d = md[pz.x];
-  const double2* wt = d.wt + (size_t)pz.y * d.K_pad;
-  float2* w32 = reinterpret_cast<float2*>(d.wt32) + (size_t)pz.y * d.K_pad;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < d.K_pad;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const double2 v = wt[i];
-    w32[i] = make_float2((float)v.x, (float)v.y);
-  }
+  tm_weight_variants(d.K_pad, d.wt + (size_t)pz.y * d.K_pad,
+                     reinterpret_cast<float4*>(d.wt32) + (size_t)pz.y * (d.K_pad / 2) * TM_WVAR);
 }
 
 // uneven batch: split sum, * G * N(a), I - M per (model, omega) pair; mpart is
@@ -424,13 +443,13 @@ __global__ void tm_multi_reduce_kernel(const kls_mdesc* __restrict__ md,
   const size_t plane = (size_t)d.Na_pad * 128;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
     const int b = e / Na, a = e % Na;
-    const int at = a / TM_AB, l2 = 2 * (a % TM_AB);
+    const int at = a / TM_AB, la = a % TM_AB;    // rows (a, r) at la, (a, i) at 64 + la
     const double* src =
-        d.mpart + (size_t)(pz.y * tiles_a + at) * d.msplits * plane + (size_t)b * 128 + l2;
+        d.mpart + (size_t)(pz.y * tiles_a + at) * d.msplits * plane + (size_t)b * 128 + la;
     double sr = 0.0, si = 0.0;
     for (int s = 0; s < d.msplits; ++s) {
       sr += src[(size_t)s * plane];
-      si += src[(size_t)s * plane + 1];
+      si += src[(size_t)s * plane + TM_AB];
     }
     const double n = d.Nk[a];
     const double mr = __dmul_rn(__dmul_rn(sr, d.G), n), mi = __dmul_rn(__dmul_rn(si, d.G), n);
@@ -438,17 +457,15 @@ __global__ void tm_multi_reduce_kernel(const kls_mdesc* __restrict__ md,
   }
 }
 
-// FP32 copy of the weights, plain [omega][K_pad] order
-__global__ void tm_weights32_kernel(int64_t total, const double2* __restrict__ wt,
-                                    float2* __restrict__ wt32) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const double2 v = wt[i];
-    wt32[i] = make_float2((float)v.x, (float)v.y);
-  }
+// FP32 weight variants, [omega][K_pad / 2][3] float4
+__global__ void tm_weights32_kernel(int64_t K_pad, const double2* __restrict__ wt,
+                                    float4* __restrict__ wt32) {
+  const int z = blockIdx.y;
+  tm_weight_variants(K_pad, wt + (size_t)z * K_pad, wt32 + (size_t)z * (K_pad / 2) * TM_WVAR);
 }
 
-// split sum, * G * N(a), I - M: partial [tile][split][b][2 a_local + (0 r | 1 i)]
+// split sum, * G * N(a), I - M: partial [tile][split][b][A row], A row
+// a_local (Re) or 64 + a_local (Im)
 __global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, double G,
                                  const double* __restrict__ Nk, const double* __restrict__ part,
                                  double2* __restrict__ A, double2* __restrict__ Mout,
@@ -457,12 +474,12 @@ __global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, doub
   const size_t plane = (size_t)Npad * 128;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
     const int b = e / Na, a = e % Na;
-    const int at = a / TM_AB, l2 = 2 * (a % TM_AB);
-    const double* src = part + (size_t)(z * tiles_a + at) * splits * plane + (size_t)b * 128 + l2;
+    const int at = a / TM_AB, la = a % TM_AB;    // rows (a, r) at la, (a, i) at 64 + la
+    const double* src = part + (size_t)(z * tiles_a + at) * splits * plane + (size_t)b * 128 + la;
     double sr = 0.0, si = 0.0;
     for (int s = 0; s < splits; ++s) {
       sr += src[(size_t)s * plane];
-      si += src[(size_t)s * plane + 1];
+      si += src[(size_t)s * plane + TM_AB];
     }
     const double n = Nk[a];
     double mr = __dmul_rn(__dmul_rn(sr, G), n), mi = __dmul_rn(__dmul_rn(si, G), n);
@@ -500,7 +517,7 @@ struct kls_mixed_tm {
   int chunk = TM_CHUNK;         // stages per FP32 accumulation chunk
   double* part = nullptr;       // [n tiles][splits][Npad][128]
   size_t part_elems = 0;
-  float2* wt32 = nullptr;       // [n][K_pad]
+  float2* wt32 = nullptr;       // [n][K_pad / 2][3] float4 weight variants
   size_t wt32_elems = 0;
 };
 
@@ -600,7 +617,7 @@ int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned lon
     KLS_CK(c, cudaMalloc(&t->part, need * sizeof(double)));
     t->part_elems = need;
   }
-  const size_t nw = (size_t)n * c->K_pad;
+  const size_t nw = (size_t)n * c->K_pad * TM_WVAR;      // float2
   if (nw > t->wt32_elems) {
     cudaFree(t->wt32);
     t->wt32 = nullptr;
@@ -608,8 +625,9 @@ int kls_tm_contract(kls_ctx* c, kls_mixed_tm* t, int n, int* d_err, unsigned lon
     KLS_CK(c, cudaMalloc(&t->wt32, nw * sizeof(float2)));
     t->wt32_elems = nw;
   }
-  tm_weights32_kernel<<<(unsigned)std::min<size_t>((nw + 255) / 256, 4096), 256, 0, c->stream>>>(
-      (int64_t)nw, c->d_wt, t->wt32);
+  const unsigned wblocks = (unsigned)std::min<int64_t>((c->K_pad / 2 + 255) / 256, 2048);
+  tm_weights32_kernel<<<dim3(wblocks, n), 256, 0, c->stream>>>(
+      c->K_pad, c->d_wt, reinterpret_cast<float4*>(t->wt32));
   KLS_LAUNCHED(c);
   TmParams P{};
   P.Npad = c->Na_pad;

@@ -436,14 +436,14 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
     } else {
       if (!c->mixed && (r = kls_mixed_prepare(c))) return bail(mfail(m, r, c->err));
       if (m->tm) {
-        // TMEM-operand form: plain FP32 weights and this form's partials
+        // TMEM-operand form: FP32 weight variants and this form's partials
         unsigned long long wns = 0;
         kls_mixed_tm* t = kls_mixed_tm_state(c, &wns);
         kls_tm_model td;
         kls_tm_describe(c, t, wns, batch, &td);
         float2* w32 = nullptr;
         double* mp = nullptr;
-        if ((r = malloc_buf(m, &w32, (size_t)batch * c->K_pad)) ||
+        if ((r = malloc_buf(m, &w32, (size_t)batch * c->K_pad * KLS_TM_WVAR)) ||
             (r = malloc_buf(m, &mp, (size_t)td.n_tiles * td.splits * c->Na_pad * 128)))
           return bail(r);
         td.wt32 = w32;

@@ -200,6 +200,45 @@ __device__ __forceinline__ uint32_t pack_split(float a, float b, uint32_t& lo) {
   lo = *reinterpret_cast<uint32_t*>(&l);
   return *reinterpret_cast<uint32_t*>(&h);
 }
+// packed FP32 pairs (sm_100 f32x2 arithmetic): the low word holds the first
+// element; each lane computes exactly what two scalar operations would
+__device__ __forceinline__ uint64_t f2_pack(float a, float b) {
+  return ((uint64_t)__float_as_uint(b) << 32) | __float_as_uint(a);
+}
+__device__ __forceinline__ uint64_t f2_bf16x2(uint32_t v) {   // (bf_lo(v), bf_hi(v))
+  return ((uint64_t)(v & 0xffff0000u) << 32) | (uint32_t)(v << 16);
+}
+__device__ __forceinline__ uint64_t f2_add(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+// pack_split of a packed pair: the same bits as pack_split(lo word, hi word)
+__device__ __forceinline__ uint32_t pack_split2(uint64_t v, uint32_t& lo) {
+  uint32_t h, l;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(h)
+      : "f"(__uint_as_float((uint32_t)(v >> 32))), "f"(__uint_as_float((uint32_t)v)));
+  const uint64_t r = f2_sub(v, f2_bf16x2(h));          // exact residuals
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(l)
+      : "f"(__uint_as_float((uint32_t)(r >> 32))), "f"(__uint_as_float((uint32_t)r)));
+  lo = l;
+  return h;
+}
 // byte offset of the 16-byte chunk (row n, k-chunk c) in a K-major SW128 tile
 __device__ __forceinline__ uint32_t sw128_off(int n, int c) {
   return (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4));
