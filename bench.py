@@ -848,6 +848,10 @@ def ours(args):
     value = world * nb * args.steps / (ms * 1e-3)
     stage = stage_times(_lib.KLS_MODE_FP64)
     achieved = nb * flops_per_det / (stage[1] * 1e-3) / 1e12
+    # real DMMA flops the kernel issues (padded tiles): 4 or 3 real products
+    f64_3m = tunes["fp64"].form == _lib.KLS_F64_3M
+    issued_per_det = (6.0 if f64_3m else 8.0) * dims.N_alpha_pad ** 2 * dims.K_pad
+    issued = nb * issued_per_det / (stage[1] * 1e-3) / 1e12
 
     # ---- end to end through the C ABI with host buffers -----------------------
     h_om = np.ascontiguousarray(all_om)
@@ -1018,7 +1022,7 @@ def ours(args):
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    traffic, traffic_scaled = read_traffic("contract_kernel")
+    traffic, traffic_scaled = read_traffic("contract3m_kernel" if f64_3m else "contract_kernel")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
@@ -1031,11 +1035,18 @@ def ours(args):
                    "K": dims.K, "omegas_per_step": nb, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (W table %.1f GB in HBM)" % (
                        2 * 8 * dims.K_pad * dims.N_alpha_pad / 1e9)},
-        "roofline": {"bound": "tensor", "kernel": "contract_kernel (FP64 DMMA m8n8k4 on the tensor pipe)",
+        "roofline": {"bound": "tensor",
+                     "kernel": ("contract3m_kernel (FP64 DMMA m8n8k4, 3 real products per "
+                                "complex one)" if f64_3m else
+                                "contract_kernel (FP64 DMMA m8n8k4, 4 real products)"),
                      "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                      "frac": achieved / peak64,
                      "peak_note": "of measured: cuBLAS DGEMM 8192^3 best-of-5 in this run",
                      "algorithmic_flops_per_launch": nb * flops_per_det,
+                     "algorithmic_note": "8 N_alpha^2 K per determinant (a complex MAC as 4 "
+                                         "real ones); the 3M form issues 3, so its frac can "
+                                         "exceed the DMMA pipe's",
+                     "dmma_issued_tflops": issued, "dmma_issued_frac": issued / peak64,
                      "traffic": traffic, "traffic_scaled": traffic_scaled, "stage_ms": {"weights": stage[0], "contract": stage[1],
                                                       "reduce": stage[2], "lu": stage[3]}},
         "cpu_baseline": cpu,
@@ -1045,8 +1056,9 @@ def ours(args):
         "gpu_launches": int(launches),
         "clocks": clk,
         "autotune": {k: {"splits": t.splits, "default_splits": t.default_splits,
-                         "form": {0: "fp64", 1: "one CTA", 2: "CTA pair",
-                                  3: "TMEM-operand CTA pair"}.get(t.form, t.form),
+                         "form": ({0: "FP64 4M", 1: "FP64 3M"} if k == "fp64" else
+                                  {1: "one CTA", 2: "CTA pair",
+                                   3: "TMEM-operand CTA pair"}).get(t.form, t.form),
                          "candidates": t.candidates, "ms_per_omega": t.ms_per_omega,
                          "default_ms_per_omega": t.default_ms_per_omega}
                      for k, t in tunes.items()},

@@ -57,6 +57,11 @@ extern "C" {
                                    away: ~1e-11 of max|M|) at the cost of a
                                    KLS_MODE_MIXED evaluation                  */
 
+/* ---- forms of the FP64 contraction (kls_set_f64_form) -------------------- */
+#define KLS_F64_4M           0  /* four real DMMA products per complex one     */
+#define KLS_F64_3M           1  /* three (Gauss): Re = P1 - P2,
+                                   Im = (P3 - P1) - P2 with P3 = (ar+ai)(br+bi) */
+
 /* ---- configuration: the [physics] [model] [grid] TOML sections ---------- *
  * Mirrors PhysicsConfig / ModelConfig / GridConfig
  * (Configuration.jl:31-67).  q1 is real-valued here (the reference types it
@@ -335,12 +340,18 @@ typedef struct kls_tune_result {
     int32_t candidates;           /* candidates timed (0: from the cache)     */
     double  ms_per_omega;         /* contraction time of the choice           */
     double  default_ms_per_omega; /* and of the untuned choice (0: cached)    */
-    int32_t form;                 /* split-BF16 kernel chosen (KLS_MIXED_*)   */
+    int32_t form;                 /* kernel chosen: KLS_MIXED_* for the split
+                                     form, KLS_F64_* for FP64                 */
 } kls_tune_result;
 int kls_autotune(kls_ctx* ctx, int mode, int batch, kls_tune_result* out);
 /* Set the K split count of `mode` by hand (clamped to what the table
  * allows); determinants stay batch-independent for a fixed count.         */
 int kls_set_splits(kls_ctx* ctx, int mode, int splits);
+/* FP64 contraction form (no reference counterpart): KLS_F64_4M (default) or
+ * KLS_F64_3M; the K split count is reset to the form's default.  Both stay
+ * within the FP64 parity tolerances; they differ in the last bits.  An
+ * uneven batch (kls_multi_create) needs every FP64 model in the same form. */
+int kls_set_f64_form(kls_ctx* ctx, int form);
 
 /* ---- determinant stage form (no reference counterpart) -------------------- *
  * KLS_LU_CLUSTER factors each I - M(omega) on one thread-block cluster of 8

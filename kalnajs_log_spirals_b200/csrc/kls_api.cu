@@ -858,11 +858,12 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
   if (mode == KLS_MODE_MIXED && !c->mixed && (r = kls_mixed_prepare(c))) return r;
   const bool mixed = mode == KLS_MODE_MIXED;
   const int def = mixed ? kls_mixed_default_splits(c) : kls_choose_splits(c);
-  const int def_form = mixed ? kls_mixed_form_of(c) : 0;
+  const int def_form = mixed ? kls_mixed_form_of(c) : c->f64_form;
   const int max_s = mixed ? (int)std::max<int64_t>(1, c->K_pad / 64)
                           : (int)std::max<int64_t>(1, c->K_pad / (16 * 8));
   auto apply = [&](int s, int form) -> int {
     if (mixed && (r = kls_mixed_set_form(c, form))) return r;
+    if (!mixed) c->f64_form = form;
     return apply_splits(c, mode, s);
   };
   kls_tune_result res{};
@@ -875,16 +876,17 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
     auto it = g_tune.find(key);
     if (it != g_tune.end()) {
       res.splits = std::min(it->second.first, max_s);
-      res.form = mixed ? (it->second.second ? it->second.second : def_form) : 0;
+      res.form = mixed ? (it->second.second ? it->second.second : def_form) : it->second.second;
       if ((r = apply(res.splits, res.form))) return r;
       if (out) *out = res;
       return KLS_OK;
     }
   }
-  // the split-BF16 form also chooses its kernel: one CTA, a CTA pair, or the
-  // TMEM-operand pair; split candidates around each form's own default
+  // each mode also chooses its kernel: one CTA, a CTA pair or the
+  // TMEM-operand pair (split-BF16), 4 or 3 real products (FP64); split
+  // candidates around each form's own default
   std::vector<int> forms = mixed ? std::vector<int>{KLS_MIXED_ONE_CTA, KLS_MIXED_PAIR}
-                                 : std::vector<int>{0};
+                                 : std::vector<int>{KLS_F64_4M, KLS_F64_3M};
   if (mixed && kls_mixed_set_form(c, KLS_MIXED_TMEM) == KLS_OK) forms.push_back(KLS_MIXED_TMEM);
   if (mixed) kls_mixed_set_form(c, def_form);
   double best_ms = INFINITY;
@@ -894,6 +896,9 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
     if (mixed) {
       if ((r = kls_mixed_set_form(c, form))) return r;
       fdef = kls_mixed_default_splits(c);
+    } else {
+      c->f64_form = form;
+      fdef = kls_choose_splits(c);
     }
     std::vector<int> cand = {std::max(1, fdef / 2), fdef, 2 * fdef, 3 * fdef};
     for (int& s : cand) s = std::max(1, std::min(s, max_s));
@@ -991,6 +996,18 @@ int kls_set_fault_injection(kls_ctx* c, int mode) {
   }
   if (!c->mixed && (r = kls_mixed_prepare(c))) return r;
   return kls_mixed_set_wait(c, 0, mode);
+}
+
+int kls_set_f64_form(kls_ctx* c, int form) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (form != KLS_F64_4M && form != KLS_F64_3M)
+    return kls_fail(c, KLS_ERR_CONFIG, "unknown FP64 contraction form");
+  if (c->f64_form != form) {
+    c->f64_form = form;
+    return apply_splits(c, KLS_MODE_FP64, kls_choose_splits(c));
+  }
+  return KLS_OK;
 }
 
 int kls_set_lu_mode(kls_ctx* c, int mode) {

@@ -246,6 +246,134 @@ contract_kernel(ContractParams P, const double* __restrict__ Wre, const double* 
   contract_tile(P, Wre, Wim, wt, part, smem, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// ---- 3M (Gauss) form: three real products per complex product -------------
+// With A = W_b (ar + i ai) and B = w conj(W_a) (br + i bi):
+//   P1 = ar br, P2 = ai bi, P3 = (ar + ai)(br + bi),
+//   Re = P1 - P2, Im = (P3 - P1) - P2,
+// so each k step takes 3 DMMAs per output fragment instead of 4.  The three
+// accumulators need 1.5x the registers of the 4M form's two, so the 64 x 64
+// tile is split over 8 warps of 32 x 16 (one CTA per SM, the same 8 warps
+// per SM as two 4M CTAs) and the pipeline is 4 stages deep.
+constexpr int CT3_THREADS = 256;
+constexpr int CT3_STAGES = 4;
+constexpr size_t CT3_SMEM = (size_t)CT3_STAGES * CT_STAGE_DOUBLES * sizeof(double);
+
+__device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
+                                                 const double* __restrict__ Wre,
+                                                 const double* __restrict__ Wim,
+                                                 const double2* __restrict__ wt,
+                                                 double2* __restrict__ part, double* smem,
+                                                 int tile, int split, int z) {
+  const int tm = tile / P.tiles_1d, tn = tile % P.tiles_1d;
+  const int b0 = tm * KLS_TILE, a0 = tn * KLS_TILE;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;             // 32 b rows x 16 a columns per warp
+  const int64_t kbeg = (int64_t)split * P.k_per_split;
+  const int64_t kend = min(P.K_pad, kbeg + P.k_per_split);
+  const int nk = kbeg < kend ? (int)((kend - kbeg) / CT_BK) : 0;
+  const double2* wz = wt + (size_t)z * P.K_pad;
+  const size_t ld = (size_t)P.Na_pad;
+
+  auto stage_ptr = [&](int s) { return smem + (size_t)s * CT_STAGE_DOUBLES; };
+  auto load_stage = [&](int s, int kt) {
+    double* st = stage_ptr(s);
+    const int64_t k0 = kbeg + (int64_t)kt * CT_BK;
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+      int cidx = tid + it * CT3_THREADS;       // 0..2047
+      int plane = cidx >> 9;                   // 0: A re, 1: A im, 2: B re, 3: B im
+      int rem = cidx & 511;
+      int row = rem >> 5, col = (rem & 31) * 2;
+      const double* src = (plane & 1) ? Wim : Wre;
+      int c0 = (plane < 2) ? b0 : a0;
+      cp_async16(st + plane * CT_PLANE + row * CT_S + col,
+                 src + (size_t)(k0 + row) * ld + c0 + col);
+    }
+    if (tid < CT_BK) cp_async16(st + 4 * CT_PLANE + 2 * tid, wz + k0 + tid);
+  };
+
+  double p1[4][2][2], p2[4][2][2], p3[4][2][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) p1[i][j][h] = p2[i][j][h] = p3[i][j][h] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < CT3_STAGES - 1; ++s) {
+    if (s < nk) load_stage(s, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<CT3_STAGES - 2>();
+    __syncthreads();
+    int nxt = kt + CT3_STAGES - 1;
+    if (nxt < nk) load_stage(nxt % CT3_STAGES, nxt);
+    cp_async_commit();
+    const double* st = stage_ptr(kt % CT3_STAGES);
+    const double* sAr = st;
+    const double* sAi = st + CT_PLANE;
+    const double* sBr = st + 2 * CT_PLANE;
+    const double* sBi = st + 3 * CT_PLANE;
+    const double* sd = st + 4 * CT_PLANE;
+#pragma unroll
+    for (int kk = 0; kk < CT_BK; kk += 4) {
+      const int kr = kk + (lane & 3);
+      const double dr = sd[2 * kr], di = sd[2 * kr + 1];
+      double ar[4], ai[4], as[4], br[2], bi[2], bs[2];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        int off = kr * CT_S + wm * 32 + i * 8 + (lane >> 2);
+        ar[i] = sAr[off];
+        ai[i] = sAi[off];
+        as[i] = __dadd_rn(ar[i], ai[i]);
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        int off = kr * CT_S + wn * 16 + j * 8 + (lane >> 2);
+        double xr = sBr[off], xi = sBi[off];
+        // the same weighted fragment as the 4M form
+        br[j] = __fma_rn(dr, xr, __dmul_rn(di, xi));
+        bi[j] = __fma_rn(di, xr, -__dmul_rn(dr, xi));
+        bs[j] = __dadd_rn(br[j], bi[j]);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          dmma(p1[i][j][0], p1[i][j][1], ar[i], br[j]);
+          dmma(p2[i][j][0], p2[i][j][1], ai[i], bi[j]);
+          dmma(p3[i][j][0], p3[i][j][1], as[i], bs[j]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  double2* out = part + ((size_t)z * P.splits + split) * ld * ld;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int b = b0 + wm * 32 + i * 8 + (lane >> 2);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      int a = a0 + wn * 16 + j * 8 + 2 * (lane & 3);
+      double2* o = out + (size_t)b * ld + a;
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        o[h] = make_double2(__dsub_rn(p1[i][j][h], p2[i][j][h]),
+                            __dsub_rn(__dsub_rn(p3[i][j][h], p1[i][j][h]), p2[i][j][h]));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(CT3_THREADS, 1)
+contract3m_kernel(ContractParams P, const double* __restrict__ Wre,
+                  const double* __restrict__ Wim, const double2* __restrict__ wt,
+                  double2* __restrict__ part) {
+  extern __shared__ __align__(16) double smem[];
+  contract_tile_3m(P, Wre, Wim, wt, part, smem, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // Persistent form over an uneven batch: every CTA takes work items
 // (model, omega, tile, split) from an atomic counter until the list is
 // exhausted.  The list runs model by model, largest first, tile fastest, so
@@ -273,6 +401,30 @@ multi_contract_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restri
     P.k_per_split = d.k_per_split;
     contract_tile(P, d.Wre, d.Wim, d.wt, d.part, smem, it.tile, it.split, it.z);
     __syncthreads();          // shared stages and s_item are reused by the next item
+  }
+}
+
+// the same persistent loop over the 3M tile
+__global__ void __launch_bounds__(CT3_THREADS, 1)
+multi_contract3m_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict__ items,
+                        int n_items, int* __restrict__ counter) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int i = s_item;
+    if (i >= n_items) break;
+    const kls_item it = items[i];
+    const kls_mdesc& d = md[it.model];
+    ContractParams P;
+    P.Na_pad = d.Na_pad;
+    P.tiles_1d = d.Na_pad / KLS_TILE;
+    P.splits = d.splits;
+    P.K_pad = d.K_pad;
+    P.k_per_split = d.k_per_split;
+    contract_tile_3m(P, d.Wre, d.Wim, d.wt, d.part, smem, it.tile, it.split, it.z);
+    __syncthreads();
   }
 }
 
@@ -326,15 +478,27 @@ __global__ void multi_reduce_kernel(const kls_mdesc* __restrict__ md,
 // table allows, at least 8 slabs per split): then n omegas take n * q nearly
 // full waves for every n.  At N_alpha_pad = 320 (25 tiles) on 296 slots
 // that is 71 splits: 1775 CTAs per omega = 99.9% of 6 waves.
+// CTAs of the FP64 contraction form `form` resident on the device at once
+static int f64_slots(int device, int form, bool persistent) {
+  int sms = 148, per_sm = 1;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const void* fn = form == KLS_F64_3M
+                       ? (persistent ? (const void*)multi_contract3m_kernel
+                                     : (const void*)contract3m_kernel)
+                       : (persistent ? (const void*)multi_contract_kernel
+                                     : (const void*)contract_kernel);
+  const int threads = form == KLS_F64_3M ? CT3_THREADS : CT_THREADS;
+  const size_t smem = form == KLS_F64_3M ? CT3_SMEM : CT_SMEM;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return sms * per_sm;
+}
+
 int kls_choose_splits(const kls_ctx* c) {
   const int tiles = (c->Na_pad / KLS_TILE) * (c->Na_pad / KLS_TILE);
-  int sms = 148, per_sm = 2;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-  cudaFuncSetAttribute(contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CT_SMEM);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, contract_kernel, CT_THREADS,
-                                                    CT_SMEM) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  const int slots = sms * per_sm;
+  const int slots = f64_slots(c->device, c->f64_form, false);
   int64_t max_s = c->K_pad / (CT_BK * 8);            // at least 8 slabs per split
   if (max_s > 512) max_s = 512;
   if (max_s < 1) max_s = 1;
@@ -364,8 +528,6 @@ int kls_run_weights(kls_ctx* c, int n, const double* anchor) {
 }
 
 int kls_run_contract_f64(kls_ctx* c, int n, int splits) {
-  KLS_CK(c, cudaFuncSetAttribute(contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)CT_SMEM));
   ContractParams P{};
   P.Na_pad = c->Na_pad;
   P.tiles_1d = c->Na_pad / KLS_TILE;
@@ -373,6 +535,16 @@ int kls_run_contract_f64(kls_ctx* c, int n, int splits) {
   P.K_pad = c->K_pad;
   P.k_per_split = kls_f64_k_per_split(c->K_pad, splits);
   dim3 grid(P.tiles_1d * P.tiles_1d, splits, n);
+  if (c->f64_form == KLS_F64_3M) {
+    KLS_CK(c, cudaFuncSetAttribute(contract3m_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)CT3_SMEM));
+    contract3m_kernel<<<grid, CT3_THREADS, CT3_SMEM, c->stream>>>(P, c->d_Wre, c->d_Wim,
+                                                                  c->d_wt, c->d_part);
+    KLS_LAUNCHED(c);
+    return KLS_OK;
+  }
+  KLS_CK(c, cudaFuncSetAttribute(contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)CT_SMEM));
   contract_kernel<<<grid, CT_THREADS, CT_SMEM, c->stream>>>(P, c->d_Wre, c->d_Wim, c->d_wt,
                                                             c->d_part);
   KLS_LAUNCHED(c);
@@ -391,16 +563,23 @@ int kls_run_reduce(kls_ctx* c, int n, int splits, bool export_M) {
 // ---- uneven batch over models (kls_multi.cu) ------------------------------------
 int kls_multi_launch_f64(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs, int n_pairs,
                          const kls_item* d_items, int n_items, int* d_counter, int grid,
-                         int64_t max_K_pad) {
+                         int64_t max_K_pad, int form) {
   int wblocks = (int)std::min<int64_t>((max_K_pad + 255) / 256, 1024);
   multi_weights_kernel<<<dim3(wblocks, n_pairs), 256, 0, st>>>(d_md, d_pairs);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return (int)e;
-  if ((e = cudaFuncSetAttribute(multi_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)CT_SMEM)) != cudaSuccess)
+  const bool g3 = form == KLS_F64_3M;
+  if ((e = cudaFuncSetAttribute(g3 ? (const void*)multi_contract3m_kernel
+                                   : (const void*)multi_contract_kernel,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(g3 ? CT3_SMEM : CT_SMEM))) != cudaSuccess)
     return (int)e;
   if ((e = cudaMemsetAsync(d_counter, 0, sizeof(int), st)) != cudaSuccess) return (int)e;
-  multi_contract_kernel<<<grid, CT_THREADS, CT_SMEM, st>>>(d_md, d_items, n_items, d_counter);
+  if (g3)
+    multi_contract3m_kernel<<<grid, CT3_THREADS, CT3_SMEM, st>>>(d_md, d_items, n_items,
+                                                                 d_counter);
+  else
+    multi_contract_kernel<<<grid, CT_THREADS, CT_SMEM, st>>>(d_md, d_items, n_items, d_counter);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   multi_reduce_kernel<<<dim3(256, n_pairs), 256, 0, st>>>(d_md, d_pairs);
   return (int)cudaGetLastError();
@@ -413,16 +592,7 @@ int kls_multi_launch_f64_weights(cudaStream_t st, const kls_mdesc* d_md, const i
   return (int)cudaGetLastError();
 }
 
-int kls_multi_contract_slots(int device) {
-  int sms = 148, per_sm = 2;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaFuncSetAttribute(multi_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)CT_SMEM);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, multi_contract_kernel, CT_THREADS,
-                                                    CT_SMEM) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
-  return sms * per_sm;
-}
+int kls_multi_contract_slots(int device, int form) { return f64_slots(device, form, true); }
 
 int64_t kls_f64_k_per_split(int64_t K_pad, int splits) {
   int64_t slabs = K_pad / CT_BK;

@@ -108,6 +108,7 @@ struct kls_ctx {
   // per-batch workspace (grown on demand)
   int ws_omega = 0;           // omegas the workspace holds
   int splits = 1;             // K splits of the contraction (fixed per context)
+  int f64_form = KLS_F64_4M;  // FP64 contraction: 4 or 3 (Gauss) real products
   double* d_omega = nullptr;  // [ws_omega][2]
   double2* d_wt = nullptr;    // [ws_omega][K_pad]
   double2* d_part = nullptr;  // [ws_omega][splits][Na_pad][Na_pad]
@@ -191,12 +192,12 @@ void kls_mixed_free(kls_ctx* c);
 // uneven batch over models (kls_multi.cu drives these)
 int kls_multi_launch_f64(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs, int n_pairs,
                          const kls_item* d_items, int n_items, int* d_counter, int grid,
-                         int64_t max_K_pad);
+                         int64_t max_K_pad, int form);
 int kls_multi_launch_lu(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs, int n_pairs,
                         int max_Na);
 int kls_multi_launch_f64_weights(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs,
                                  int n_pairs, int64_t max_K_pad);
-int kls_multi_contract_slots(int device);
+int kls_multi_contract_slots(int device, int form);
 int64_t kls_f64_k_per_split(int64_t K_pad, int splits);
 int kls_multi_launch_mixed(cudaStream_t st, const kls_mdesc* d_md, const int2* d_pairs,
                            int n_pairs, const kls_item* d_items, const int* d_starts, int grid,

@@ -31,6 +31,7 @@
 
 struct kls_multi {
   int device = 0, mode = 0, batch = 0, n_models = 0;
+  int f64_form = KLS_F64_4M;        // FP64: every model's contraction form
   std::vector<kls_ctx*> ctx;
   cudaStream_t stream = nullptr;
   std::string err;
@@ -136,7 +137,7 @@ int build_items(kls_multi* m) {
             m->items.push_back(kls_item{i, z, t, s, 1, 0, (int)std::max<int64_t>(0, ke - kb), 0});
           }
     }
-    m->grid = std::max(1, std::min((int)m->items.size(), kls_multi_contract_slots(m->device)));
+    m->grid = std::max(1, std::min((int)m->items.size(), kls_multi_contract_slots(m->device, m->f64_form)));
     return KLS_OK;
   }
   m->list.clear();
@@ -214,7 +215,7 @@ int launch_batch(kls_multi* m) {
   const int np = (int)m->pairs.size();
   if (m->mode == KLS_MODE_FP64) {
     r = kls_multi_launch_f64(m->stream, m->d_md, m->d_pairs, np, m->d_items, (int)m->items.size(),
-                             m->d_counter, m->grid, m->max_K_pad);
+                             m->d_counter, m->grid, m->max_K_pad, m->f64_form);
   } else {
     // the mixed weights are converted from the FP64 weights of the same pass
     r = kls_multi_launch_f64_weights(m->stream, m->d_md, m->d_pairs, np, m->max_K_pad);
@@ -365,10 +366,13 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
     if (mode == KLS_MODE_FP64 && !models[i]->d_Wre)
       return mfail(nullptr, KLS_ERR_STATE,
                    "model " + std::to_string(i) + ": the FP64 table was released");
+    if (mode == KLS_MODE_FP64 && models[i]->f64_form != models[0]->f64_form)
+      return mfail(nullptr, KLS_ERR_CONFIG, "FP64 models of a batch need one contraction form");
   }
   kls_multi* m = new kls_multi();
   m->device = models[0]->device;
   m->mode = mode;
+  m->f64_form = models[0]->f64_form;
   m->batch = batch;
   m->n_models = n_models;
   m->ctx.assign(models, models + n_models);

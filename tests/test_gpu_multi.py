@@ -43,7 +43,8 @@ def pcs(lib_path):
         x.close()
 
 
-@pytest.mark.parametrize("Tgpu,form", [("Float64", None), ("Float32", _lib.KLS_MIXED_ONE_CTA),
+@pytest.mark.parametrize("Tgpu,form", [("Float64", None), ("Float64", "3m"),
+                                       ("Float32", _lib.KLS_MIXED_ONE_CTA),
                                        ("Float32", _lib.KLS_MIXED_TMEM)])
 def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu, form):
     n = 7                                  # passes of 3: 3 + 3 + 1
@@ -51,7 +52,9 @@ def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu, form):
     singles = []
     for pc, o in zip(pcs, om):
         dev = K.to_device(pc, K.GPUType.NVIDIA, Tgpu)
-        if form is not None:
+        if form == "3m":
+            pc.ctx.call("kls_set_f64_form", _lib.KLS_F64_3M)
+        elif form is not None:
             # the batch runs this form's kernel body when it is every model's form
             pc.ctx.call("kls_set_mixed_form", form)
         singles.append(K.compute_determinant_batched(o, pc, dev, batch_size=16, log_abs=True))
@@ -59,6 +62,9 @@ def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu, form):
     d, la = mb.det(om)
     info = mb.info()
     mb.close()
+    if form == "3m":
+        for pc in pcs:
+            pc.ctx.call("kls_set_f64_form", _lib.KLS_F64_4M)
     for i, (ds, ls) in enumerate(singles):
         assert np.array_equal(d[i], ds), (i, np.max(np.abs(d[i] - ds) / np.abs(ds)))
         assert np.array_equal(la[i], ls), i
@@ -238,3 +244,16 @@ def test_batched_m3_real_q1_model_matches_oracle(pcs):
     assert np.all(np.abs(d64[1] - ref) <= 1e-11 * np.abs(ref) + 4 * sens), \
         np.abs(d64[1] - ref) / np.abs(ref)
     assert np.max(np.abs(d32[1] - ref) / np.abs(ref)) < 1e-3
+
+
+def test_batch_needs_one_fp64_form(pcs):
+    pcs[1].ctx.call("kls_set_f64_form", _lib.KLS_F64_3M)
+    try:
+        with pytest.raises(K.KlsError) as e:
+            K.ModelBatch(pcs, "Float64", batch=2)
+        assert e.value.code == _lib.KLS_ERR_CONFIG
+        with pytest.raises(K.KlsError) as e:
+            pcs[0].ctx.call("kls_set_f64_form", 2)
+        assert e.value.code == _lib.KLS_ERR_CONFIG
+    finally:
+        pcs[1].ctx.call("kls_set_f64_form", _lib.KLS_F64_4M)

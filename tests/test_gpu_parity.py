@@ -109,6 +109,24 @@ def test_M_and_det(case):
     assert np.all(np.abs(d - ref["dets"]) <= tol), (name, np.abs(d - ref["dets"]) / np.abs(ref["dets"]))
 
 
+def test_M_and_det_3m_form(case):
+    """The 3M (Gauss) FP64 contraction against the oracle, same tolerances."""
+    name, ref, pc = case
+    pc.ctx.call("kls_set_f64_form", 1)
+    try:
+        M = K.build_M_matrix(ref["omegas"][0], pc)
+        d = K.compute_determinant_batched(ref["omegas"], pc)
+        a = K.compute_determinant_batched(ref["omegas"][:3], pc, batch_size=3)
+        b = np.array([K.compute_determinant(w, pc) for w in ref["omegas"][:3]])
+    finally:
+        pc.ctx.call("kls_set_f64_form", 0)
+    ok, worst = close(M, ref, "M0", 1e-11)
+    assert ok, (name, worst, relmax(M, ref["M0"]))
+    tol = 1e-11 * np.abs(ref["dets"]) + 4 * ref["sens_dets"]
+    assert np.all(np.abs(d - ref["dets"]) <= tol), (name, np.abs(d - ref["dets"]) / np.abs(ref["dets"]))
+    assert np.array_equal(a, b)
+
+
 def test_batch_composition_is_bitwise_stable(case):
     name, ref, pc = case
     om = np.array([0.88 + 0.12j, 0.7 + 0.2j, 0.91 + 0.02j, 1.3 + 0.4j] * 5)
