@@ -219,7 +219,12 @@ int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cf
  *            determinant gives the next secant slope.  It stops when the
  *            next step is shorter than mixed_step_tol (that step is taken
  *            without an evaluation), when |det| does not fall (the split
- *            form's noise floor) or after mixed_max_iter steps.
+ *            form's noise floor) or after mixed_max_iter steps.  While
+ *            the first step is longer than far_step (a start far from the
+ *            root), it is preceded by steps of FP64 accuracy that follow
+ *            the reference's own path: det at an FP64 anchor (one FP64
+ *            determinant per step) and the slope by an anchored forward
+ *            difference of step m * nc->delta.
  *   phase 2: kls_set_anchor at the last point (one FP64 determinant), then
  *            KLS_MODE_ANCHORED determinants, secant steps from those values
  *            (FP64 accuracy near the anchor), starting with the phase-1
@@ -239,6 +244,7 @@ typedef struct kls_hybrid_cfg {
     int32_t fp64_max_iter;
     double  anchor_radius;
     int32_t final_fp64;
+    double  far_step;
 } kls_hybrid_cfg;
 /* evals[0..2] (may be NULL): split-BF16, plain FP64 (anchors included) and
  * anchored determinant evaluations.                                        */

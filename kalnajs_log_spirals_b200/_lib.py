@@ -87,7 +87,8 @@ class kls_newton_result(C.Structure):
 class kls_hybrid_cfg(C.Structure):
     _fields_ = [("mixed_delta", C.c_double), ("mixed_step_tol", C.c_double),
                 ("mixed_max_iter", C.c_int32), ("fp64_max_iter", C.c_int32),
-                ("anchor_radius", C.c_double), ("final_fp64", C.c_int32)]
+                ("anchor_radius", C.c_double), ("final_fp64", C.c_int32),
+                ("far_step", C.c_double)]
 
 
 class kls_scan_cfg(C.Structure):

@@ -636,13 +636,17 @@ class HybridConfig:
     phase hands over once its next step is below 1e-5 (its root error is
     ~1e-6).  Anchored determinants stay within FP64 accuracy for ~1e-5 around
     the anchor; a step beyond anchor_radius re-anchors (one FP64
-    determinant)."""
+    determinant).  From a start whose first Newton step is longer than
+    far_step the iteration first follows the reference's path with steps of
+    FP64 accuracy (one FP64 and one anchored determinant each), so that a
+    long path from a grid edge ends on the root the FP64 Newton reaches."""
     mixed_delta: float = 1e-3
     mixed_step_tol: float = 1e-5
     mixed_max_iter: int = 30
     fp64_max_iter: int = 50
     anchor_radius: float = 1e-5
     final_fp64: bool = False
+    far_step: float = 2e-2
 
 
 def set_anchor(precomputed: PrecomputedData, omega: complex) -> complex:
@@ -677,7 +681,8 @@ def newton_search_hybrid(config: KalnajsConfig, precomputed: PrecomputedData,
                              int(bool(n.use_line_search)), int(n.max_line_search), KLS_MODE_FP64)
     h = _lib.kls_hybrid_cfg(float(hc.mixed_delta), float(hc.mixed_step_tol),
                             int(hc.mixed_max_iter), int(hc.fp64_max_iter),
-                            float(hc.anchor_radius), int(bool(hc.final_fp64)))
+                            float(hc.anchor_radius), int(bool(hc.final_fp64)),
+                            float(hc.far_step))
     res = _lib.kls_newton_result()
     ev = (C.c_int32 * 3)()
     hist = np.zeros((int(n.max_iter), 3))

@@ -620,7 +620,7 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
   int r = check_ready(c);
   if (r) return r;
   if (!nc || !hc || !res || hc->mixed_max_iter < 0 || hc->fp64_max_iter < 1 ||
-      !(hc->mixed_delta > 0.0) || !(hc->anchor_radius > 0.0))
+      !(hc->mixed_delta > 0.0) || !(hc->anchor_radius > 0.0) || !(hc->far_step > 0.0))
     return kls_fail(c, KLS_ERR_CONFIG, "bad hybrid Newton arguments");
   using cplx = std::complex<double>;
   const double m = (double)c->cfg.m, tol = nc->tol;
@@ -675,6 +675,36 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
     S = (d[1] - d[0]) / h;
   }
   bool haveS = usable(S);
+  // ---- phase 0 (far from a root): while the Newton step is longer than
+  //      far_step, steps of FP64 accuracy that follow the reference's path:
+  //      det at an FP64 anchor, slope by an anchored forward difference
+  //      (step m * nc->delta, as the reference's Jacobian)
+  for (int it = 0; haveS && it < hc->fp64_max_iter && std::abs(f / S) > hc->far_step; ++it) {
+    double d2[2];
+    if ((r = kls_set_anchor(c, w.real(), w.imag(), d2))) return r;
+    ++n_fp64;
+    const cplx fa(d2[0], d2[1]);
+    hist(w, std::abs(fa));
+    const cplx wd = w + m * nc->delta;
+    cplx fd;
+    if ((r = det(&wd, 1, KLS_MODE_ANCHORED, &fd))) return r;
+    const cplx Sa = (fd - fa) / (m * nc->delta);
+    if (!usable(Sa)) {
+      finish(w, fa, false);
+      return kls_fail(c, KLS_ERR_SINGULAR, "singular Jacobian in the far phase");
+    }
+    f = fa;
+    S = Sa;
+    if (std::abs(fa) < tol) break;               // already at a root
+    const cplx wn = clamp(w - fa / Sa);
+    if (wn == w) break;
+    w = wn;
+    if (std::abs(fa / Sa) <= hc->far_step) {     // hand over to the split-BF16 phase
+      if ((r = det(&w, 1, KLS_MODE_MIXED, &f))) return r;
+      hist(w, std::abs(f));
+      break;
+    }
+  }
   for (int it = 0; haveS && it < hc->mixed_max_iter; ++it) {
     const cplx wn = clamp(w - f / S);
     if (std::abs(wn - w) < hc->mixed_step_tol) {   // below the split form's resolution

@@ -161,7 +161,7 @@ end
 
 struct KlsHybridCfg
     mixed_delta::Float64; mixed_step_tol::Float64; mixed_max_iter::Int32; fp64_max_iter::Int32
-    anchor_radius::Float64; final_fp64::Int32
+    anchor_radius::Float64; final_fp64::Int32; far_step::Float64
 end
 
 struct KlsTuneResult
@@ -179,13 +179,13 @@ function newton_search_hybrid(config, precomp::PrecomputedData, Omega_p_init::Re
                               gamma_init::Real; mixed_delta::Real=1e-3,
                               mixed_step_tol::Real=1e-5, mixed_max_iter::Integer=30,
                               fp64_max_iter::Integer=50, anchor_radius::Real=1e-5,
-                              final_fp64::Bool=false)
+                              final_fp64::Bool=false, far_step::Real=2e-2)
     n = config.newton
     check(precomp.handle, ccall((:kls_prepare_mixed, LIBKLS), Cint, (Ptr{Cvoid},), precomp.handle))
     nc = Ref(KlsNewtonCfg(n.max_iter, n.tol, n.delta, n.use_line_search, n.max_line_search,
                           KLS_MODE_FP64))
     hc = Ref(KlsHybridCfg(mixed_delta, mixed_step_tol, mixed_max_iter, fp64_max_iter,
-                          anchor_radius, Int32(final_fp64)))
+                          anchor_radius, Int32(final_fp64), far_step))
     res = Ref(KlsNewtonResult())
     evals = zeros(Int32, 3)
     hist = zeros(Float64, 3, n.max_iter)

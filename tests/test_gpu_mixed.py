@@ -131,3 +131,26 @@ def test_mixed_and_hybrid_newton(lib_path):
     evals = (rh.mixed_evals, rh.fp64_evals, rh.anchored_evals)
     assert abs(rh.det_val) < 1e-12 and abs(d64_at_h) < 1e-12, (rh.det_val, d64_at_h, evals)
     assert rh.fp64_evals <= 2, evals
+
+
+def test_hybrid_far_start_follows_the_fp64_path(lib_path):
+    """From a start whose first Newton step is long, the hybrid's far phase
+    (FP64 anchor + anchored forward difference per step) reaches the root the
+    plain FP64 Newton reaches from the same start (1e-10)."""
+    from kalnajs_log_spirals_b200.api import newton_search_hybrid
+    c = kconfig(**SMALL)
+    c.newton.tol = 1e-12
+    c.newton.use_line_search = False
+    pc = K.precompute_all(c)
+    checked = 0
+    for Op0, g0 in [(0.47, 0.16), (0.41, 0.09), (0.50, 0.20), (0.45, 0.05)]:
+        r64 = K.newton_search(c, pc, None, K.GPUType.NVIDIA, "Float64", Op0, g0)
+        if not (r64.converged and r64.gamma > 1e-4):
+            continue
+        rh = newton_search_hybrid(c, pc, Op0, g0)
+        assert rh.converged, (Op0, g0)
+        assert abs(rh.Omega_p - r64.Omega_p) <= 1e-10 and abs(rh.gamma - r64.gamma) <= 1e-10, \
+            (Op0, g0, rh.Omega_p - r64.Omega_p, rh.gamma - r64.gamma)
+        checked += 1
+    pc.close()
+    assert checked >= 1
