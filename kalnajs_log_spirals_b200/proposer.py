@@ -206,19 +206,46 @@ def shortlist(mlp: MLP, spec: ModelSpec, k: int = 48, n_Op: int = 41, n_gamma: i
     return OP.ravel(order="F")[idx], GM.ravel(order="F")[idx], idx
 
 
-def propose(mlp: MLP, spec: ModelSpec, det_fn, k: int = 48, **grid) -> Tuple[float, float, int]:
+def propose(mlp: MLP, spec: ModelSpec, det_fn, k: int = 48, descend: int = 6,
+            **grid) -> Tuple[float, float, int]:
     """Newton start in place of grid_scan + find_minimum (GridScan.jl:25-88, 234-246).
 
     ``det_fn(omegas) -> dets`` evaluates the true determinant at the k
-    shortlisted grid points (one batch); the start is the shortlisted point of
-    minimal |det|, first in column-major order as find_minimum takes it.  When
-    the scan's own argmin is on the shortlist this is exactly the scan's start.
+    shortlisted grid points (one batch).  From the shortlisted point of
+    minimal |det| a descent on the scan grid follows: the point's unevaluated
+    8 neighbours are evaluated (one batch) and the start moves to the lowest
+    |det| seen, up to ``descend`` times or until it stays, so a shortlist that
+    lands next to the scan's argmin still finds it.  Ties go to the first
+    point in column-major order, as find_minimum takes it.  When the scan's
+    own argmin is the lowest point reached this is exactly the scan's start.
     Returns (Omega_p, gamma, determinant evaluations used).
     """
-    Op, gm, _ = shortlist(mlp, spec, k=k, **grid)
-    d = np.asarray(det_fn(spec.m * Op + 1j * gm))
-    i = int(np.argmin(np.abs(d)))
-    return float(Op[i]), float(gm[i]), len(Op)
+    n_Op, n_gamma = grid.get("n_Op", 41), grid.get("n_gamma", 20)
+    Op_g = np.linspace(*grid.get("Op_range", (0.2, 0.6)), n_Op)
+    g_g = np.linspace(*grid.get("g_range", (0.01, 0.2)), n_gamma)
+    _, _, idx = shortlist(mlp, spec, k=k, **grid)
+    at = lambda q: (float(Op_g[q // n_gamma]), float(g_g[q % n_gamma]))
+    known = {}
+
+    def evaluate(qs):
+        pts = np.array([spec.m * at(q)[0] + 1j * at(q)[1] for q in qs])
+        for q, v in zip(qs, np.abs(np.asarray(det_fn(pts)))):
+            known[int(q)] = float(v)
+
+    evaluate([int(q) for q in idx])
+    best = min(known, key=lambda q: (known[q], q))
+    for _ in range(descend):
+        iO, ig = best // n_gamma, best % n_gamma
+        nb = [a * n_gamma + b for a in range(iO - 1, iO + 2) for b in range(ig - 1, ig + 2)
+              if 0 <= a < n_Op and 0 <= b < n_gamma and a * n_gamma + b not in known]
+        if not nb:
+            break
+        evaluate(nb)
+        nxt = min(known, key=lambda q: (known[q], q))
+        if nxt == best:
+            break
+        best = nxt
+    return at(best)[0], at(best)[1], len(known)
 
 
 @dataclasses.dataclass

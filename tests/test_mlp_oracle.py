@@ -85,8 +85,28 @@ def test_propose_picks_the_smallest_true_determinant_of_the_shortlist():
         calls.append(len(om))
         return (om.real / 2 - 0.42) + 1j * (om.imag - 0.06)
 
-    Op, g, used = P.propose(net, spec, det_fn, k=12)
+    Op, g, used = P.propose(net, spec, det_fn, k=12, descend=0)
     assert calls == [12] and used == 12
     Ops, gs, _ = P.shortlist(net, spec, k=12)
     best = np.argmin(np.abs((Ops - 0.42) + 1j * (gs - 0.06)))
     assert (Op, g) == (float(Ops[best]), float(gs[best]))
+
+
+def test_propose_descends_to_the_grid_minimum():
+    """The grid descent after the shortlist reaches the grid point of least
+    |det| when the shortlist only lands near it."""
+    spec = P.ModelSpec(4, 7.0, 2)
+    net = _StubNet(0.36, 0.12)                     # shortlist around a point 3 columns away
+    calls = []
+
+    def det_fn(om):
+        calls.append(len(om))
+        return (om.real / 2 - 0.42) + 1j * (om.imag - 0.06)
+
+    Op, g, used = P.propose(net, spec, det_fn, k=6)
+    grid_Op = np.linspace(0.2, 0.6, 41)
+    grid_g = np.linspace(0.01, 0.2, 20)
+    d = np.abs((grid_Op[:, None] - 0.42) + 1j * (grid_g[None, :] - 0.06))
+    i, j = np.unravel_index(np.argmin(d), d.shape)
+    assert (Op, g) == (float(grid_Op[i]), float(grid_g[j]))
+    assert calls[0] == 6 and used == sum(calls) and len(calls) > 1
