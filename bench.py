@@ -615,16 +615,24 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
         t_learned = time.perf_counter() - t0
         growing = bool(r64.converged and r64.gamma > 1e-4)
         same = False
+        a = b = None
         if growing and rh.converged:
             a, b = polish(K, cfg, pc, r64.Omega_p, r64.gamma), polish(K, cfg, pc, rh.Omega_p,
                                                                       rh.gamma)
             same = abs(a[0] - b[0]) <= 1e-10 and abs(a[1] - b[1]) <= 1e-10
+        # diagnostics (untimed): plain FP64 Newton from the proposal's start
+        rp = K.newton_search(cfg, pc, None, K.GPUType.NVIDIA, "Float64", Op_p, g_p)
         pc.close()
         rows.append({"n_zang": sp.n_zang, "q1": sp.q1, "m": sp.m, "growing_mode": growing,
                      "same_root": same, "start_equals_scan_argmin": (Op_p, g_p) == (Op0, g0),
                      "plain_fp64_s": s.n_Op * s.n_gamma * t_fp64_det + t_n64,
                      "mixed_scan_s": t_scan_mx, "learned_s": t_learned,
-                     "Omega_p": r64.Omega_p, "gamma": r64.gamma})
+                     "Omega_p": r64.Omega_p, "gamma": r64.gamma,
+                     "scan_start": [Op0, g0], "proposal_start": [Op_p, g_p],
+                     "fp64_from_proposal": [rp.Omega_p, rp.gamma, bool(rp.converged)],
+                     "hybrid": [rh.Omega_p, rh.gamma, bool(rh.converged), rh.mixed_evals,
+                                rh.fp64_evals, rh.anchored_evals],
+                     "polished_scan_root": a, "polished_hybrid_root": b})
     grow = [r for r in rows if r["growing_mode"]]
     ok = [r for r in grow if r["same_root"]]
     mean = lambda k, rs: float(np.mean([r[k] for r in rs])) if rs else None

@@ -212,31 +212,32 @@ int kls_newton(kls_ctx* ctx, double Omega_p0, double gamma0, const kls_newton_cf
  * |det| < nc->tol holds on a determinant of FP64 accuracy).  det(I - M(omega))
  * is holomorphic in omega = m Omega_p + i gamma, so one complex slope S gives
  * the reference's whole 2x2 finite-difference Jacobian (dF/dOmega_p = m S,
- * dF/dgamma = i S) and the step is delta omega = -det / S:
+ * dF/dgamma = i S) and the step is delta omega = -det / S.  Steps are
+ * accepted as the reference accepts them (every step, no line search),
+ * except that a step shorter than 1e-4 that does not lower |det| ends a
+ * phase (the determinant's rounding decides such steps):
  *   phase 1: secant iteration on split-BF16 determinants.  The first slope
  *            is the forward difference of the pair (omega, omega + h),
  *            h = m*mixed_delta, evaluated as one batch; each later step's
- *            determinant gives the next secant slope.  It stops when the
- *            next step is shorter than mixed_step_tol (that step is taken
- *            without an evaluation), when |det| does not fall (the split
- *            form's noise floor) or after mixed_max_iter steps.  While
- *            the first step is longer than far_step (a start far from the
- *            root), it is preceded by steps of FP64 accuracy that follow
- *            the reference's own path: det at an FP64 anchor (one FP64
- *            determinant per step) and the slope by an anchored forward
- *            difference of step m * nc->delta.
+ *            determinant gives the next secant slope.  While the Newton step
+ *            is longer than far_step, steps of FP64 accuracy follow the
+ *            reference's own path instead: det at an FP64 anchor and the
+ *            slope by an anchored forward difference of step m * nc->delta.
+ *            The phase ends when the next step is shorter than
+ *            mixed_step_tol (taken without an evaluation), at the noise
+ *            floor, or after mixed_max_iter + fp64_max_iter steps.
  *   phase 2: kls_set_anchor at the last point (one FP64 determinant), then
- *            KLS_MODE_ANCHORED determinants, secant steps from those values
- *            (FP64 accuracy near the anchor), starting with the phase-1
- *            slope.  A step that lands farther than anchor_radius from the
- *            anchor moves the anchor there (another FP64 determinant).  A
- *            step that does not lower |det| is retried once with a slope by
- *            forward difference (step nc->delta); the phase ends when |det|
- *            < tol and the next step is below 1e-11 (|det| < tol alone fixes
- *            the root only to tol / |det'|), when |det| < tol and |det|
- *            stops falling, or after fp64_max_iter steps.  final_fp64 != 0
- *            adds one plain FP64 determinant at the result, which then
- *            decides `converged` and is the returned det.                 */
+ *            KLS_MODE_ANCHORED determinants (FP64 accuracy near the anchor),
+ *            secant steps starting with the phase-1 slope; a step beyond
+ *            anchor_radius of the anchor moves the anchor (another FP64
+ *            determinant) and is followed by a forward-difference slope.  A
+ *            short step that does not lower |det| is retried once with a
+ *            forward-difference slope.  The phase ends when |det| < tol and
+ *            the next step is below 1e-11 (|det| < tol alone fixes the root
+ *            only to tol / |det'|), when |det| < tol and stops falling, or
+ *            after fp64_max_iter steps.  final_fp64 != 0 adds one plain FP64
+ *            determinant at the result, which then decides `converged` and
+ *            is the returned det.                                          */
 typedef struct kls_hybrid_cfg {
     double  mixed_delta;
     double  mixed_step_tol;

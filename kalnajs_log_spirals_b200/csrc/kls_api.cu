@@ -663,7 +663,13 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
   // d det / d omega gives the whole 2x2 finite-difference Jacobian of the
   // reference (dF/dOmega_p = m S, dF/dgamma = i S) and the Newton step is
   // delta omega = -det / S.
-  // ---- phase 1: split-BF16 secant iteration
+  // Steps are taken as the reference takes them (NewtonSolver.jl:66-161:
+  // every step accepted, no line search), except that a step of the noise
+  // scale that does not lower |det| ends a phase: there the determinant's
+  // rounding, not the root, decides the direction.
+  const double noise_step = 1e-4;
+  // ---- phase 1: split-BF16 secant iteration, with far steps of FP64
+  //      accuracy while the Newton step is longer than far_step
   const double h = m * hc->mixed_delta;
   cplx S, f;
   {
@@ -675,61 +681,65 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
     S = (d[1] - d[0]) / h;
   }
   bool haveS = usable(S);
-  // ---- phase 0 (far from a root): while the Newton step is longer than
-  //      far_step, steps of FP64 accuracy that follow the reference's path:
-  //      det at an FP64 anchor, slope by an anchored forward difference
-  //      (step m * nc->delta, as the reference's Jacobian)
-  for (int it = 0; haveS && it < hc->fp64_max_iter && std::abs(f / S) > hc->far_step; ++it) {
+  // far step at w: det at an FP64 anchor, slope by an anchored forward
+  // difference (step m * nc->delta, the reference's Jacobian step); leaves
+  // f = FP64 det at w, S = that slope
+  auto far_slope = [&]() -> int {
     double d2[2];
-    if ((r = kls_set_anchor(c, w.real(), w.imag(), d2))) return r;
+    int q = kls_set_anchor(c, w.real(), w.imag(), d2);
+    if (q) return q;
     ++n_fp64;
-    const cplx fa(d2[0], d2[1]);
-    hist(w, std::abs(fa));
+    f = cplx(d2[0], d2[1]);
+    hist(w, std::abs(f));
     const cplx wd = w + m * nc->delta;
     cplx fd;
-    if ((r = det(&wd, 1, KLS_MODE_ANCHORED, &fd))) return r;
-    const cplx Sa = (fd - fa) / (m * nc->delta);
-    if (!usable(Sa)) {
-      finish(w, fa, false);
-      return kls_fail(c, KLS_ERR_SINGULAR, "singular Jacobian in the far phase");
+    if ((q = det(&wd, 1, KLS_MODE_ANCHORED, &fd))) return q;
+    S = (fd - f) / (m * nc->delta);
+    haveS = usable(S);
+    return KLS_OK;
+  };
+  bool fp64_f = false;                           // f is of FP64 accuracy (a far step's)
+  for (int it = 0; haveS && it < hc->mixed_max_iter + hc->fp64_max_iter; ++it) {
+    if (std::abs(f / S) > hc->far_step) {
+      if (!fp64_f && (r = far_slope())) return r;
+      if (!haveS) break;
+      fp64_f = true;
+      if (std::abs(f) < tol) break;
+      const cplx wn = clamp(w - f / S);
+      if (wn == w) break;
+      w = wn;
+      if ((r = far_slope())) return r;         // det and slope at the new point
+      continue;
     }
-    f = fa;
-    S = Sa;
-    if (std::abs(fa) < tol) break;               // already at a root
-    const cplx wn = clamp(w - fa / Sa);
-    if (wn == w) break;
-    w = wn;
-    if (std::abs(fa / Sa) <= hc->far_step) {     // hand over to the split-BF16 phase
+    if (fp64_f) {                                // back to the split form at w
       if ((r = det(&w, 1, KLS_MODE_MIXED, &f))) return r;
       hist(w, std::abs(f));
-      break;
+      fp64_f = false;
     }
-  }
-  for (int it = 0; haveS && it < hc->mixed_max_iter; ++it) {
     const cplx wn = clamp(w - f / S);
-    if (std::abs(wn - w) < hc->mixed_step_tol) {   // below the split form's resolution
+    const double step = std::abs(wn - w);
+    if (step < hc->mixed_step_tol) {             // below the split form's resolution
       w = wn;
       break;
     }
     cplx fn;
     if ((r = det(&wn, 1, KLS_MODE_MIXED, &fn))) return r;
     hist(wn, std::abs(fn));
-    if (!(std::abs(fn) < std::abs(f))) break;      // noise floor (or a bad slope): stop here
+    if (!(std::abs(fn) < std::abs(f)) && step < noise_step) break;   // noise floor: stay at w
     const cplx Sn = (fn - f) / (wn - w);
     w = wn;
     f = fn;
     if (usable(Sn)) S = Sn;
   }
   // ---- phase 2: FP64 anchor, then anchored determinants
-  cplx wa = w, fa;
-  {
+  cplx wa = w;
+  if (!fp64_f) {                                 // (a far step left its anchor at w)
     double d2[2];
     if ((r = kls_set_anchor(c, w.real(), w.imag(), d2))) return r;
     ++n_fp64;
-    fa = cplx(d2[0], d2[1]);
+    f = cplx(d2[0], d2[1]);
+    hist(w, std::abs(f));
   }
-  f = fa;
-  hist(w, std::abs(f));
   // a determinant of FP64 accuracy at wn: anchored near the anchor, else a
   // new anchor there
   auto eval2 = [&](cplx wn, cplx* out) -> int {
@@ -758,17 +768,25 @@ int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newto
       return kls_fail(c, KLS_ERR_SINGULAR, "singular Jacobian in the FP64-anchored phase");
     }
     const cplx wn = clamp(w - f / S);
-    if (std::abs(f) < tol && std::abs(wn - w) <= 1e-11) { converged = true; break; }
+    const double step = std::abs(wn - w);
+    if (std::abs(f) < tol && step <= 1e-11) { converged = true; break; }
     if (wn == w) break;                            // clamped in place
     cplx fn;
     if ((r = eval2(wn, &fn))) return r;
     hist(wn, std::abs(fn));
-    if (std::abs(fn) < std::abs(f)) {
-      const cplx Sn = (fn - f) / (wn - w);         // secant slope
+    if (std::abs(fn) < std::abs(f) || step >= noise_step) {
+      // accepted (a long step is accepted even if |det| grows, as the
+      // reference accepts every step); secant slope after a short step, a
+      // fresh forward difference at the new point after a long one
+      const cplx Sn = (fn - f) / (wn - w);
       w = wn;
       f = fn;
-      if (usable(Sn)) S = Sn;
-      fresh = false;
+      if (step < noise_step && usable(Sn)) {
+        S = Sn;
+        fresh = false;
+      } else {
+        haveS = false;
+      }
       continue;
     }
     if (std::abs(f) < tol) { converged = true; break; }   // |det| stopped falling below tol

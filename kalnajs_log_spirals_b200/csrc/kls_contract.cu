@@ -250,12 +250,13 @@ contract_kernel(ContractParams P, const double* __restrict__ Wre, const double* 
 // With A = W_b (ar + i ai) and B = w conj(W_a) (br + i bi):
 //   P1 = ar br, P2 = ai bi, P3 = (ar + ai)(br + bi),
 //   Re = P1 - P2, Im = (P3 - P1) - P2,
-// so each k step takes 3 DMMAs per output fragment instead of 4.  The three
-// accumulators need 1.5x the registers of the 4M form's two, so the 64 x 64
-// tile is split over 8 warps of 32 x 16 (one CTA per SM, the same 8 warps
-// per SM as two 4M CTAs) and the pipeline is 4 stages deep.
-constexpr int CT3_THREADS = 256;
-constexpr int CT3_STAGES = 4;
+// so each k step takes 3 DMMAs per output fragment instead of 4.  Same tile
+// and warp layout as the 4M form (4 warps of 32 x 32, 2 CTAs per SM); the
+// three accumulators take 192 of the 255 registers, and the B fragment of
+// each column block is formed just before its 12 DMMAs to keep the rest live
+// set small.
+constexpr int CT3_THREADS = 128;
+constexpr int CT3_STAGES = 3;
 constexpr size_t CT3_SMEM = (size_t)CT3_STAGES * CT_STAGE_DOUBLES * sizeof(double);
 
 __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
@@ -267,7 +268,7 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
   const int tm = tile / P.tiles_1d, tn = tile % P.tiles_1d;
   const int b0 = tm * KLS_TILE, a0 = tn * KLS_TILE;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 2, wn = warp & 3;             // 32 b rows x 16 a columns per warp
+  const int wm = warp >> 1, wn = warp & 1;             // 32 x 32 per warp
   const int64_t kbeg = (int64_t)split * P.k_per_split;
   const int64_t kend = min(P.K_pad, kbeg + P.k_per_split);
   const int nk = kbeg < kend ? (int)((kend - kbeg) / CT_BK) : 0;
@@ -279,7 +280,7 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
     double* st = stage_ptr(s);
     const int64_t k0 = kbeg + (int64_t)kt * CT_BK;
 #pragma unroll
-    for (int it = 0; it < 8; ++it) {
+    for (int it = 0; it < 16; ++it) {
       int cidx = tid + it * CT3_THREADS;       // 0..2047
       int plane = cidx >> 9;                   // 0: A re, 1: A im, 2: B re, 3: B im
       int rem = cidx & 511;
@@ -292,11 +293,11 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
     if (tid < CT_BK) cp_async16(st + 4 * CT_PLANE + 2 * tid, wz + k0 + tid);
   };
 
-  double p1[4][2][2], p2[4][2][2], p3[4][2][2];
+  double p1[4][4][2], p2[4][4][2], p3[4][4][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 2; ++j)
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int h = 0; h < 2; ++h) p1[i][j][h] = p2[i][j][h] = p3[i][j][h] = 0.0;
 
@@ -321,7 +322,7 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
     for (int kk = 0; kk < CT_BK; kk += 4) {
       const int kr = kk + (lane & 3);
       const double dr = sd[2 * kr], di = sd[2 * kr + 1];
-      double ar[4], ai[4], as[4], br[2], bi[2], bs[2];
+      double ar[4], ai[4], as[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         int off = kr * CT_S + wm * 32 + i * 8 + (lane >> 2);
@@ -330,22 +331,20 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
         as[i] = __dadd_rn(ar[i], ai[i]);
       }
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        int off = kr * CT_S + wn * 16 + j * 8 + (lane >> 2);
+      for (int j = 0; j < 4; ++j) {
+        int off = kr * CT_S + wn * 32 + j * 8 + (lane >> 2);
         double xr = sBr[off], xi = sBi[off];
         // the same weighted fragment as the 4M form
-        br[j] = __fma_rn(dr, xr, __dmul_rn(di, xi));
-        bi[j] = __fma_rn(di, xr, -__dmul_rn(dr, xi));
-        bs[j] = __dadd_rn(br[j], bi[j]);
-      }
+        const double br = __fma_rn(dr, xr, __dmul_rn(di, xi));
+        const double bi = __fma_rn(di, xr, -__dmul_rn(dr, xi));
+        const double bs = __dadd_rn(br, bi);
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          dmma(p1[i][j][0], p1[i][j][1], ar[i], br[j]);
-          dmma(p2[i][j][0], p2[i][j][1], ai[i], bi[j]);
-          dmma(p3[i][j][0], p3[i][j][1], as[i], bs[j]);
+        for (int i = 0; i < 4; ++i) {
+          dmma(p1[i][j][0], p1[i][j][1], ar[i], br);
+          dmma(p2[i][j][0], p2[i][j][1], ai[i], bi);
+          dmma(p3[i][j][0], p3[i][j][1], as[i], bs);
         }
+      }
     }
   }
   cp_async_wait<0>();
@@ -355,8 +354,8 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
   for (int i = 0; i < 4; ++i) {
     int b = b0 + wm * 32 + i * 8 + (lane >> 2);
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      int a = a0 + wn * 16 + j * 8 + 2 * (lane & 3);
+    for (int j = 0; j < 4; ++j) {
+      int a = a0 + wn * 32 + j * 8 + 2 * (lane & 3);
       double2* o = out + (size_t)b * ld + a;
 #pragma unroll
       for (int h = 0; h < 2; ++h)
@@ -366,7 +365,7 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
   }
 }
 
-__global__ void __launch_bounds__(CT3_THREADS, 1)
+__global__ void __launch_bounds__(CT3_THREADS, 2)
 contract3m_kernel(ContractParams P, const double* __restrict__ Wre,
                   const double* __restrict__ Wim, const double2* __restrict__ wt,
                   double2* __restrict__ part) {
@@ -405,7 +404,7 @@ multi_contract_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restri
 }
 
 // the same persistent loop over the 3M tile
-__global__ void __launch_bounds__(CT3_THREADS, 1)
+__global__ void __launch_bounds__(CT3_THREADS, 2)
 multi_contract3m_kernel(const kls_mdesc* __restrict__ md, const kls_item* __restrict__ items,
                         int n_items, int* __restrict__ counter) {
   extern __shared__ __align__(16) double smem[];

@@ -207,11 +207,14 @@ def shortlist(mlp: MLP, spec: ModelSpec, k: int = 48, n_Op: int = 41, n_gamma: i
 
 
 def propose(mlp: MLP, spec: ModelSpec, det_fn, k: int = 48, descend: int = 6,
-            **grid) -> Tuple[float, float, int]:
+            edge_rows: int = 1, **grid) -> Tuple[float, float, int]:
     """Newton start in place of grid_scan + find_minimum (GridScan.jl:25-88, 234-246).
 
     ``det_fn(omegas) -> dets`` evaluates the true determinant at the k
-    shortlisted grid points (one batch).  From the shortlisted point of
+    shortlisted grid points and at the ``edge_rows`` grid rows of lowest
+    gamma (one batch): next to the real axis the resonant denominators make
+    |det| vary on scales finer than the network resolves, and modes of
+    small gamma put the scan's argmin on that row.  From the point of
     minimal |det| a descent on the scan grid follows: the point's unevaluated
     8 neighbours are evaluated (one batch) and the start moves to the lowest
     |det| seen, up to ``descend`` times or until it stays, so a shortlist that
@@ -232,7 +235,8 @@ def propose(mlp: MLP, spec: ModelSpec, det_fn, k: int = 48, descend: int = 6,
         for q, v in zip(qs, np.abs(np.asarray(det_fn(pts)))):
             known[int(q)] = float(v)
 
-    evaluate([int(q) for q in idx])
+    edge = [a * n_gamma + b for a in range(n_Op) for b in range(min(edge_rows, n_gamma))]
+    evaluate(sorted(set(int(q) for q in idx) | set(edge)))
     best = min(known, key=lambda q: (known[q], q))
     for _ in range(descend):
         iO, ig = best // n_gamma, best % n_gamma

@@ -257,3 +257,32 @@ def test_batch_needs_one_fp64_form(pcs):
         assert e.value.code == _lib.KLS_ERR_CONFIG
     finally:
         pcs[1].ctx.call("kls_set_f64_form", _lib.KLS_F64_4M)
+
+
+def test_batch_matches_the_oracle(pcs):
+    """Each model of the uneven batch (real-valued q1, m = 2 and 3, four sizes)
+    against the oracle's own determinants (oracle/np_oracle.py, the reference's
+    per-harmonic form) at 3 omegas: 1e-9 relative in FP64 (no per-element
+    sensitivity is stored for these models; the fixture-based parity tests
+    hold 1e-11 plus the 2-ulp-ln sensitivity), 1e-3 in the split-BF16 form."""
+    from oracle import np_oracle as O
+    om = np.stack([omegas(3, 40 + i) * (m / 2) for i, (m, *_) in enumerate(MODELS)])
+    got = {}
+    for Tgpu in ("Float64", "Float32"):
+        mb = K.ModelBatch(pcs, Tgpu, batch=3)
+        got[Tgpu], _ = mb.det(om)
+        mb.close()
+    for i, c in enumerate(configs()):
+        g, md = c.grid, c.model
+        oc = O.OracleConfig(m=int(c.physics.m), G=float(c.physics.G), L0=float(md.L0),
+                            n_zang=int(md.n_zang), q1=float(md.q1), NR=g.NR, Ne=g.Ne,
+                            Rc_min=g.Rc_min, Rc_max=g.Rc_max, v_min=g.v_min,
+                            N_alpha=g.N_alpha, alpha_max=g.alpha_max, l_min=g.l_min,
+                            l_max=g.l_max, nw=g.nw, nwa=g.nwa)
+        opc = O.precompute_all(oc)
+        ref = np.array([O.compute_det(opc, w) for w in om[i]])
+        r64 = np.abs(got["Float64"][i] - ref) / np.abs(ref)
+        rmx = np.abs(got["Float32"][i] - ref) / np.abs(ref)
+        print(f"model {i} (m={oc.m}, q1={oc.q1}): FP64 {r64.max():.1e}, split-BF16 {rmx.max():.1e}")
+        assert r64.max() < 1e-9, (i, r64)
+        assert rmx.max() < 1e-3, (i, rmx)

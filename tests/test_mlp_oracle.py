@@ -85,7 +85,7 @@ def test_propose_picks_the_smallest_true_determinant_of_the_shortlist():
         calls.append(len(om))
         return (om.real / 2 - 0.42) + 1j * (om.imag - 0.06)
 
-    Op, g, used = P.propose(net, spec, det_fn, k=12, descend=0)
+    Op, g, used = P.propose(net, spec, det_fn, k=12, descend=0, edge_rows=0)
     assert calls == [12] and used == 12
     Ops, gs, _ = P.shortlist(net, spec, k=12)
     best = np.argmin(np.abs((Ops - 0.42) + 1j * (gs - 0.06)))
@@ -103,10 +103,26 @@ def test_propose_descends_to_the_grid_minimum():
         calls.append(len(om))
         return (om.real / 2 - 0.42) + 1j * (om.imag - 0.06)
 
-    Op, g, used = P.propose(net, spec, det_fn, k=6)
+    Op, g, used = P.propose(net, spec, det_fn, k=6, edge_rows=0)
     grid_Op = np.linspace(0.2, 0.6, 41)
     grid_g = np.linspace(0.01, 0.2, 20)
     d = np.abs((grid_Op[:, None] - 0.42) + 1j * (grid_g[None, :] - 0.06))
     i, j = np.unravel_index(np.argmin(d), d.shape)
     assert (Op, g) == (float(grid_Op[i]), float(grid_g[j]))
     assert calls[0] == 6 and used == sum(calls) and len(calls) > 1
+
+
+def test_propose_includes_the_lowest_gamma_row():
+    """A deep minimum on the grid row next to the real axis, far from the
+    network's shortlist, is found through the edge row."""
+    spec = P.ModelSpec(4, 7.0, 2)
+    net = _StubNet(0.25, 0.15)
+    calls = []
+
+    def det_fn(om):                                # a root just below the grid at Omega_p 0.52
+        calls.append(len(om))
+        return (om.real / 2 - 0.52) + 1j * (om.imag - 0.005)
+
+    Op, g, used = P.propose(net, spec, det_fn, k=12)
+    assert (Op, g) == (float(np.linspace(0.2, 0.6, 41)[32]), 0.01)
+    assert calls[0] == 12 + 41 - len(set(range(0, 41 * 20, 20)) & set(P.shortlist(net, spec, k=12)[2]))
