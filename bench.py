@@ -712,6 +712,27 @@ def uneven_batch(args, K, P, local, sync):
     for pc in pcs:
         pc.close()
     rate = n_det / (dev_ms * 1e-3)
+    # the smallest batched model against the oracle (its own table, built on
+    # the host cores) at 3 of the evaluated points: split-BF16 det error
+    oracle_check = None
+    small = [i for i, sp in enumerate(specs) if sp.size == P.SIZES[0]]
+    if small:
+        from oracle import np_oracle_large as L
+        i = small[0]
+        oc = oracle_config(P.model_config(base, specs[i]))
+        t0 = time.perf_counter()
+        lp = L.precompute_large(oc, workers=os.cpu_count() or 1)
+        try:
+            pick = [0, nG // 3, (2 * nG) // 3]
+            ref = np.array([L.compute_det_large(lp, om[i, q]) for q in pick])
+        finally:
+            lp.close()
+        rel = np.abs(dets[i, pick] - ref) / np.abs(ref)
+        oracle_check = {"model": i, "spec": [specs[i].n_zang, specs[i].q1, specs[i].m,
+                                             *specs[i].size],
+                        "omegas": [[complex(om[i, q]).real, complex(om[i, q]).imag] for q in pick],
+                        "split_bf16_rel_det_err_vs_oracle": [float(x) for x in rel],
+                        "oracle_s": time.perf_counter() - t0}
     if args.uneven_out:
         np.savez_compressed(args.uneven_out, log_abs=la.reshape(len(specs), cols, nG),
                             arg=np.angle(dets).reshape(len(specs), cols, nG),
@@ -728,6 +749,7 @@ def uneven_batch(args, K, P, local, sync):
         "one_model_at_a_time_det_evals_per_s": len(specs) * nG / t_seq,
         "projected_full_grid_s": len(specs) * nO * nG / rate,
         "maps_saved": args.uneven_out or None,
+        "oracle_check": oracle_check,
         "batch_launch": {"items": info["n_items"], "ctas": info["grid"],
                          "schedule": ["persistent round robin", "one CTA (pair) per item"][
                              info["schedule"]],
