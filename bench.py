@@ -611,30 +611,51 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
         Op_p, g_p, used = P.propose(mlp, sp, lambda w: K.compute_determinant_batched(
             w, pc, devmx, batch_size=16), k=48, n_Op=s.n_Op, n_gamma=s.n_gamma,
             Op_range=(s.Omega_p_min, s.Omega_p_max), g_range=(s.gamma_min, s.gamma_max))
-        rh = newton_search_hybrid(cfg, pc, Op_p, g_p)
-        t_learned = time.perf_counter() - t0
-        growing = bool(r64.converged and r64.gamma > 1e-4)
-        same = False
-        a = b = None
-        if growing and rh.converged:
-            a, b = polish(K, cfg, pc, r64.Omega_p, r64.gamma), polish(K, cfg, pc, rh.Omega_p,
-                                                                      rh.gamma)
-            same = abs(a[0] - b[0]) <= 1e-10 and abs(a[1] - b[1]) <= 1e-10
-        # diagnostics (untimed): plain FP64 Newton from the proposal's start
+        t_prop = time.perf_counter() - t0
+        # the proposal refined three ways: FP64 Newton (the workload's own
+        # refinement), the hybrid with its defaults, and the hybrid with far
+        # steps of FP64 accuracy down to 2e-3 (grid starts are coarse)
+        t0 = time.perf_counter()
         rp = K.newton_search(cfg, pc, None, K.GPUType.NVIDIA, "Float64", Op_p, g_p)
+        t_rp = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rh = newton_search_hybrid(cfg, pc, Op_p, g_p)
+        t_h = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rh2 = newton_search_hybrid(cfg, pc, Op_p, g_p, K.api.HybridConfig(far_step=2e-3))
+        t_h2 = time.perf_counter() - t0
+        growing = bool(r64.converged and r64.gamma > 1e-4)
+        a = polish(K, cfg, pc, r64.Omega_p, r64.gamma) if growing else None
+
+        def same_as_scan(r):
+            if not (growing and r.converged):
+                return False, None
+            b = polish(K, cfg, pc, r.Omega_p, r.gamma)
+            return abs(a[0] - b[0]) <= 1e-10 and abs(a[1] - b[1]) <= 1e-10, b
+
+        same, _ = same_as_scan(rp)
+        same_h, b = same_as_scan(rh)
+        same_h2, _ = same_as_scan(rh2)
         pc.close()
         rows.append({"n_zang": sp.n_zang, "q1": sp.q1, "m": sp.m, "growing_mode": growing,
-                     "same_root": same, "start_equals_scan_argmin": (Op_p, g_p) == (Op0, g0),
+                     "same_root": same, "same_root_hybrid": same_h,
+                     "same_root_hybrid_far_2e-3": same_h2,
+                     "start_equals_scan_argmin": (Op_p, g_p) == (Op0, g0),
+                     "proposal_dets": used,
                      "plain_fp64_s": s.n_Op * s.n_gamma * t_fp64_det + t_n64,
-                     "mixed_scan_s": t_scan_mx, "learned_s": t_learned,
+                     "mixed_scan_s": t_scan_mx, "learned_s": t_prop + t_rp,
+                     "learned_hybrid_s": t_prop + t_h, "learned_hybrid_far_s": t_prop + t_h2,
                      "Omega_p": r64.Omega_p, "gamma": r64.gamma,
                      "scan_start": [Op0, g0], "proposal_start": [Op_p, g_p],
                      "fp64_from_proposal": [rp.Omega_p, rp.gamma, bool(rp.converged)],
                      "hybrid": [rh.Omega_p, rh.gamma, bool(rh.converged), rh.mixed_evals,
                                 rh.fp64_evals, rh.anchored_evals],
+                     "hybrid_far_2e-3": [rh2.Omega_p, rh2.gamma, bool(rh2.converged),
+                                         rh2.mixed_evals, rh2.fp64_evals, rh2.anchored_evals],
                      "polished_scan_root": a, "polished_hybrid_root": b})
     grow = [r for r in rows if r["growing_mode"]]
     ok = [r for r in grow if r["same_root"]]
+    rate = lambda key: (len([r for r in grow if r[key]]) / len(grow)) if grow else None
     mean = lambda k, rs: float(np.mean([r[k] for r in rs])) if rs else None
     mlp.close()
     return {"models": n_models, "model_seed": 7, "size": "default (NR=501 Ne=51 N_alpha=301 l=+-100)",
@@ -645,11 +666,19 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
                          "epochs": 300, "loss_first_last": [float(hist[0]), float(hist[-1])]},
             "same_root_rule": "both roots polished by 2 FP64 Newton steps, then |dOmega_p|, "
                               "|dgamma| <= 1e-10",
+            "refinement": "success_rate: proposal refined by FP64 Newton (the workload's "
+                          "refinement); also by the hybrid Newton (defaults) and by the hybrid "
+                          "with far_step 2e-3",
             "with_growing_mode": len(grow), "same_root_within_1e-10": len(ok),
             "success_rate": len(ok) / len(grow) if grow else None,
+            "success_rate_hybrid": rate("same_root_hybrid"),
+            "success_rate_hybrid_far_2e-3": rate("same_root_hybrid_far_2e-3"),
             "mean_time_to_root_s": {"plain_fp64 (scan at the measured FP64 det time)":
                                     mean("plain_fp64_s", grow),
-                                    "learned_proposal_then_hybrid": mean("learned_s", grow)},
+                                    "learned_proposal_then_fp64_newton": mean("learned_s", grow),
+                                    "learned_proposal_then_hybrid": mean("learned_hybrid_s", grow),
+                                    "learned_proposal_then_hybrid_far_2e-3":
+                                        mean("learned_hybrid_far_s", grow)},
             "per_model": rows}
 
 
