@@ -107,6 +107,9 @@ int ensure_ws(kls_ctx* c, int n) {
 
 // One launch sequence for n (<= ws) omegas already in c->d_omega.
 int run_batch(kls_ctx* c, int n, int mode, bool export_M) {
+  KlsRange range(mode == KLS_MODE_FP64 ? "kls det batch (FP64)"
+                 : mode == KLS_MODE_MIXED ? "kls det batch (split-BF16)"
+                                          : "kls det batch (anchored)");
   int r;
   const int splits = c->splits;
   if (mode != KLS_MODE_FP64 && mode != KLS_MODE_MIXED && mode != KLS_MODE_ANCHORED)
@@ -310,6 +313,7 @@ int kls_set_stream(kls_ctx* c, void* s) {
 }
 
 int kls_precompute(kls_ctx* c) {
+  KlsRange range("kls_precompute");
   if (!c) return KLS_ERR_CONFIG;
   KLS_CK(c, cudaSetDevice(c->device));
   int r;
@@ -476,6 +480,7 @@ int kls_build_M(kls_ctx* c, double wr, double wi, int mode, double* M) {
 }
 
 int kls_set_anchor(kls_ctx* c, double wr, double wi, double* det_ri) {
+  KlsRange range("kls_set_anchor");
   int r = check_ready(c);
   if (r) return r;
   if (!std::isfinite(wr) || !std::isfinite(wi))
@@ -505,6 +510,7 @@ int kls_set_anchor(kls_ctx* c, double wr, double wi, double* det_ri) {
 
 int kls_scan(kls_ctx* c, const kls_scan_cfg* sc, double* det_grid, double* log_abs_grid,
              double* Op0, double* g0) {
+  KlsRange range("kls_scan");
   int r = check_ready(c);
   if (r) return r;
   if (!sc || sc->n_Op < 1 || sc->n_gamma < 1 || !det_grid)
@@ -540,6 +546,7 @@ int kls_scan(kls_ctx* c, const kls_scan_cfg* sc, double* det_grid, double* log_a
 
 int kls_newton(kls_ctx* c, double Op_init, double g_init, const kls_newton_cfg* nc,
                kls_newton_result* res, double* history) {
+  KlsRange range("kls_newton");
   int r = check_ready(c);
   if (r) return r;
   if (!nc || !res || nc->max_iter < 1) return kls_fail(c, KLS_ERR_CONFIG, "bad Newton arguments");
@@ -617,6 +624,7 @@ int kls_newton(kls_ctx* c, double Op_init, double g_init, const kls_newton_cfg* 
 int kls_newton_hybrid(kls_ctx* c, double Op_init, double g_init, const kls_newton_cfg* nc,
                       const kls_hybrid_cfg* hc, kls_newton_result* res, int32_t* evals,
                       double* history) {
+  KlsRange range("kls_newton_hybrid");
   int r = check_ready(c);
   if (r) return r;
   if (!nc || !hc || !res || hc->mixed_max_iter < 0 || hc->fp64_max_iter < 1 ||
@@ -896,6 +904,7 @@ int time_contraction(kls_ctx* c, int mode, int n, double* ms) {
 }  // namespace
 
 int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
+  KlsRange range("kls_autotune");
   int r = check_ready(c);
   if (r) return r;
   if (mode != KLS_MODE_FP64 && mode != KLS_MODE_MIXED)

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <string>
 #include "kls.h"
@@ -233,3 +234,12 @@ void kls_tm_describe(const kls_ctx* c, const kls_mixed_tm* t, unsigned long long
 int kls_tm_multi_launch(cudaStream_t st, const kls_mdesc* d_md, const kls_tm_model* d_tm,
                         const int2* d_pairs, int n_pairs, const int4* d_items, int n_items,
                         int64_t max_K_pad, int max_Npad, int* d_err);
+
+// NVTX range for the lifetime of a scope (profilers show the library's
+// stages by name; without a tool attached a push/pop is a no-op call)
+struct KlsRange {
+  explicit KlsRange(const char* name) { nvtxRangePushA(name); }
+  ~KlsRange() { nvtxRangePop(); }
+  KlsRange(const KlsRange&) = delete;
+  KlsRange& operator=(const KlsRange&) = delete;
+};
