@@ -185,6 +185,10 @@ int kls_export_W(kls_ctx* ctx, int il0, int nl, double* W_ri);
  * determinant (a non-finite table row or weight) returns KLS_ERR_NONFINITE. */
 int kls_det_batch(kls_ctx* ctx, const double* omega_ri, int n, int mode,
                   double* det_ri, double* log_abs);
+/* compute_determinant for one omega (MatrixBuilder.jl:197): det_re, det_im
+ * and log_abs (may be NULL); the same launch sequence as a batch of one.   */
+int kls_det(kls_ctx* ctx, double omega_re, double omega_im, int mode, double* det_re,
+            double* det_im, double* log_abs);
 /* Same with device buffers on the context's stream; no host synchronisation.*/
 int kls_det_batch_device(kls_ctx* ctx, const double* d_omega_ri, int n, int mode,
                          double* d_det_ri, double* d_log_abs);

@@ -134,6 +134,7 @@ SIGNATURES = {
     "kls_det_batch_device": (C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
     "kls_build_M": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _D]),
     "kls_set_anchor": (C.c_int, [_P, C.c_double, C.c_double, _D]),
+    "kls_det": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _D, _D, _D]),
     "kls_set_f64_form": (C.c_int, [_P, C.c_int]),
     "kls_scan": (C.c_int, [_P, C.POINTER(kls_scan_cfg), _D, _D, _D, _D]),
     "kls_newton": (C.c_int, [_P, C.c_double, C.c_double, C.POINTER(kls_newton_cfg),

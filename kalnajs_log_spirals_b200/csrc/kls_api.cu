@@ -431,6 +431,19 @@ int kls_det_batch(kls_ctx* c, const double* omega_ri, int n, int mode, double* d
   return det_batch_host(c, omega_ri, n, mode, det_ri, log_abs);
 }
 
+int kls_det(kls_ctx* c, double wr, double wi, int mode, double* det_re, double* det_im,
+            double* log_abs) {
+  int r = check_ready(c);
+  if (r) return r;
+  if (!det_re || !det_im) return kls_fail(c, KLS_ERR_CONFIG, "bad arguments to kls_det");
+  const double om[2] = {wr, wi};
+  double d[2];
+  if ((r = det_batch_host(c, om, 1, mode, d, log_abs))) return r;
+  *det_re = d[0];
+  *det_im = d[1];
+  return KLS_OK;
+}
+
 int kls_det_batch_device(kls_ctx* c, const double* d_omega, int n, int mode, double* d_det,
                          double* d_log_abs) {
   int r = check_ready(c);

@@ -127,6 +127,17 @@ def test_M_and_det_3m_form(case):
     assert np.array_equal(a, b)
 
 
+def test_single_omega_entry_point(case):
+    """kls_det (one omega) is the batch of one: same bits, same log|det|."""
+    import ctypes as C
+    name, ref, pc = case
+    w = complex(ref["omegas"][0])
+    dr, di, la = C.c_double(), C.c_double(), C.c_double()
+    pc.ctx.call("kls_det", w.real, w.imag, K.KLS_MODE_FP64, C.byref(dr), C.byref(di), C.byref(la))
+    d, l = K.compute_determinant_batched(np.array([w]), pc, log_abs=True)
+    assert complex(dr.value, di.value) == d[0] and la.value == l[0]
+
+
 def test_batch_composition_is_bitwise_stable(case):
     name, ref, pc = case
     om = np.array([0.88 + 0.12j, 0.7 + 0.2j, 0.91 + 0.02j, 1.3 + 0.4j] * 5)
