@@ -12,13 +12,17 @@ plain FP64 form.  One step = one Newton finite-difference triple
           omegas, D2H of dets and log|det| inside the timed region)
 
 Also reported: roofline of the contraction kernel (algorithmic FLOPs
-8 N_alpha^2 K per determinant against an in-run cuBLAS DGEMM peak), Newton
-time-to-root from the reference start, precompute time, the CPU baseline (the
-oracle's BLAS form timed on the host cores on a bounded sample) and SM clocks
-sampled during the timed region.
+8 N_alpha^2 K per determinant against an in-run cuBLAS DGEMM peak, and the
+DMMA work the chosen 4M or 3M form issues), the split-BF16 form, Newton
+time-to-root from the reference start (plain FP64 against the hybrid: split-
+BF16 secant steps, one FP64 anchor, anchored finish), parity against the
+default-size oracle fixture, precompute time, the CPU baseline (the oracle's
+BLAS form, one whole determinant on the host cores) and SM clocks sampled
+during the timed region.
 
---impl reference times the reference algorithm's CPU form (oracle port, one
-ZGEMM per harmonic + LAPACK LU, all host threads) on the same metric.
+--impl reference times the reference algorithm's CPU form (oracle port: the
+oracle builds its own table, then one ZGEMM per harmonic + LAPACK LU per
+whole determinant, all host threads) on the same metric.
 Multi-GPU (torchrun): independent replicas, each rank evaluating its own
 omegas ("replicas only"; the path needs no collective).
 """
