@@ -735,14 +735,18 @@ def uneven_batch(args, K, P, local, sync):
     info = mb.info()
     mb.close()
     n_det = len(specs) * n_pts
-    # one column model by model through each context's own batch call
-    sync()
-    t0 = time.perf_counter()
+    # one column model by model through each context's own batch call; each
+    # context is released after its column (a context's own split-BF16
+    # partials for B omegas are GBs at the default size, 16 would not fit
+    # beside the tables)
+    t_seq = 0.0
     for pc, o in zip(pcs, om):
         dev = K.to_device(pc, K.GPUType.NVIDIA, "Float32")
+        sync()
+        t0 = time.perf_counter()
         K.compute_determinant_batched(o[:nG], pc, dev, batch_size=B)
-    t_seq = time.perf_counter() - t0
-    for pc in pcs:
+        sync()
+        t_seq += time.perf_counter() - t0
         pc.close()
     rate = n_det / (dev_ms * 1e-3)
     # the smallest batched model against the oracle (its own table, built on
