@@ -14,7 +14,7 @@
 constexpr int KLS_TILE = 64;
 constexpr int KLS_KROW_ALIGN = 64;   // K rows padded to a multiple of this
 // TMEM-operand split-BF16 form: FP32 weight variants per k pair (float4 each)
-constexpr int KLS_TM_WVAR = 3;
+constexpr int KLS_TM_WVAR = 2;
 
 // Per-orbit scalar fields written by the orbit kernel (struct of arrays,
 // each NPh doubles, orbit index p = iR + NR*ie as in the reference).

@@ -33,10 +33,11 @@
 //   2       TMEM allocation / release (512 columns: D at [0, Npad), A stages
 //           of 64 columns at the top: three for Npad <= 320, else two)
 //   3       weights ring: bulk copies of the FP32 w(omega) of the CTA's omega,
-//           three pre-signed coefficient pairs per two k
-//   4..11   producers, 2 per TMEM lane quadrant (Re / Im coefficient halves);
-//           lanes 0..63 hold rows (a, r), lanes 64..127 rows (a, i), so each
-//           warp's formula is uniform, evaluated in packed f32x2 arithmetic
+//           two pre-signed coefficient pairs per two k
+//   4..11   producers, 2 per TMEM lane quadrant (halves of the stage's k);
+//           lane 2a holds row (a, r), lane 2a + 1 row (a, i); each lane forms
+//           one component of U (packed f32x2 arithmetic) and takes the other
+//           half of its row from its partner lane
 //   12..19  drain, 2 per lane quadrant (halves of the D columns): TMEM ->
 //           FP64 partial (stores for the first chunk, L2 reductions after)
 // Every wait is bounded (the context's wait limit, 2 s by default); a wait
@@ -62,7 +63,7 @@ constexpr int TM_NDRAIN = 8;           // drain warps 12..19
 constexpr int TM_TMEM_COLS = 512;
 constexpr int TM_YTILE = TM_AB * TM_KB * 2;   // 4 KB: 64 rows x 64 B
 constexpr int TM_WVAR = KLS_TM_WVAR;          // coefficient variants per k pair
-constexpr int TM_WBYTES = TM_KB / 2 * TM_WVAR * 16;   // 768 B: weights of one stage
+constexpr int TM_WBYTES = TM_KB / 2 * TM_WVAR * 16;   // 512 B: weights of one stage
 
 __host__ __device__ constexpr int tm_astages(int Npad) { return Npad <= 320 ? 3 : 2; }
 
@@ -268,15 +269,20 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
     }
   } else if (warp >= 4 && warp < 4 + TM_NPROD) {
     // ---------------- producers: A rows of this CTA's 64 alphas into TMEM
-    const int pw = warp - 4, q = pw & 3, h = pw >> 2;
+    const int pw = warp - 4, q = pw & 3, kh = pw >> 2;
     const int l = 32 * q + lane;               // TMEM lane = A row
-    const int p = q >> 1, al = l & 63;         // rows (a, r): lanes 0..63, (a, i): 64..127
-    // half 0 (Re W columns): (a, r) <- Re U, (a, i) <- Im U; half 1 (Im W
-    // columns): (a, r) <- -Im U, (a, i) <- Re U; with U = w conj(W) each is
-    // c1 * ReW + c2 * ImW, (c1, c2) = (wr, wi), (wi, -wr) or (-wi, wr): the
-    // weights ring holds the three variants, this warp reads one
-    const int var = h == p ? 0 : (p == 1 ? 1 : 2);
-    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16) + acol + (uint32_t)(h * 16);
+    const int al = l >> 1, p = l & 1;          // rows (a, r) at lane 2a, (a, i) at 2a + 1
+    // With U = w conj(W): row (a, r) is [Re U | -Im U] and (a, i) is
+    // [Im U | Re U] over the halves (Re W columns | Im W columns) of the
+    // stage.  Each lane forms its own component over this warp's 16 k
+    // (k pairs j = 8 kh .. 8 kh + 7), c1 ReW + c2 ImW with (c1, c2) = (wr, wi)
+    // (Re U, lane 2a) or (wi, -wr) (Im U, lane 2a + 1), for half 0, and takes
+    // its half-1 values from its partner lane, negated for the (a, r) row
+    // (the split of -x is the negated split of x, so the bits are those the
+    // formula would give).
+    const int var = p;                         // weight variant 0 or 1
+    const uint32_t neg = p ? 0u : 0x80008000u; // sign bits of a BF16 pair
+    const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16) + acol + (uint32_t)(kh * 8);
     const bool skip_one = P.fault_skip && leader && tile_pair == 0 && split == 0 && pw == 0;
     for (int i = 0; i < nkb; ++i) {
       const int s = i % TM_STAGES, as = i % NA, ws = i % TM_WSTAGES;
@@ -289,10 +295,11 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
       tc_fence_after();
       // (c1 pair, c2 pair) of k = 2j, 2j + 1 at float4 number TM_WVAR j + var
       const float4* wz = reinterpret_cast<const float4*>(wring + ws * TM_WBYTES) + var;
-      uint32_t hi[16], lo[16];
+      uint32_t hi[8], lo[8], hi1[8], lo1[8];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
+      for (int cc = 0; cc < 2; ++cc) {
         // 16-byte chunk c of the alpha's table rows: k = 8c .. 8c + 7
+        const int c = 2 * kh + cc;
         const uint32_t off = sw64_off(al, c);
         const uint4 Rh = *reinterpret_cast<const uint4*>(y_tile(s, 0, 0) + off);
         const uint4 Ih = *reinterpret_cast<const uint4*>(y_tile(s, 0, 1) + off);
@@ -305,11 +312,18 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
           const uint64_t wi = f2_add(f2_bf16x2((&Ih.x)[e]), f2_bf16x2((&Il.x)[e]));
           const float4 cw = wz[TM_WVAR * j];
           const uint64_t v = f2_fma(f2_pack(cw.x, cw.y), wr, f2_mul(f2_pack(cw.z, cw.w), wi));
-          hi[j] = pack_split2(v, lo[j]);
+          hi[4 * cc + e] = pack_split2(v, lo[4 * cc + e]);
         }
       }
-      TMEM_ST16(tl + (uint32_t)(as * 64), hi);
-      TMEM_ST16(tl + (uint32_t)(as * 64 + 32), lo);
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        hi1[t] = __shfl_xor_sync(0xffffffffu, hi[t], 1) ^ neg;
+        lo1[t] = __shfl_xor_sync(0xffffffffu, lo[t], 1) ^ neg;
+      }
+      TMEM_ST8(tl + (uint32_t)(as * 64), hi);
+      TMEM_ST8(tl + (uint32_t)(as * 64 + 32), lo);
+      TMEM_ST8(tl + (uint32_t)(as * 64 + 16), hi1);
+      TMEM_ST8(tl + (uint32_t)(as * 64 + 48), lo1);
       asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       tc_fence_before();
       __syncwarp();
@@ -409,18 +423,17 @@ mixed_tm_multi_kernel(const kls_tm_model* __restrict__ md, const int4* __restric
   tm_body(&d.tb_h, &d.tb_l, &d.ty_h, &d.ty_l, P, it.y, it.z, d.wt32, d.part, err);
 }
 
-// FP32 weights as the producers read them: for k = 2j, 2j + 1 three float4
-// (c1 pair, c2 pair) = (wr, wi), (wi, -wr), (-wi, wr); negation is exact, so
-// every variant rounds like the plain FP32 weight
+// FP32 weights as the producers read them: for k = 2j, 2j + 1 two float4
+// (c1 pair, c2 pair) = (wr, wi) and (wi, -wr); negation is exact, so each
+// variant rounds like the plain FP32 weight
 __device__ __forceinline__ void tm_weight_variants(int64_t K_pad, const double2* __restrict__ wt,
                                                    float4* __restrict__ out) {
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < K_pad / 2;
        j += (int64_t)gridDim.x * blockDim.x) {
     const double2 a = wt[2 * j], b = wt[2 * j + 1];
     const float r0 = (float)a.x, i0 = (float)a.y, r1 = (float)b.x, i1 = (float)b.y;
-    out[3 * j] = make_float4(r0, r1, i0, i1);
-    out[3 * j + 1] = make_float4(i0, i1, -r0, -r1);
-    out[3 * j + 2] = make_float4(-i0, -i1, r0, r1);
+    out[2 * j] = make_float4(r0, r1, i0, i1);
+    out[2 * j + 1] = make_float4(i0, i1, -r0, -r1);
   }
 }
 
@@ -443,13 +456,13 @@ __global__ void tm_multi_reduce_kernel(const kls_mdesc* __restrict__ md,
   const size_t plane = (size_t)d.Na_pad * 128;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
     const int b = e / Na, a = e % Na;
-    const int at = a / TM_AB, la = a % TM_AB;    // rows (a, r) at la, (a, i) at 64 + la
+    const int at = a / TM_AB, la = 2 * (a % TM_AB);   // rows (a, r) at 2a, (a, i) at 2a + 1
     const double* src =
         d.mpart + (size_t)(pz.y * tiles_a + at) * d.msplits * plane + (size_t)b * 128 + la;
     double sr = 0.0, si = 0.0;
     for (int s = 0; s < d.msplits; ++s) {
       sr += src[(size_t)s * plane];
-      si += src[(size_t)s * plane + TM_AB];
+      si += src[(size_t)s * plane + 1];
     }
     const double n = d.Nk[a];
     const double mr = __dmul_rn(__dmul_rn(sr, d.G), n), mi = __dmul_rn(__dmul_rn(si, d.G), n);
@@ -457,7 +470,7 @@ __global__ void tm_multi_reduce_kernel(const kls_mdesc* __restrict__ md,
   }
 }
 
-// FP32 weight variants, [omega][K_pad / 2][3] float4
+// FP32 weight variants, [omega][K_pad / 2][TM_WVAR] float4
 __global__ void tm_weights32_kernel(int64_t K_pad, const double2* __restrict__ wt,
                                     float4* __restrict__ wt32) {
   const int z = blockIdx.y;
@@ -465,7 +478,7 @@ __global__ void tm_weights32_kernel(int64_t K_pad, const double2* __restrict__ w
 }
 
 // split sum, * G * N(a), I - M: partial [tile][split][b][A row], A row
-// a_local (Re) or 64 + a_local (Im)
+// 2 a_local (Re) or 2 a_local + 1 (Im)
 __global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, double G,
                                  const double* __restrict__ Nk, const double* __restrict__ part,
                                  double2* __restrict__ A, double2* __restrict__ Mout,
@@ -474,12 +487,12 @@ __global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, doub
   const size_t plane = (size_t)Npad * 128;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Na * Na; e += gridDim.x * blockDim.x) {
     const int b = e / Na, a = e % Na;
-    const int at = a / TM_AB, la = a % TM_AB;    // rows (a, r) at la, (a, i) at 64 + la
+    const int at = a / TM_AB, la = 2 * (a % TM_AB);   // rows (a, r) at 2a, (a, i) at 2a + 1
     const double* src = part + (size_t)(z * tiles_a + at) * splits * plane + (size_t)b * 128 + la;
     double sr = 0.0, si = 0.0;
     for (int s = 0; s < splits; ++s) {
       sr += src[(size_t)s * plane];
-      si += src[(size_t)s * plane + TM_AB];
+      si += src[(size_t)s * plane + 1];
     }
     const double n = Nk[a];
     double mr = __dmul_rn(__dmul_rn(sr, G), n), mi = __dmul_rn(__dmul_rn(si, G), n);
@@ -517,7 +530,7 @@ struct kls_mixed_tm {
   int chunk = TM_CHUNK;         // stages per FP32 accumulation chunk
   double* part = nullptr;       // [n tiles][splits][Npad][128]
   size_t part_elems = 0;
-  float2* wt32 = nullptr;       // [n][K_pad / 2][3] float4 weight variants
+  float2* wt32 = nullptr;       // [n][K_pad / 2][TM_WVAR] float4 weight variants
   size_t wt32_elems = 0;
 };
 

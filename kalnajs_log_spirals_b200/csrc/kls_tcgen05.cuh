@@ -189,6 +189,13 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
       "r"(r[15])                                                                                 \
       : "memory")
 
+#define TMEM_ST8(taddr, r)                                                                       \
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(  \
+                   taddr),                                                                       \
+               "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),      \
+               "r"(r[7])                                                                         \
+               : "memory")
+
 __device__ __forceinline__ float bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
 __device__ __forceinline__ float bf_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
 // error-free split of two FP32 values into BF16 high parts (returned, a in
