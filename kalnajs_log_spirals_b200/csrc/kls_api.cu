@@ -971,6 +971,10 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
       fdef = kls_choose_splits(c);
     }
     std::vector<int> cand = {std::max(1, fdef / 2), fdef, 2 * fdef, 3 * fdef};
+    // the TMEM-operand form's default is the number of resident CTA pairs:
+    // fewer splits leave a single omega (Newton's evaluations) on part of a
+    // wave, so only whole multiples of it are candidates
+    if (mixed && form == KLS_MIXED_TMEM) cand = {fdef, 2 * fdef, 3 * fdef};
     for (int& s : cand) s = std::max(1, std::min(s, max_s));
     std::sort(cand.begin(), cand.end());
     cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
