@@ -788,8 +788,8 @@ def uneven_batch(args, K, P, local, sync):
         "maps_saved": args.uneven_out or None,
         "oracle_check": oracle_check,
         "batch_launch": {"items": info["n_items"], "ctas": info["grid"],
-                         "schedule": ["persistent round robin", "one CTA (pair) per item"][
-                             info["schedule"]],
+                         "schedule": ["persistent round robin", "one CTA (pair) per item",
+                                      "one launch per model"][info["schedule"]],
                          "schedule_pass_ms": info["schedule_ms"],
                          "graph_replay": bool(info["graph"]),
                          "kernels_per_pass": info["launches_per_replay"]},

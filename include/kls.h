@@ -316,9 +316,12 @@ typedef struct kls_multi_info {
     int32_t launches_per_replay;  /* kernels in one pass                      */
     int64_t replays;              /* passes so far                            */
     double  last_ms;              /* device time of the last pass (ms)        */
-    int32_t schedule;             /* mixed form: 0 persistent round robin,
-                                     1 one CTA (pair) per item (the faster of the two
-                                     passes timed at creation)                */
+    int32_t schedule;             /* mixed form, the faster of two passes timed
+                                     at creation: one-CTA / pair kernels: 0
+                                     persistent round robin or 1 one CTA per
+                                     item; TMEM-operand form: 1 one launch with
+                                     a CTA pair per item or 2 one launch per
+                                     model                                    */
     double  schedule_ms[2];       /* those two passes (ms)                    */
 } kls_multi_info;
 int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, kls_multi** out);

@@ -231,9 +231,12 @@ int kls_tm_reduce(kls_ctx* c, kls_mixed_tm* t, int n, bool export_M, const doubl
 kls_mixed_tm* kls_mixed_tm_state(const kls_ctx* c, unsigned long long* wait_ns);
 void kls_tm_describe(const kls_ctx* c, const kls_mixed_tm* t, unsigned long long wait_ns,
                      int batch, kls_tm_model* out);
+// per_model: one launch of the single-model kernel per model (h_tm: host
+// copies of the descriptors) instead of one launch over every item
 int kls_tm_multi_launch(cudaStream_t st, const kls_mdesc* d_md, const kls_tm_model* d_tm,
                         const int2* d_pairs, int n_pairs, const int4* d_items, int n_items,
-                        int64_t max_K_pad, int max_Npad, int* d_err);
+                        int64_t max_K_pad, int max_Npad, int* d_err, const kls_tm_model* h_tm,
+                        int n_models, bool per_model);
 
 // NVTX range for the lifetime of a scope (profilers show the library's
 // stages by name; without a tool attached a push/pop is a no-op call)

@@ -683,14 +683,39 @@ void kls_tm_describe(const kls_ctx* c, const kls_mixed_tm* t, unsigned long long
 
 int kls_tm_multi_launch(cudaStream_t st, const kls_mdesc* d_md, const kls_tm_model* d_tm,
                         const int2* d_pairs, int n_pairs, const int4* d_items, int n_items,
-                        int64_t max_K_pad, int max_Npad, int* d_err) {
+                        int64_t max_K_pad, int max_Npad, int* d_err, const kls_tm_model* h_tm,
+                        int n_models, bool per_model) {
   cudaError_t e;
   const int wblocks = (int)std::min<int64_t>((max_K_pad + 255) / 256, 1024);
   tm_multi_weights32_kernel<<<dim3(wblocks, n_pairs), 256, 0, st>>>(d_md, d_pairs);
   if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   if ((e = tm_set_smem_limits()) != cudaSuccess) return (int)e;
-  mixed_tm_multi_kernel<<<2 * n_items, TM_THREADS, tm_smem(max_Npad), st>>>(d_tm, d_items, d_err);
-  if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  if (per_model) {
+    // one launch of the single-model kernel per model (tensor maps as
+    // kernel parameters): the same body and parameters, hence the same bits
+    for (int i = 0; i < n_models; ++i) {
+      const kls_tm_model& d = h_tm[i];
+      TmParams P{};
+      P.Npad = d.Npad;
+      P.tiles_a = d.tiles_a;
+      P.n_tiles = d.n_tiles;
+      P.splits = d.splits;
+      P.kb_per_split = d.kb_per_split;
+      P.nkb_total = d.nkb_total;
+      P.K_pad = d.K_pad;
+      P.wait_ns = d.wait_ns;
+      P.fault_skip = 0;
+      P.chunk = d.chunk;
+      const dim3 grid((unsigned)(2 * ((d.n_tiles + 1) / 2)), (unsigned)d.splits);
+      mixed_tm_kernel<<<grid, TM_THREADS, tm_smem(d.Npad), st>>>(d.tb_h, d.tb_l, d.ty_h, d.ty_l,
+                                                                 P, d.wt32, d.part, d_err);
+      if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+    }
+  } else {
+    mixed_tm_multi_kernel<<<2 * n_items, TM_THREADS, tm_smem(max_Npad), st>>>(d_tm, d_items,
+                                                                               d_err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
+  }
   tm_multi_reduce_kernel<<<dim3(256, n_pairs), 256, 0, st>>>(d_md, d_pairs);
   return (int)cudaGetLastError();
 }

@@ -40,7 +40,8 @@ struct kls_multi {
   std::vector<kls_item> items;
   std::vector<kls_item> list;       // mixed: items in locality order
   std::vector<int> starts;          // mixed: per-CTA item ranges
-  int schedule = 0;                 // mixed: 0 persistent round robin, 1 one CTA per item
+  int schedule = 0;                 // mixed: 0 persistent round robin, 1 one CTA (pair) per
+                                    // item, 2 (TMEM form) one launch per model
   bool tm = false;                  // mixed: every model in the TMEM-operand form
   std::vector<kls_tm_model> tmd;    // its per-model descriptors
   std::vector<int4> tm_items;       // (model, tile pair, split): one CTA pair each
@@ -221,7 +222,8 @@ int launch_batch(kls_multi* m) {
     r = kls_multi_launch_f64_weights(m->stream, m->d_md, m->d_pairs, np, m->max_K_pad);
     if (!r && m->tm)
       r = kls_tm_multi_launch(m->stream, m->d_md, m->d_tm, m->d_pairs, np, m->d_tm_items,
-                              (int)m->tm_items.size(), m->max_K_pad, m->max_Npad, m->d_err);
+                              (int)m->tm_items.size(), m->max_K_pad, m->max_Npad, m->d_err,
+                              m->tmd.data(), (int)m->tmd.size(), m->schedule == 2);
     else if (!r)
       r = kls_multi_launch_mixed(m->stream, m->d_md, m->d_pairs, np, m->d_items, m->d_starts,
                                  m->grid, m->max_K_pad, m->d_err);
@@ -517,9 +519,17 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
       return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (items)"));
     if ((r = eager_pass(m, nullptr))) return bail(r);
   } else if (m->tm) {
-    float ms = 0.f;
-    if ((r = eager_pass(m, nullptr)) || (r = eager_pass(m, &ms))) return bail(r);
-    m->schedule_ms[0] = m->schedule_ms[1] = ms;     // one schedule: a CTA pair per item
+    // two schedules, timed: one launch with a CTA pair per (model, tile pair,
+    // split) item, or one launch of the single-model kernel per model; both
+    // run the same body on the same items, so the bits are the same
+    if ((r = eager_pass(m, nullptr))) return bail(r);
+    for (int p = 0; p < 2; ++p) {
+      float ms = 0.f;
+      m->schedule = p ? 2 : 1;
+      if ((r = eager_pass(m, &ms))) return bail(r);
+      m->schedule_ms[p] = ms;
+    }
+    m->schedule = m->schedule_ms[1] < m->schedule_ms[0] ? 2 : 1;
   } else {
     // schedule tuning: one warm-up pass, then one timed pass per schedule
     if ((r = schedule_items(m, 0)) || (r = eager_pass(m, nullptr))) return bail(r);
@@ -602,7 +612,8 @@ int kls_multi_get_info(const kls_multi* m, kls_multi_info* out) {
   out->replays = m->replays;
   out->last_ms = m->last_ms;
   // kernels per replay: weights (+ FP32 copy), contraction, reduction, LU
-  out->launches_per_replay = m->mode == KLS_MODE_FP64 ? 4 : 5;
+  out->launches_per_replay = m->mode == KLS_MODE_FP64 ? 4
+                              : m->schedule == 2 ? 4 + (int32_t)m->tmd.size() : 5;
   out->schedule = m->schedule;
   out->schedule_ms[0] = m->schedule_ms[0];
   out->schedule_ms[1] = m->schedule_ms[1];
