@@ -42,7 +42,13 @@ struct kls_multi {
   std::vector<int> starts;          // mixed: per-CTA item ranges
   int schedule = 0;                 // mixed: 0 persistent round robin, 1 one CTA (pair) per
                                     // item, 2 (TMEM form) one launch per model
-  bool tm = false;                  // mixed: every model in the TMEM-operand form
+  bool tm = false;                  // mixed: some model in the TMEM-operand form
+  bool old = false;                 // mixed: some model in the one-CTA / pair forms
+  std::vector<char> use_tm;         // per model: TMEM-operand form
+  std::vector<int2> pairs_tm, pairs_old;   // (model, omega) pairs of each form
+  int2 *d_pairs_tm = nullptr, *d_pairs_old = nullptr;
+  int tm_schedule = 1;              // TMEM form: 1 one launch over items, 2 one per model
+  double tm_schedule_ms[2] = {0, 0};
   std::vector<kls_tm_model> tmd;    // its per-model descriptors
   std::vector<int4> tm_items;       // (model, tile pair, split): one CTA pair each
   kls_tm_model* d_tm = nullptr;
@@ -117,9 +123,14 @@ constexpr int MIX_BK = 64, MIX_BM = 128, MIX_AB = 64;
 int build_items(kls_multi* m) {
   m->items.clear();
   m->pairs.clear();
+  m->pairs_tm.clear();
+  m->pairs_old.clear();
   for (int i = 0; i < m->n_models; ++i)
-    for (int z = 0; z < m->batch; ++z) m->pairs.push_back(make_int2(i, z));
-  if (m->tm) return KLS_OK;               // items built by build_tm_items
+    for (int z = 0; z < m->batch; ++z) {
+      m->pairs.push_back(make_int2(i, z));
+      (m->use_tm[i] ? m->pairs_tm : m->pairs_old).push_back(make_int2(i, z));
+    }
+  if (m->mode != KLS_MODE_FP64 && !m->old) return KLS_OK;   // TMEM items: build_tm_items
   std::vector<int> order(m->n_models);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -143,6 +154,7 @@ int build_items(kls_multi* m) {
   }
   m->list.clear();
   for (int i : order) {
+    if (m->use_tm[i]) continue;           // in the TMEM-operand launch
     const kls_mdesc& d = m->md[i];
     const int tiles = (2 * d.Na_pad / MIX_BM) * (d.Na_pad / MIX_AB);
     for (int z = 0; z < m->batch; z += d.om_per_item) {
@@ -164,7 +176,7 @@ int build_items(kls_multi* m) {
 // read the same k-range of one table.
 void build_tm_items(kls_multi* m) {
   m->tm_items.clear();
-  std::vector<int> order(m->n_models);
+  std::vector<int> order(m->tmd.size());
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     const kls_tm_model &x = m->tmd[a], &y = m->tmd[b];
@@ -176,8 +188,7 @@ void build_tm_items(kls_multi* m) {
     for (int s = 0; s < d.splits; ++s)
       for (int p = 0; p < pairs; ++p) m->tm_items.push_back(make_int4(i, p, s, 0));
   }
-  m->grid = 2 * (int)m->tm_items.size();
-  m->schedule = 1;
+  m->tm_schedule = 1;
 }
 
 // Mixed form: per-CTA item ranges of the ordered list.  Schedule 0: a
@@ -221,12 +232,12 @@ int launch_batch(kls_multi* m) {
     // the mixed weights are converted from the FP64 weights of the same pass
     r = kls_multi_launch_f64_weights(m->stream, m->d_md, m->d_pairs, np, m->max_K_pad);
     if (!r && m->tm)
-      r = kls_tm_multi_launch(m->stream, m->d_md, m->d_tm, m->d_pairs, np, m->d_tm_items,
-                              (int)m->tm_items.size(), m->max_K_pad, m->max_Npad, m->d_err,
-                              m->tmd.data(), (int)m->tmd.size(), m->schedule == 2);
-    else if (!r)
-      r = kls_multi_launch_mixed(m->stream, m->d_md, m->d_pairs, np, m->d_items, m->d_starts,
-                                 m->grid, m->max_K_pad, m->d_err);
+      r = kls_tm_multi_launch(m->stream, m->d_md, m->d_tm, m->d_pairs_tm, (int)m->pairs_tm.size(),
+                              m->d_tm_items, (int)m->tm_items.size(), m->max_K_pad, m->max_Npad,
+                              m->d_err, m->tmd.data(), (int)m->tmd.size(), m->tm_schedule == 2);
+    if (!r && m->old)
+      r = kls_multi_launch_mixed(m->stream, m->d_md, m->d_pairs_old, (int)m->pairs_old.size(),
+                                 m->d_items, m->d_starts, m->grid, m->max_K_pad, m->d_err);
   }
   if (r) return mcuda(m, (cudaError_t)r, "uneven batch launch");
   r = kls_multi_launch_lu(m->stream, m->d_md, m->d_pairs, np, m->max_Na);
@@ -406,14 +417,17 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
     return bail(mcuda(m, cudaGetLastError(), "cudaMemset"));
 
   m->md.resize(n_models);
+  m->use_tm.assign(n_models, 0);
   if (mode == KLS_MODE_MIXED) {
-    // one kernel for the whole batch: the TMEM-operand form when it is every
-    // model's form, else the one-CTA kernel body
-    m->tm = true;
+    // each model runs its own form's kernel body: the models in the
+    // TMEM-operand form share one contraction launch, the others (one-CTA or
+    // pair form, which return the same bits) share the one-CTA kernel's
     for (int i = 0; i < n_models; ++i) {
       if (!models[i]->mixed && (r = kls_mixed_prepare(models[i])))
         return bail(mfail(m, r, models[i]->err));
-      if (!kls_mixed_tm_state(models[i], nullptr)) m->tm = false;
+      m->use_tm[i] = kls_mixed_tm_state(models[i], nullptr) != nullptr;
+      if (m->use_tm[i]) m->tm = true;
+      else m->old = true;
     }
   }
   for (int i = 0; i < n_models; ++i) {
@@ -441,7 +455,7 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
         return bail(r);
     } else {
       if (!c->mixed && (r = kls_mixed_prepare(c))) return bail(mfail(m, r, c->err));
-      if (m->tm) {
+      if (m->use_tm[i]) {
         // TMEM-operand form: FP32 weight variants and this form's partials
         unsigned long long wns = 0;
         kls_mixed_tm* t = kls_mixed_tm_state(c, &wns);
@@ -507,10 +521,16 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
   const size_t n_it = std::max(m->items.size(), m->list.size());
   if ((r = malloc_buf(m, &m->d_md, m->md.size())) || (r = malloc_buf(m, &m->d_items, n_it)) ||
       (r = malloc_buf(m, &m->d_pairs, m->pairs.size())) ||
+      (r = malloc_buf(m, &m->d_pairs_tm, m->pairs_tm.size())) ||
+      (r = malloc_buf(m, &m->d_pairs_old, m->pairs_old.size())) ||
       (r = malloc_buf(m, &m->d_starts, n_it + 1)))
     return bail(r);
   if (cudaMemcpy(m->d_md, m->md.data(), m->md.size() * sizeof(kls_mdesc), cudaMemcpyHostToDevice) ||
       cudaMemcpy(m->d_pairs, m->pairs.data(), m->pairs.size() * sizeof(int2),
+                 cudaMemcpyHostToDevice) ||
+      cudaMemcpy(m->d_pairs_tm, m->pairs_tm.data(), m->pairs_tm.size() * sizeof(int2),
+                 cudaMemcpyHostToDevice) ||
+      cudaMemcpy(m->d_pairs_old, m->pairs_old.data(), m->pairs_old.size() * sizeof(int2),
                  cudaMemcpyHostToDevice))
     return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (descriptors)"));
   if (mode == KLS_MODE_FP64) {
@@ -518,27 +538,31 @@ int kls_multi_create(kls_ctx* const* models, int n_models, int mode, int batch, 
                    cudaMemcpyHostToDevice) != cudaSuccess)
       return bail(mcuda(m, cudaGetLastError(), "cudaMemcpy (items)"));
     if ((r = eager_pass(m, nullptr))) return bail(r);
-  } else if (m->tm) {
-    // two schedules, timed: one launch with a CTA pair per (model, tile pair,
-    // split) item, or one launch of the single-model kernel per model; both
-    // run the same body on the same items, so the bits are the same
-    if ((r = eager_pass(m, nullptr))) return bail(r);
-    for (int p = 0; p < 2; ++p) {
-      float ms = 0.f;
-      m->schedule = p ? 2 : 1;
-      if ((r = eager_pass(m, &ms))) return bail(r);
-      m->schedule_ms[p] = ms;
-    }
-    m->schedule = m->schedule_ms[1] < m->schedule_ms[0] ? 2 : 1;
   } else {
-    // schedule tuning: one warm-up pass, then one timed pass per schedule
-    if ((r = schedule_items(m, 0)) || (r = eager_pass(m, nullptr))) return bail(r);
-    for (int p = 0; p < 2; ++p) {
-      float ms = 0.f;
-      if ((r = schedule_items(m, p)) || (r = eager_pass(m, &ms))) return bail(r);
-      m->schedule_ms[p] = ms;
+    // schedule tuning, one warm-up pass first.  One-CTA / pair-form models:
+    // a persistent round robin or one CTA per item; TMEM-form models: one
+    // launch with a CTA pair per (model, tile pair, split) item or one launch
+    // of the single-model kernel per model.  Every schedule runs the same
+    // bodies on the same items, so the bits do not depend on the choice.
+    if (m->old && (r = schedule_items(m, 0))) return bail(r);
+    if ((r = eager_pass(m, nullptr))) return bail(r);
+    if (m->old) {
+      for (int p = 0; p < 2; ++p) {
+        float ms = 0.f;
+        if ((r = schedule_items(m, p)) || (r = eager_pass(m, &ms))) return bail(r);
+        m->schedule_ms[p] = ms;
+      }
+      if ((r = schedule_items(m, m->schedule_ms[1] < m->schedule_ms[0] ? 1 : 0))) return bail(r);
     }
-    if ((r = schedule_items(m, m->schedule_ms[1] < m->schedule_ms[0] ? 1 : 0))) return bail(r);
+    if (m->tm) {
+      for (int p = 0; p < 2; ++p) {
+        float ms = 0.f;
+        m->tm_schedule = p ? 2 : 1;
+        if ((r = eager_pass(m, &ms))) return bail(r);
+        m->tm_schedule_ms[p] = ms;
+      }
+      m->tm_schedule = m->tm_schedule_ms[1] < m->tm_schedule_ms[0] ? 2 : 1;
+    }
   }
   if ((r = capture(m))) return bail(r);
   *out = m;
@@ -606,17 +630,25 @@ int kls_multi_get_info(const kls_multi* m, kls_multi_info* out) {
   out->n_models = m->n_models;
   out->batch = m->batch;
   out->mode = m->mode;
-  out->n_items = (int32_t)(m->tm ? m->tm_items.size() : m->items.size());
-  out->grid = m->grid;
+  const bool fp64 = m->mode == KLS_MODE_FP64;
+  out->n_items = (int32_t)((fp64 || m->old ? m->items.size() : 0) + (m->tm ? m->tm_items.size() : 0));
+  out->grid = (fp64 || m->old ? m->grid : 0) + (m->tm ? 2 * (int32_t)m->tm_items.size() : 0);
   out->graph = m->exec ? 1 : 0;
   out->replays = m->replays;
   out->last_ms = m->last_ms;
   // kernels per replay: weights (+ FP32 copy), contraction, reduction, LU
-  out->launches_per_replay = m->mode == KLS_MODE_FP64 ? 4
-                              : m->schedule == 2 ? 4 + (int32_t)m->tmd.size() : 5;
-  out->schedule = m->schedule;
-  out->schedule_ms[0] = m->schedule_ms[0];
-  out->schedule_ms[1] = m->schedule_ms[1];
+  // FP64: weights, contraction, reduction, LU; mixed: FP64 weights, per form
+  // (FP32 weights, contraction launch(es), reduction), LU
+  out->launches_per_replay =
+      fp64 ? 4
+           : 2 + (m->old ? 3 : 0) +
+                 (m->tm ? 2 + (m->tm_schedule == 2 ? (int32_t)m->tmd.size() : 1) : 0);
+  // the one-CTA / pair forms' schedule when the batch has such models, else
+  // the TMEM-operand form's
+  const bool tm_only = !fp64 && m->tm && !m->old;
+  out->schedule = tm_only ? m->tm_schedule : m->schedule;
+  out->schedule_ms[0] = tm_only ? m->tm_schedule_ms[0] : m->schedule_ms[0];
+  out->schedule_ms[1] = tm_only ? m->tm_schedule_ms[1] : m->schedule_ms[1];
   return KLS_OK;
 }
 

@@ -45,7 +45,8 @@ def pcs(lib_path):
 
 @pytest.mark.parametrize("Tgpu,form", [("Float64", None), ("Float64", "3m"),
                                        ("Float32", _lib.KLS_MIXED_ONE_CTA),
-                                       ("Float32", _lib.KLS_MIXED_TMEM)])
+                                       ("Float32", _lib.KLS_MIXED_TMEM),
+                                       ("Float32", "mixed forms")])
 def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu, form):
     n = 7                                  # passes of 3: 3 + 3 + 1
     om = np.stack([omegas(n, 10 + i) * (m / 2) for i, (m, *_) in enumerate(MODELS)])
@@ -54,6 +55,11 @@ def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu, form):
         dev = K.to_device(pc, K.GPUType.NVIDIA, Tgpu)
         if form == "3m":
             pc.ctx.call("kls_set_f64_form", _lib.KLS_F64_3M)
+        elif form == "mixed forms":
+            # TMEM-operand form and the older forms side by side in one batch
+            pc.ctx.call("kls_set_mixed_form",
+                        [_lib.KLS_MIXED_TMEM, _lib.KLS_MIXED_ONE_CTA, _lib.KLS_MIXED_TMEM,
+                         _lib.KLS_MIXED_PAIR][len(singles)])
         elif form is not None:
             # the batch runs this form's kernel body when it is every model's form
             pc.ctx.call("kls_set_mixed_form", form)
@@ -72,7 +78,7 @@ def test_batch_is_bitwise_the_single_model_result(pcs, Tgpu, form):
     assert info["launches_per_replay"] >= 4 and info["n_items"] > 0 and info["grid"] > 0
     if form == _lib.KLS_MIXED_TMEM:
         assert info["grid"] == 2 * info["n_items"]            # one CTA pair per item
-    else:
+    elif form != "mixed forms":
         assert info["n_items"] >= info["grid"]
     if Tgpu == "Float32":
         assert info["schedule"] in ((1, 2) if form == _lib.KLS_MIXED_TMEM else (0, 1))
