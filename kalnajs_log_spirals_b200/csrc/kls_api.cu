@@ -974,7 +974,15 @@ int kls_autotune(kls_ctx* c, int mode, int batch, kls_tune_result* out) {
     // the TMEM-operand form's default is the number of resident CTA pairs:
     // fewer splits leave a single omega (Newton's evaluations) on part of a
     // wave, so only whole multiples of it are candidates
-    if (mixed && form == KLS_MIXED_TMEM) cand = {fdef, 2 * fdef, 3 * fdef};
+    if (mixed && form == KLS_MIXED_TMEM) {
+      cand = {fdef};
+      // more splits only while the FP64 partials of `batch` omegas stay within
+      // 2 GiB (batch x N_pad/64 tiles x splits x N_pad x 128 doubles): an
+      // uneven batch of many default-size models holds one such buffer each
+      const double per_split = (double)batch * (c->Na_pad / 64) * c->Na_pad * 128 * 8;
+      for (int k = 2; k <= 3; ++k)
+        if (per_split * k * fdef <= 2.0 * 1024 * 1024 * 1024) cand.push_back(k * fdef);
+    }
     for (int& s : cand) s = std::max(1, std::min(s, max_s));
     std::sort(cand.begin(), cand.end());
     cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
