@@ -53,7 +53,8 @@ using namespace kls_tc;
 
 constexpr int TM_AB = 64;              // alphas per CTA (128 A rows)
 constexpr int TM_KB = 32;              // complex k per stage
-constexpr int TM_STAGES = 3;           // shared-memory stages (B halves + A sources)
+constexpr int TM_BSTAGES_MAX = 4;      // shared-memory stages of the B halves (4 or 3)
+constexpr int TM_YSTAGES = 3;          // shared-memory stages of the A-source tiles
 constexpr int TM_ASTAGES_MAX = 3;      // TMEM stages of A (3 when Npad <= 320, else 2)
 constexpr int TM_WSTAGES = 8;          // weights ring
 constexpr int TM_CHUNK = 128;          // default stages per FP32 accumulation chunk (4096 k)
@@ -68,11 +69,12 @@ constexpr int TM_WBYTES = TM_KB / 2 * TM_WVAR * 16;   // 512 B: weights of one s
 __host__ __device__ constexpr int tm_astages(int Npad) { return Npad <= 320 ? 3 : 2; }
 
 __host__ __device__ constexpr int tm_btile(int Npad) { return (Npad / 2) * TM_KB * 2; }
-__host__ __device__ constexpr int tm_stage_bytes(int Npad) {
-  return 4 * tm_btile(Npad) + 4 * TM_YTILE;
-}
+// B ring depth: 4 stages up to Npad = 320 (224 KB of shared memory in all),
+// 3 at Npad = 384
+__host__ __device__ constexpr int tm_bstages(int Npad) { return Npad <= 320 ? 4 : 3; }
 size_t tm_smem(int Npad) {
-  return (size_t)TM_STAGES * tm_stage_bytes(Npad) + TM_WSTAGES * TM_WBYTES + 1024;
+  return (size_t)tm_bstages(Npad) * 4 * tm_btile(Npad) + (size_t)TM_YSTAGES * 4 * TM_YTILE +
+         TM_WSTAGES * TM_WBYTES + 1024;
 }
 
 struct TmParams {
@@ -101,8 +103,8 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
                                         const float2* __restrict__ wt32,
                                         double* __restrict__ part, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t bar_b_full[TM_STAGES], bar_b_empty[TM_STAGES],
-      bar_y_full[TM_STAGES], bar_y_empty[TM_STAGES], bar_w_full[TM_WSTAGES],
+  __shared__ __align__(8) uint64_t bar_b_full[TM_BSTAGES_MAX], bar_b_empty[TM_BSTAGES_MAX],
+      bar_y_full[TM_YSTAGES], bar_y_empty[TM_YSTAGES], bar_w_full[TM_WSTAGES],
       bar_w_empty[TM_WSTAGES], bar_a_full[TM_ASTAGES_MAX], bar_a_empty[TM_ASTAGES_MAX], bar_acc_full,
       bar_acc_empty, bar_done;
   __shared__ uint32_t s_tmem;
@@ -127,23 +129,27 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
   const int NA = tm_astages(P.Npad);         // TMEM stages of A
   const uint32_t acol = (uint32_t)(TM_TMEM_COLS - 64 * NA);
   const int Nh = P.Npad / nmma;              // N of each MMA
-  const int SB = tm_stage_bytes(P.Npad), BT = tm_btile(P.Npad);
+  const int BT = tm_btile(P.Npad), NB = tm_bstages(P.Npad);
   const unsigned long long lim = P.wait_ns;
 
-  // B tile (part 0 hi / 1 lo, sub 0 Re rows / 1 Im rows) and A-source tile
+  // B tile (part 0 hi / 1 lo, sub 0 Re rows / 1 Im rows) of B stage s, and
+  // A-source tile of A-source stage s
+  uint8_t* yring = smem + (size_t)NB * 4 * BT;
   auto b_tile = [&](int s, int pt, int sub) {
-    return smem + (size_t)s * SB + (size_t)(2 * pt + sub) * BT;
+    return smem + (size_t)(4 * s + 2 * pt + sub) * BT;
   };
   auto y_tile = [&](int s, int pt, int sub) {
-    return smem + (size_t)s * SB + 4 * (size_t)BT + (size_t)(2 * pt + sub) * TM_YTILE;
+    return yring + (size_t)(4 * s + 2 * pt + sub) * TM_YTILE;
   };
-  uint8_t* wring = smem + (size_t)TM_STAGES * SB;
+  uint8_t* wring = yring + (size_t)TM_YSTAGES * 4 * TM_YTILE;
 
   if (tid == 0) {
     s_abort = 0;
-    for (int s = 0; s < TM_STAGES; ++s) {
+    for (int s = 0; s < NB; ++s) {
       mbar_init(smem_u32(&bar_b_full[s]), 1);
       mbar_init(smem_u32(&bar_b_empty[s]), 1);
+    }
+    for (int s = 0; s < TM_YSTAGES; ++s) {
       mbar_init(smem_u32(&bar_y_full[s]), 1);
       mbar_init(smem_u32(&bar_y_empty[s]), TM_NPROD);
     }
@@ -178,35 +184,35 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
       int issued = 0;
       const int yb = (int)crank * Nh2;
       for (int i = 0; i < nkb; ++i) {
-        const int s = i % TM_STAGES, r = i / TM_STAGES;
-        if (!mbar_wait_cl_lim(smem_u32(&bar_b_empty[s]), (r & 1) ^ 1, &s_abort, err, 1, lim)) break;
-        if (!mbar_wait_lim(smem_u32(&bar_y_empty[s]), (r & 1) ^ 1, &s_abort, err, 11, lim)) break;
+        const int sb = i % NB, rb = i / NB, sy = i % TM_YSTAGES, ry = i / TM_YSTAGES;
+        if (!mbar_wait_cl_lim(smem_u32(&bar_b_empty[sb]), (rb & 1) ^ 1, &s_abort, err, 1, lim))
+          break;
+        if (!mbar_wait_lim(smem_u32(&bar_y_empty[sy]), (ry & 1) ^ 1, &s_abort, err, 11, lim)) break;
         // stage g of 32 k: half (g & 1) of the table's 64-k block g >> 1
         const int g = kb0 + i, kx = (g & 1) * TM_KB, kz = g >> 1;
-        if (leader) mbar_arrive_tx(smem_u32(&bar_b_full[s]), 2 * 4 * BT);
-        const uint32_t fb = mapa_u32(smem_u32(&bar_b_full[s]), 0);
-        tma_load_3d_pair(smem_u32(b_tile(s, 0, 0)), tbh, kx, yb, kz, fb);
-        tma_load_3d_pair(smem_u32(b_tile(s, 0, 1)), tbh, kx, P.Npad + yb, kz, fb);
-        tma_load_3d_pair(smem_u32(b_tile(s, 1, 0)), tbl, kx, yb, kz, fb);
-        tma_load_3d_pair(smem_u32(b_tile(s, 1, 1)), tbl, kx, P.Npad + yb, kz, fb);
-        const uint32_t yf = smem_u32(&bar_y_full[s]);
+        if (leader) mbar_arrive_tx(smem_u32(&bar_b_full[sb]), 2 * 4 * BT);
+        const uint32_t fb = mapa_u32(smem_u32(&bar_b_full[sb]), 0);
+        tma_load_3d_pair(smem_u32(b_tile(sb, 0, 0)), tbh, kx, yb, kz, fb);
+        tma_load_3d_pair(smem_u32(b_tile(sb, 0, 1)), tbh, kx, P.Npad + yb, kz, fb);
+        tma_load_3d_pair(smem_u32(b_tile(sb, 1, 0)), tbl, kx, yb, kz, fb);
+        tma_load_3d_pair(smem_u32(b_tile(sb, 1, 1)), tbl, kx, P.Npad + yb, kz, fb);
+        const uint32_t yf = smem_u32(&bar_y_full[sy]);
         mbar_arrive_tx(yf, 4 * TM_YTILE);
-        tma_load_3d(smem_u32(y_tile(s, 0, 0)), tyh, kx, a0, kz, yf);
-        tma_load_3d(smem_u32(y_tile(s, 0, 1)), tyh, kx, P.Npad + a0, kz, yf);
-        tma_load_3d(smem_u32(y_tile(s, 1, 0)), tyl, kx, a0, kz, yf);
-        tma_load_3d(smem_u32(y_tile(s, 1, 1)), tyl, kx, P.Npad + a0, kz, yf);
+        tma_load_3d(smem_u32(y_tile(sy, 0, 0)), tyh, kx, a0, kz, yf);
+        tma_load_3d(smem_u32(y_tile(sy, 0, 1)), tyh, kx, P.Npad + a0, kz, yf);
+        tma_load_3d(smem_u32(y_tile(sy, 1, 0)), tyl, kx, a0, kz, yf);
+        tma_load_3d(smem_u32(y_tile(sy, 1, 1)), tyl, kx, P.Npad + a0, kz, yf);
         issued = i + 1;
       }
       // the last copies into this CTA's shared memory land before it may exit
       // (the peer's B copies complete on the leader's barrier, which the
       // leader checks; the final cluster barrier orders the peer's exit)
-      for (int i = max(0, issued - TM_STAGES); i < issued; ++i) {
-        mbar_wait_lim(smem_u32(&bar_y_full[i % TM_STAGES]), (i / TM_STAGES) & 1, nullptr, err, 6,
-                      lim);
-        if (leader)
-          mbar_wait_cl_lim(smem_u32(&bar_b_full[i % TM_STAGES]), (i / TM_STAGES) & 1, nullptr,
-                           err, 6, lim);
-      }
+      for (int i = max(0, issued - TM_YSTAGES); i < issued; ++i)
+        mbar_wait_lim(smem_u32(&bar_y_full[i % TM_YSTAGES]), (i / TM_YSTAGES) & 1, nullptr, err,
+                      6, lim);
+      if (leader)
+        for (int i = max(0, issued - NB); i < issued; ++i)
+          mbar_wait_cl_lim(smem_u32(&bar_b_full[i % NB]), (i / NB) & 1, nullptr, err, 6, lim);
     }
   } else if (warp == 3) {
     // ---------------- weights ring
@@ -232,14 +238,14 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
     if (leader && lane == 0 && nkb > 0) {
       const uint32_t idesc = idesc_bf16(256, Nh);
       for (int i = 0; i < nkb; ++i) {
-        const int s = i % TM_STAGES, as = i % NA;
+        const int s = i % NB, as = i % NA;
         const int ci = i % CH, ch = i / CH;
         const bool first = ci == 0;
         const bool last = ci == CH - 1 || i == nkb - 1;
         if (first && ch > 0 &&
             !mbar_wait_cl_lim(smem_u32(&bar_acc_empty), (ch - 1) & 1, &s_abort, err, 7, lim))
           break;
-        if (!mbar_wait_cl_lim(smem_u32(&bar_b_full[s]), (i / TM_STAGES) & 1, &s_abort, err, 2, lim))
+        if (!mbar_wait_cl_lim(smem_u32(&bar_b_full[s]), (i / NB) & 1, &s_abort, err, 2, lim))
           break;
         if (!mbar_wait_cl_lim(smem_u32(&bar_a_full[as]), (i / NA) & 1, &s_abort, err, 3, lim))
           break;
@@ -285,8 +291,8 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
     const uint32_t tl = tmem + ((uint32_t)(32 * q) << 16) + acol + (uint32_t)(kh * 8);
     const bool skip_one = P.fault_skip && leader && tile_pair == 0 && split == 0 && pw == 0;
     for (int i = 0; i < nkb; ++i) {
-      const int s = i % TM_STAGES, as = i % NA, ws = i % TM_WSTAGES;
-      bool ok = mbar_wait_lim(smem_u32(&bar_y_full[s]), (i / TM_STAGES) & 1, &s_abort, err, 4, lim);
+      const int s = i % TM_YSTAGES, as = i % NA, ws = i % TM_WSTAGES;
+      bool ok = mbar_wait_lim(smem_u32(&bar_y_full[s]), (i / TM_YSTAGES) & 1, &s_abort, err, 4, lim);
       if (ok) ok = mbar_wait_lim(smem_u32(&bar_w_full[ws]), (i / TM_WSTAGES) & 1, &s_abort, err, 8,
                                  lim);
       if (ok) ok = mbar_wait_cl_lim(smem_u32(&bar_a_empty[as]), ((i / NA) & 1) ^ 1, &s_abort, err,
@@ -506,14 +512,19 @@ __global__ void tm_reduce_kernel(int Na, int Npad, int tiles_a, int splits, doub
 }
 
 // The dynamic shared-memory limit is a property of the kernel, shared by
-// every context in the process: set it once to the largest stage layout
-// (N_alpha_pad = 384), so that contexts of any size can launch.
+// every context in the process: set it once to the largest stage layout of
+// any N_alpha_pad (64 .. 384), so that contexts of any size can launch.
+size_t tm_smem_max() {
+  size_t mx = 0;
+  for (int n = 64; n <= 384; n += 64) mx = std::max(mx, tm_smem(n));
+  return mx;
+}
 cudaError_t tm_set_smem_limits() {
   cudaError_t e = cudaFuncSetAttribute(mixed_tm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)tm_smem(384));
+                                       (int)tm_smem_max());
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(mixed_tm_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tm_smem(384));
+                             (int)tm_smem_max());
   return e;
 }
 
@@ -712,7 +723,7 @@ int kls_tm_multi_launch(cudaStream_t st, const kls_mdesc* d_md, const kls_tm_mod
       if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
     }
   } else {
-    mixed_tm_multi_kernel<<<2 * n_items, TM_THREADS, tm_smem(max_Npad), st>>>(d_tm, d_items,
+    mixed_tm_multi_kernel<<<2 * n_items, TM_THREADS, tm_smem_max(), st>>>(d_tm, d_items,
                                                                                d_err);
     if ((e = cudaGetLastError()) != cudaSuccess) return (int)e;
   }
