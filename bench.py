@@ -76,6 +76,8 @@ def parse():
                     help="also evaluate the proposer on N held-out models at the default size")
     ap.add_argument("--heldout-save", default="",
                     help="save the held-out network's parameters (.npy) after training")
+    ap.add_argument("--heldout-far", type=float, default=2e-3,
+                    help="far_step of the held-out evaluation's second hybrid refinement")
     ap.add_argument("--heldout-params", default="",
                     help="load the held-out network's parameters (.npy) instead of training")
     ap.add_argument("--uneven-columns", type=int, default=1,
@@ -626,7 +628,7 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
         rh = newton_search_hybrid(cfg, pc, Op_p, g_p)
         t_h = time.perf_counter() - t0
         t0 = time.perf_counter()
-        rh2 = newton_search_hybrid(cfg, pc, Op_p, g_p, K.api.HybridConfig(far_step=2e-3))
+        rh2 = newton_search_hybrid(cfg, pc, Op_p, g_p, K.api.HybridConfig(far_step=args.heldout_far))
         t_h2 = time.perf_counter() - t0
         growing = bool(r64.converged and r64.gamma > 1e-4)
         a = polish(K, cfg, pc, r64.Omega_p, r64.gamma) if growing else None
@@ -643,7 +645,7 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
         pc.close()
         rows.append({"n_zang": sp.n_zang, "q1": sp.q1, "m": sp.m, "growing_mode": growing,
                      "same_root": same, "same_root_hybrid": same_h,
-                     "same_root_hybrid_far_2e-3": same_h2,
+                     "same_root_hybrid_far": same_h2,
                      "start_equals_scan_argmin": (Op_p, g_p) == (Op0, g0),
                      "proposal_dets": used,
                      "plain_fp64_s": s.n_Op * s.n_gamma * t_fp64_det + t_n64,
@@ -654,7 +656,7 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
                      "fp64_from_proposal": [rp.Omega_p, rp.gamma, bool(rp.converged)],
                      "hybrid": [rh.Omega_p, rh.gamma, bool(rh.converged), rh.mixed_evals,
                                 rh.fp64_evals, rh.anchored_evals],
-                     "hybrid_far_2e-3": [rh2.Omega_p, rh2.gamma, bool(rh2.converged),
+                     "hybrid_far": [rh2.Omega_p, rh2.gamma, bool(rh2.converged),
                                          rh2.mixed_evals, rh2.fp64_evals, rh2.anchored_evals],
                      "polished_scan_root": a, "polished_hybrid_root": b})
     grow = [r for r in rows if r["growing_mode"]]
@@ -676,12 +678,12 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
             "with_growing_mode": len(grow), "same_root_within_1e-10": len(ok),
             "success_rate": len(ok) / len(grow) if grow else None,
             "success_rate_hybrid": rate("same_root_hybrid"),
-            "success_rate_hybrid_far_2e-3": rate("same_root_hybrid_far_2e-3"),
+            "success_rate_hybrid_far_2e-3": rate("same_root_hybrid_far"),
             "mean_time_to_root_s": {"plain_fp64 (scan at the measured FP64 det time)":
                                     mean("plain_fp64_s", grow),
                                     "learned_proposal_then_fp64_newton": mean("learned_s", grow),
                                     "learned_proposal_then_hybrid": mean("learned_hybrid_s", grow),
-                                    "learned_proposal_then_hybrid_far_2e-3":
+                                    "learned_proposal_then_hybrid_far":
                                         mean("learned_hybrid_far_s", grow)},
             "per_model": rows}
 
