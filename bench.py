@@ -620,7 +620,7 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
         t_prop = time.perf_counter() - t0
         # the proposal refined three ways: FP64 Newton (the workload's own
         # refinement), the hybrid with its defaults, and the hybrid with far
-        # steps of FP64 accuracy down to 2e-3 (grid starts are coarse)
+        # steps of FP64 accuracy down to --heldout-far (grid starts are coarse)
         t0 = time.perf_counter()
         rp = K.newton_search(cfg, pc, None, K.GPUType.NVIDIA, "Float64", Op_p, g_p)
         t_rp = time.perf_counter() - t0
@@ -674,11 +674,12 @@ def heldout_eval(args, K, P, base_cfg, n_models: int, t_fp64_det: float, local, 
                               "|dgamma| <= 1e-10",
             "refinement": "success_rate: proposal refined by FP64 Newton (the workload's "
                           "refinement); also by the hybrid Newton (defaults) and by the hybrid "
-                          "with far_step 2e-3",
+                          "with far_step --heldout-far",
             "with_growing_mode": len(grow), "same_root_within_1e-10": len(ok),
             "success_rate": len(ok) / len(grow) if grow else None,
             "success_rate_hybrid": rate("same_root_hybrid"),
-            "success_rate_hybrid_far_2e-3": rate("same_root_hybrid_far"),
+            "success_rate_hybrid_far": rate("same_root_hybrid_far"),
+            "far_step": args.heldout_far,
             "mean_time_to_root_s": {"plain_fp64 (scan at the measured FP64 det time)":
                                     mean("plain_fp64_s", grow),
                                     "learned_proposal_then_fp64_newton": mean("learned_s", grow),
