@@ -22,13 +22,14 @@
 // Im rows Npad + a), so each SM reads Npad / 2 table rows per stage.  The
 // accumulator (128 lanes x Npad FP32 columns per CTA) holds every output row
 // b and is flushed every `chunk` stages (default TM_CHUNK) into an FP64
-// partial per (tile, K split) in deterministic order; the split sum, G N(a) scaling, I - M, the
-// weights and the LU are FP64.  Products hi*hi + lo*hi + hi*lo (the lo*lo
+// partial per (tile, K split) in deterministic order; the split sum, G N(a)
+// scaling, I - M, the weights and the LU are FP64.  Products hi*hi + lo*hi + hi*lo (the lo*lo
 // term, ~2^-18 relative, is dropped).
 //
 // Warps (640 threads):
-//   0       TMA: both B half tiles (completing on the leader's barrier) and
-//           this CTA's A-source tiles (its 64 alphas)
+//   0       TMA: both B half tiles (completing on the leader's barrier; a
+//           ring of 4 stages, 3 at Npad = 384) and this CTA's A-source tiles
+//           (its 64 alphas; a ring of 3 stages)
 //   1       MMA issuer (leader CTA, one thread)
 //   2       TMEM allocation / release (512 columns: D at [0, Npad), A stages
 //           of 64 columns at the top: three for Npad <= 320, else two)
