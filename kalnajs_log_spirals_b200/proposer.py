@@ -255,7 +255,7 @@ def propose(mlp: MLP, spec: ModelSpec, det_fn, k: int = 48, descend: int = 6,
 @dataclasses.dataclass
 class RootResult:
     """find_root outcome: the Newton result and how its start was found."""
-    newton: object                 # api.NewtonResult (hybrid Newton, FP64 finish)
+    newton: object                 # api.NewtonResult of the refinement
     start: Tuple[float, float]
     source: str                    # "proposal", "proposal_fp64" or "grid_scan"
     proposal_dets: int             # determinants spent on the proposal
@@ -263,35 +263,53 @@ class RootResult:
 
 
 def find_root(mlp: MLP, config: KalnajsConfig, precomputed, k: int = 48,
-              min_gamma: float = 1e-4) -> RootResult:
+              min_gamma: float = 1e-4, refine: str = "fp64") -> RootResult:
     """Newton root of det(I - M) with a learned start and the scan as fallback.
 
     The proposal (``propose`` over the config's scan grid, split-BF16
-    determinants) starts ``newton_search_hybrid``, whose last steps and
-    stopping test are FP64; if that does not converge, plain FP64 Newton
-    (newton_search) runs from the same start; if neither reaches a growing
-    mode (gamma > min_gamma), the reference workflow runs instead: the full
-    grid scan (GridScan.jl:25-88) in the split-BF16 form and the hybrid
-    Newton from its argmin.
+    determinants) is refined by plain FP64 Newton (``refine="fp64"``,
+    newton_search: the reference's iteration, so a start equal to the scan's
+    argmin gives the scan's root exactly; 28 of 29 held-out default-size
+    models reach the scan's root) or by ``newton_search_hybrid`` with FP64
+    far steps down to 2e-3 (``refine="hybrid"``: 2-3x faster, 22 of 29; near
+    the real axis its split-BF16 steps can leave the reference's path), with
+    plain FP64 Newton from the same start when the hybrid does not converge.
+    If no growing mode (gamma > min_gamma) is reached, the reference workflow
+    runs instead: the full grid scan (GridScan.jl:25-88) in the split-BF16
+    form and the same refinement from its argmin.
     """
     from . import api
+    if refine not in ("fp64", "hybrid"):
+        raise ValueError(f"refine must be 'fp64' or 'hybrid', not {refine!r}")
     s = config.scan
     spec = ModelSpec(int(config.model.n_zang), float(config.model.q1), int(config.physics.m))
     dev = api.to_device(precomputed, api.GPUType.NVIDIA, "Float32")
     Op, g, used = propose(mlp, spec, lambda om: api.compute_determinant_batched(
         om, precomputed, dev, batch_size=16), k=k, n_Op=s.n_Op, n_gamma=s.n_gamma,
         Op_range=(s.Omega_p_min, s.Omega_p_max), g_range=(s.gamma_min, s.gamma_max))
-    # a grid point is a coarse start: steps longer than 2e-3 are taken with
-    # FP64 accuracy, on the reference's path (22 of 29 held-out default-size
-    # models reach the scan's root this way, 21 with the hybrid's defaults)
-    r = api.newton_search_hybrid(config, precomputed, Op, g, api.HybridConfig(far_step=2e-3))
-    if r.converged and r.gamma > min_gamma:
-        return RootResult(r, (Op, g), "proposal", used, 0)
-    if not r.converged:
-        # the arbiter: plain FP64 Newton from the same start
-        r = api.newton_search(config, precomputed, None, api.GPUType.NVIDIA, "Float64", Op, g)
+
+    def fp64(Op0, g0):
+        return api.newton_search(config, precomputed, None, api.GPUType.NVIDIA, "Float64", Op0, g0)
+
+    def hybrid(Op0, g0):
+        # a grid point is a coarse start: steps longer than 2e-3 are taken
+        # with FP64 accuracy, on the reference's path
+        return api.newton_search_hybrid(config, precomputed, Op0, g0,
+                                        api.HybridConfig(far_step=2e-3))
+
+    if refine == "fp64":
+        r = fp64(Op, g)
         if r.converged and r.gamma > min_gamma:
             return RootResult(r, (Op, g), "proposal_fp64", used, 0)
+    else:
+        r = hybrid(Op, g)
+        if r.converged and r.gamma > min_gamma:
+            return RootResult(r, (Op, g), "proposal", used, 0)
+        if not r.converged:
+            # the arbiter: plain FP64 Newton from the same start
+            r = fp64(Op, g)
+            if r.converged and r.gamma > min_gamma:
+                return RootResult(r, (Op, g), "proposal_fp64", used, 0)
     _, Op0, g0 = api.grid_scan(config, precomputed, dev)
-    r = api.newton_search_hybrid(config, precomputed, Op0, g0, api.HybridConfig(far_step=2e-3))
+    r = fp64(Op0, g0) if refine == "fp64" else hybrid(Op0, g0)
     return RootResult(r, (Op0, g0), "grid_scan", used, s.n_Op * s.n_gamma)

@@ -118,6 +118,7 @@ def test_find_root_falls_back_to_the_scan(lib_path):
     mlp = P.MLP(256, 4, seed=123)                 # untrained
     forced = P.find_root(mlp, cfg, pc, k=4, min_gamma=10.0)
     free = P.find_root(mlp, cfg, pc, k=4)
+    free_h = P.find_root(mlp, cfg, pc, k=4, refine="hybrid")
     _, Op0, g0 = K.grid_scan(cfg, pc)
     ref = newton64(cfg, Op0, g0)
     pc.close()
@@ -130,4 +131,5 @@ def test_find_root_falls_back_to_the_scan(lib_path):
     assert ref.converged and forced.newton.converged
     assert abs(forced.newton.Omega_p - ref.Omega_p) <= 1e-10
     assert abs(forced.newton.gamma - ref.gamma) <= 1e-10
-    assert free.newton.converged and free.source in ("proposal", "proposal_fp64", "grid_scan")
+    assert free.newton.converged and free.source in ("proposal_fp64", "grid_scan")
+    assert free_h.newton.converged and free_h.source in ("proposal", "proposal_fp64", "grid_scan")
