@@ -30,7 +30,7 @@
 //   0       TMA: both B half tiles (completing on the leader's barrier; a
 //           ring of 4 stages, 3 at Npad = 384) and this CTA's A-source tiles
 //           (its 64 alphas; a ring of 3 stages)
-//   1       MMA issuer (leader CTA, one thread)
+//   1       MMA issuer (leader CTA; the warp waits, one elected lane issues)
 //   2       TMEM allocation / release (512 columns: D at [0, Npad), A stages
 //           of 64 columns at the top: three for Npad <= 320, else two)
 //   3       weights ring: bulk copies of the FP32 w(omega) of the CTA's omega,
@@ -235,44 +235,58 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
                       6, lim);
     }
   } else if (warp == 1) {
-    // ---------------- MMA issuer (leader)
-    if (leader && lane == 0 && nkb > 0) {
+    // ---------------- MMA issuer (leader): the whole warp waits, one elected
+    // lane issues.  B descriptors are formed once: a tile's descriptor is the
+    // first tile's plus (byte offset >> 4) (shared addresses stay below
+    // 256 KB, so the add never carries out of the 14-bit start field).
+    if (leader && nkb > 0) {
       const uint32_t idesc = idesc_bf16(256, Nh);
+      const uint64_t d00 = sw64_desc(smem_u32(b_tile(0, 0, 0)));
+      const uint32_t t16 = (uint32_t)BT >> 4;                  // one B tile
+      const uint32_t nh16 = (uint32_t)((Nh >> 1) * 64) >> 4;   // second N half
+      const bool issuer = elect_one();
       for (int i = 0; i < nkb; ++i) {
         const int s = i % NB, as = i % NA;
         const int ci = i % CH, ch = i / CH;
         const bool first = ci == 0;
         const bool last = ci == CH - 1 || i == nkb - 1;
-        if (first && ch > 0 &&
-            !mbar_wait_cl_lim(smem_u32(&bar_acc_empty), (ch - 1) & 1, &s_abort, err, 7, lim))
-          break;
-        if (!mbar_wait_cl_lim(smem_u32(&bar_b_full[s]), (i / NB) & 1, &s_abort, err, 2, lim))
-          break;
-        if (!mbar_wait_cl_lim(smem_u32(&bar_a_full[as]), (i / NA) & 1, &s_abort, err, 3, lim))
-          break;
+        bool ok = true;
+        if (first && ch > 0)
+          ok = mbar_wait_cl_lim(smem_u32(&bar_acc_empty), (ch - 1) & 1, &s_abort, err, 7, lim);
+        if (ok) ok = mbar_wait_cl_lim(smem_u32(&bar_b_full[s]), (i / NB) & 1, &s_abort, err, 2, lim);
+        if (ok) ok = mbar_wait_cl_lim(smem_u32(&bar_a_full[as]), (i / NA) & 1, &s_abort, err, 3, lim);
+        if (!__all_sync(0xffffffffu, ok)) break;
         tc_fence_after();
+        if (issuer) {
+          // tile (s, part, sub) sits at (4 s + 2 part + sub) tiles; k 16..31
+          // of a 64-byte row start 32 bytes in
+          const uint64_t ds = d00 + (uint64_t)(4 * s) * t16;
+          const uint32_t a_s = tmem + acol + (uint32_t)(as * 64);
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-          const int sub = kk >> 1;                       // Re rows, then Im rows
-          const uint32_t kb = (uint32_t)(kk & 1) * 32;   // bytes: k 0..15 / 16..31
-          const uint32_t a_hi = tmem + acol + (uint32_t)(as * 64 + kk * 8);
-          const uint32_t a_lo = a_hi + 32;
-          for (int nh = 0; nh < nmma; ++nh) {
-            const uint32_t d = tmem + (uint32_t)(nh * Nh);
-            const uint32_t boff = (uint32_t)(nh * (Nh >> 1) * 64) + kb;
-            const uint64_t bh = sw64_desc(smem_u32(b_tile(s, 0, sub)) + boff);
-            const uint64_t bl = sw64_desc(smem_u32(b_tile(s, 1, sub)) + boff);
-            umma_pair_ts(d, a_hi, bh, idesc, (first && kk == 0) ? 0u : 1u);
-            umma_pair_ts(d, a_lo, bh, idesc, 1u);
-            umma_pair_ts(d, a_hi, bl, idesc, 1u);
+          for (int kk = 0; kk < 4; ++kk) {
+            const uint64_t bh = ds + (uint64_t)((kk >> 1) * t16 + (kk & 1) * 2);   // Re, then Im rows
+            const uint64_t bl = bh + 2 * t16;
+            const uint32_t a_hi = a_s + (uint32_t)(kk * 8), a_lo = a_hi + 32;
+            const uint32_t acc0 = (first && kk == 0) ? 0u : 1u;
+#pragma unroll
+            for (int nh = 0; nh < 2; ++nh) {
+              if (nh < nmma) {
+                const uint32_t d = tmem + (uint32_t)(nh * Nh);
+                const uint64_t o = (uint64_t)(nh * nh16);
+                umma_pair_ts(d, a_hi, bh + o, idesc, acc0);
+                umma_pair_ts(d, a_lo, bh + o, idesc, 1u);
+                umma_pair_ts(d, a_hi, bl + o, idesc, 1u);
+              }
+            }
           }
+          umma_pair_commit(smem_u32(&bar_b_empty[s]));
+          umma_pair_commit(smem_u32(&bar_a_empty[as]));
+          if (last) umma_pair_commit(smem_u32(&bar_acc_full));
         }
-        umma_pair_commit(smem_u32(&bar_b_empty[s]));
-        umma_pair_commit(smem_u32(&bar_a_empty[as]));
-        if (last) umma_pair_commit(smem_u32(&bar_acc_full));
+        __syncwarp();
       }
       // completion of every issued MMA (also on the abort path)
-      umma_pair_commit(smem_u32(&bar_done));
+      if (issuer) umma_pair_commit(smem_u32(&bar_done));
     }
   } else if (warp >= 4 && warp < 4 + TM_NPROD) {
     // ---------------- producers: A rows of this CTA's 64 alphas into TMEM
@@ -339,7 +353,7 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
         mbar_arrive(smem_u32(&bar_w_empty[ws]));
         if (!(skip_one && i == 0)) {
           if (leader) mbar_arrive(smem_u32(&bar_a_full[as]));
-          else mbar_arrive_remote(mapa_u32(smem_u32(&bar_a_full[as]), 0));
+          else mbar_arrive_remote_cta(mapa_u32(smem_u32(&bar_a_full[as]), 0));
         }
       }
     }
@@ -378,7 +392,7 @@ __device__ __forceinline__ void tm_body(const CUtensorMap* tbh, const CUtensorMa
       __syncwarp();
       if (lane == 0) {
         if (leader) mbar_arrive(smem_u32(&bar_acc_empty));
-        else mbar_arrive_remote(mapa_u32(smem_u32(&bar_acc_empty), 0));
+        else mbar_arrive_remote_cta(mapa_u32(smem_u32(&bar_acc_empty), 0));
       }
     }
   }

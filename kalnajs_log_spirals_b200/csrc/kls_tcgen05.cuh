@@ -78,6 +78,15 @@ __device__ __forceinline__ bool mbar_wait_cl_lim(uint32_t a, uint32_t parity,
                                                  unsigned long long limit_ns) {
   return mbar_wait_impl<true>(a, parity, abort, err, code, limit_ns);
 }
+// one lane of the (fully active) warp, the same on every call: the warp
+// stays converged around the MMA issue, so its loop state is warp-uniform
+__device__ __forceinline__ bool elect_one() {
+  uint32_t pred;
+  asm volatile(
+      "{\n.reg .pred p;\nelect.sync _|p, 0xffffffff;\nselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(pred));
+  return pred != 0;
+}
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -260,6 +269,13 @@ __device__ __forceinline__ uint32_t mapa_u32(uint32_t a, uint32_t rank) {
 __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
                : "memory");
+}
+// the same arrive with the default (CTA-scope) release: enough where the
+// signalled work is tensor-memory traffic that tcgen05.wait has completed and
+// the tcgen05 thread-sync fences order around the barrier; it spares the
+// cluster-scope fence on every stage
+__device__ __forceinline__ void mbar_arrive_remote_cta(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
 }
 __device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
                                           uint32_t acc) {
