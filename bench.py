@@ -286,6 +286,73 @@ def cpu_det_baseline(pc, cfg, omega: complex):
                         f"exported table")
 
 
+def cpu_small_size(args, K, local):
+    """Secondary CPU figures at the small size (NR=101, Ne=21, N_alpha=101,
+    l in [-25, 25], Newton tol 1e-10) on the device's exported table:
+    the reference module's naive loops (MatrixBuilder.jl:37-87, its --gpu=CPU
+    path) as one whole determinant, and the BLAS form (NL_julia_direct.jl:
+    299-310) on all host threads and on the reference's configured 4 threads
+    (max_threads), each as one whole determinant and as a whole FP64 Newton
+    solve from the reference start; the GPU's FP64 Newton on the same model
+    beside them."""
+    import numpy as np
+    from threadpoolctl import threadpool_limits
+    from oracle import np_oracle as O
+    cfg = K.load_model(K.load_config(os.path.join(ROOT, "configs", "size_s.toml")), args.model)
+    pc = K.precompute_all(cfg, device=local)
+    try:
+        oc = oracle_config(cfg)
+        NPh, Na, nl = pc.ctx.dims.NPh, oc.N_alpha, oc.n_l
+        W = np.empty((NPh, Na, nl), dtype=np.complex128, order="F")
+        buf = np.empty(NPh * Na, dtype=np.complex128)
+        for il in range(nl):
+            pc.ctx.call("kls_export_W", il, 1, buf.view(np.float64).ctypes.data_as(
+                C.POINTER(C.c_double)))
+            W[:, :, il] = buf.reshape(Na, NPh).T
+        opc = O.Precomputed(oc, oc.m, float(oc.G), Na, nl, np.arange(oc.l_min, oc.l_max + 1),
+                            NPh, pc.alpha_arr, pc.d_alpha, None, pc.DJ_vec,
+                            pc.F0l_all.reshape(NPh, nl, order="F"),
+                            pc.Omega_res.reshape(NPh, nl, order="F"), W, pc.N_kernel)
+        m = oc.m
+        Op0, g0 = float(cfg.reference.Omega_p), float(cfg.reference.gamma)
+        nc = cfg.newton
+        w0 = complex(m * Op0, g0)
+        out = {"size": f"NR={oc.NR} Ne={oc.Ne} N_alpha={Na} l=[{oc.l_min},{oc.l_max}] "
+                       f"(K = {NPh * nl})", "host_cores": os.cpu_count(),
+               "start": [Op0, g0], "tol": float(nc.tol)}
+        t0 = time.perf_counter()
+        d_naive = O.compute_det_naive(opc, w0)
+        t_naive = time.perf_counter() - t0
+        d_gpu = K.compute_determinant(w0, pc)
+        out["naive_loops"] = {"s_per_det": t_naive, "det_evals_per_s": 1.0 / t_naive,
+                              "threads": 1, "det_rel_diff_vs_gpu": abs(d_naive - d_gpu) / abs(d_gpu)}
+        for label, nthr in (("blas_all_threads", None), ("blas_4_threads", 4)):
+            with threadpool_limits(nthr, user_api="blas"):
+                O.compute_det(opc, w0 + 1e-3)                    # warm the BLAS pool
+                t0 = time.perf_counter()
+                d_blas = O.compute_det(opc, w0)
+                t_det = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                r = O.newton_search(lambda w: O.compute_det(opc, w), m, Op0, g0,
+                                    max_iter=int(nc.max_iter), tol=float(nc.tol),
+                                    delta=float(nc.delta))
+                t_newton = time.perf_counter() - t0
+                out[label] = {"threads": blas_threads(), "s_per_det": t_det,
+                              "det_evals_per_s": 1.0 / t_det,
+                              "det_rel_diff_vs_gpu": abs(d_blas - d_gpu) / abs(d_gpu),
+                              "newton_s": t_newton, "newton_root": [r.Omega_p, r.gamma],
+                              "newton_iterations": int(r.iterations),
+                              "newton_converged": bool(r.converged)}
+        t0 = time.perf_counter()
+        rg = K.newton_search(cfg, pc, None, K.GPUType.NVIDIA, "Float64")
+        t_gpu = time.perf_counter() - t0
+        out["gpu_fp64_newton"] = {"newton_s": t_gpu, "root": [rg.Omega_p, rg.gamma],
+                                  "iterations": int(rg.iterations), "det_evals": int(rg.det_evals)}
+        return out
+    finally:
+        pc.close()
+
+
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
@@ -1065,6 +1132,11 @@ def ours(args):
         cpu = {"value": rate, "unit": UNIT, "cores": blas_threads(), "kind": "port",
                "sample": sample, "host_cores": os.cpu_count(),
                "det_rel_diff_vs_gpu_fp64": abs(d_cpu - d_gpu) / abs(d_gpu)}
+        if world == 1:
+            try:
+                cpu["small_size"] = cpu_small_size(args, K, local)
+            except Exception as e:             # a secondary figure never fails the run
+                cpu["small_size"] = {"unavailable": f"{type(e).__name__}: {e}"}
 
     refgpu = None
     if world == 1 and not args.no_refgpu:

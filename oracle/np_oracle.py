@@ -533,6 +533,34 @@ def compute_det(pc: Precomputed, omega: complex) -> complex:
     return complex(np.linalg.det(np.eye(pc.N_alpha) - M))
 
 
+def build_M_naive(pc: Precomputed, omega: complex) -> np.ndarray:
+    """M(omega) by the reference module's own CPU loops (MatrixBuilder.jl:37-67,
+    the ``--gpu=CPU`` path of run_kalnajs_gpu.jl): per harmonic the weights
+    with the |den| < 1e-12 clamp, then for every (alpha, beta) one elementwise
+    product over the orbits, ``sum(W[:, beta] .* weight .* conj.(W[:, alpha]))``,
+    and G, N(alpha) at the end.  The same sums as ``build_M`` in another order
+    (agreement to rounding); kept as the reference's slow CPU form for timing."""
+    M = np.zeros((pc.N_alpha, pc.N_alpha), dtype=np.complex128)
+    for il in range(pc.n_l):
+        W = pc.W[:, :, il]
+        den = omega - pc.Omega_res[:, il].astype(np.complex128)
+        den[np.abs(den) < 1e-12] = 1e-12 + 1e-12j
+        weight = pc.DJ * pc.F0l[:, il] / den
+        for a in range(pc.N_alpha):
+            for b in range(pc.N_alpha):
+                M[b, a] += np.sum(W[:, b] * weight * np.conj(W[:, a]))
+    M *= pc.G
+    for a in range(pc.N_alpha):
+        M[:, a] *= pc.N_kernel[a]
+    return M
+
+
+def compute_det_naive(pc: Precomputed, omega: complex) -> complex:
+    """det(I - M) with M from the naive loops (MatrixBuilder.jl:76-87)."""
+    M = build_M_naive(pc, omega)
+    return complex(np.linalg.det(np.eye(pc.N_alpha) - M))
+
+
 # --------------------------------------------------------------------------
 # GridScan.jl:25-88, 234-246
 # --------------------------------------------------------------------------
