@@ -528,6 +528,8 @@ int kls_scan(kls_ctx* c, const kls_scan_cfg* sc, double* det_grid, double* log_a
   if (r) return r;
   if (!sc || sc->n_Op < 1 || sc->n_gamma < 1 || !det_grid)
     return kls_fail(c, KLS_ERR_CONFIG, "bad scan configuration");
+  if ((long long)sc->n_Op * sc->n_gamma > INT_MAX)
+    return kls_fail(c, KLS_ERR_CONFIG, "scan grid larger than 2^31 - 1 points");
   const int nO = sc->n_Op, nG = sc->n_gamma, n = nO * nG;
   std::vector<double> om(2 * (size_t)n), la((size_t)n);
   // column-major det_grid[i_gamma, j_Op] (GridScan.jl:47, :101-104)
@@ -544,13 +546,11 @@ int kls_scan(kls_ctx* c, const kls_scan_cfg* sc, double* det_grid, double* log_a
   // argmin |det| in column-major order, first occurrence; NaN wins as in Julia
   int best = 0;
   double bv = INFINITY;
-  bool nan = false;
   for (int q = 0; q < n; ++q) {
     double v = std::hypot(det_grid[2 * q], det_grid[2 * q + 1]);
-    if (std::isnan(v)) { best = q; nan = true; break; }
+    if (std::isnan(v)) { best = q; break; }
     if (v < bv) { bv = v; best = q; }
   }
-  (void)nan;
   int i = best % nG, j = best / nG;
   if (Op0) *Op0 = kls_lin(sc->Omega_p_min, sc->Omega_p_max, nO, j);
   if (g0) *g0 = kls_lin(sc->gamma_min, sc->gamma_max, nG, i);

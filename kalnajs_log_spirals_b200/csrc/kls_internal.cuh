@@ -3,6 +3,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
+#include <climits>
 #include <cstdint>
 #include <string>
 #include "kls.h"

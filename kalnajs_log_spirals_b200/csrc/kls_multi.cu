@@ -594,6 +594,8 @@ int kls_scan_multi(kls_multi* m, const kls_scan_cfg* sc, double* det_grid, doubl
   if (!m) return KLS_ERR_CONFIG;
   if (!sc || sc->n_Op < 1 || sc->n_gamma < 1 || !det_grid)
     return mfail(m, KLS_ERR_CONFIG, "bad scan configuration");
+  if ((long long)sc->n_Op * sc->n_gamma > INT_MAX)
+    return mfail(m, KLS_ERR_CONFIG, "scan grid larger than 2^31 - 1 points");
   KM_CK(m, cudaSetDevice(m->device));
   const int nO = sc->n_Op, nG = sc->n_gamma, n = nO * nG;
   // column-major grid per model, omega = m_model * Omega_p + i gamma (GridScan.jl:47, :101-104)
