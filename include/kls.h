@@ -144,6 +144,9 @@ const char* kls_last_error(const kls_ctx* ctx);
 /* Message for failures of calls without a context (kls_create,
  * kls_det_lu_static). */
 const char* kls_create_error(void);
+/* Sizes of the context's data: the NPh, n_l and N_alpha fields of
+ * PrecomputedData (BasisFunctions.jl:30-60), the padded device sizes and the
+ * device memory the context holds. */
 int kls_get_dims(const kls_ctx* ctx, kls_dims* out);
 /* Launch subsequent work on this cudaStream_t (NULL = the context's own). */
 int kls_set_stream(kls_ctx* ctx, void* cuda_stream);
