@@ -863,9 +863,13 @@ def uneven_batch(args, K, P, local, sync):
                          "schedule_pass_ms": info["schedule_ms"],
                          "graph_replay": bool(info["graph"]),
                          "kernels_per_pass": info["launches_per_replay"]},
+        # a model whose sizes were tuned before in the process reuses the
+        # cached choice without timing it (candidates 0, no times)
         "autotune": [{"splits": t.splits, "default": t.default_splits, "form": t.form,
-                      "ms_per_omega": t.ms_per_omega,
-                      "default_ms_per_omega": t.default_ms_per_omega} for t in tunes],
+                      "cached": t.candidates == 0,
+                      "ms_per_omega": t.ms_per_omega if t.candidates else None,
+                      "default_ms_per_omega": t.default_ms_per_omega if t.candidates else None}
+                     for t in tunes],
         "setup_s": t_setup,
         "form": "split-BF16 (FP64 tables released after the split)"}
 
