@@ -193,10 +193,15 @@ def load(path: str = LIB_PATH) -> C.CDLL:
 
 
 def dptr(a) -> _D:
-    """double* of a C-contiguous float64 numpy array (or NULL for None)."""
+    """double* of a contiguous (C or Fortran order) float64 or complex128 numpy
+    array, or NULL for None; anything else raises TypeError (the library
+    would read or write it as doubles)."""
     if a is None:
         return C.cast(None, _D)
-    assert a.dtype.name in ("float64", "complex128") and a.flags.c_contiguous or a.flags.f_contiguous
+    if a.dtype.name not in ("float64", "complex128") or not (a.flags.c_contiguous
+                                                           or a.flags.f_contiguous):
+        raise TypeError(f"expected a contiguous float64/complex128 array, got {a.dtype} "
+                        f"(C {a.flags.c_contiguous}, F {a.flags.f_contiguous})")
     return a.ctypes.data_as(_D)
 
 

@@ -125,3 +125,16 @@ def test_model_constants():
     o = O.ToomreZang.from_config(O.OracleConfig())
     assert m.DF_const == pytest.approx(o.DF_const, rel=1e-15)
     assert m.sigma_r0 == 1 / np.sqrt(7) and m.q_zang == 6
+
+
+def test_dptr_accepts_only_contiguous_doubles():
+    """The ctypes helper hands the library double* buffers: float64 or
+    complex128, contiguous in C or Fortran order; other arrays raise."""
+    import numpy as np
+    assert _lib.dptr(np.zeros(4)) is not None
+    assert _lib.dptr(np.zeros((3, 2), order="F")) is not None
+    assert _lib.dptr(np.zeros(2, dtype=np.complex128)) is not None
+    for bad in (np.zeros(4, dtype=np.float32), np.zeros(4, dtype=np.int64),
+                np.zeros((4, 4))[:, 1]):
+        with pytest.raises(TypeError):
+            _lib.dptr(bad)
