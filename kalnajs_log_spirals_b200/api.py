@@ -747,7 +747,8 @@ class ModelBatch:
     def det(self, omegas) -> Tuple[np.ndarray, np.ndarray]:
         """omegas [n_models, n] complex -> (det [n_models, n], log|det| [n_models, n])."""
         om = np.ascontiguousarray(np.asarray(omegas, dtype=np.complex128))
-        assert om.ndim == 2 and om.shape[0] == len(self.models)
+        if om.ndim != 2 or om.shape[0] != len(self.models):
+            raise ValueError(f"expected omegas of shape [{len(self.models)}, n], got {om.shape}")
         n = om.shape[1]
         d = np.empty_like(om)
         la = np.empty(om.shape)

@@ -83,18 +83,29 @@ class MLP:
 
     def set_params(self, p: np.ndarray) -> None:
         p = np.ascontiguousarray(p, dtype=np.float32)
-        assert p.size == self.nparams
+        if p.size != self.nparams:
+            raise ValueError(f"expected {self.nparams} parameters, got {p.size}")
         self._ck(self.lib.kls_mlp_set_params(self.h, self._f(p)))
 
+    @staticmethod
+    def _rows(A: np.ndarray, width: int, n: Optional[int] = None) -> np.ndarray:
+        """A as contiguous float32 [n, width]; the library reads n * width
+        floats, so any other shape is an error here."""
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        if A.ndim != 2 or A.shape[1] != width or (n is not None and A.shape[0] != n):
+            raise ValueError(f"expected a [{'n' if n is None else n}, {width}] array, "
+                             f"got shape {A.shape}")
+        return A
+
     def forward(self, X: np.ndarray) -> np.ndarray:
-        X = np.ascontiguousarray(X, dtype=np.float32)
+        X = self._rows(X, 5)
         Y = np.empty((X.shape[0], 3), dtype=np.float32)
         self._ck(self.lib.kls_mlp_forward(self.h, self._f(X), X.shape[0], self._f(Y)))
         return Y
 
     def grad(self, X: np.ndarray, T: np.ndarray) -> Tuple[np.ndarray, float]:
-        X = np.ascontiguousarray(X, dtype=np.float32)
-        T = np.ascontiguousarray(T, dtype=np.float32)
+        X = self._rows(X, 5)
+        T = self._rows(T, 3, X.shape[0])
         g = np.empty(self.nparams, dtype=np.float32)
         loss = np.zeros(1, dtype=np.float32)
         self._ck(self.lib.kls_mlp_grad(self.h, self._f(X), self._f(T), X.shape[0], self._f(g),
@@ -103,8 +114,8 @@ class MLP:
 
     def train(self, X: np.ndarray, T: np.ndarray, epochs: int = 40, batch: int = 4096,
               lr: float = 2e-3, seed: int = 0) -> np.ndarray:
-        X = np.ascontiguousarray(X, dtype=np.float32)
-        T = np.ascontiguousarray(T, dtype=np.float32)
+        X = self._rows(X, 5)
+        T = self._rows(T, 3, X.shape[0])
         hist = np.zeros(max(epochs, 1), dtype=np.float32)
         self._ck(self.lib.kls_mlp_train(self.h, self._f(X), self._f(T), X.shape[0], epochs, batch,
                                         lr, seed, self._f(hist)))

@@ -99,3 +99,16 @@ def test_shortlist_is_sorted_column_major_and_of_size_k():
     # the bowl's centre and its 8 neighbours are the 9 lowest predictions
     want = sorted(a * nG + b for a in range(9, 12) for b in range(4, 7))
     assert list(idx) == want
+
+
+def test_network_inputs_are_shape_checked_before_the_library_reads_them():
+    """The library reads n x 5 features and n x 3 targets: other shapes raise
+    on the host instead of being read out of bounds."""
+    import pytest
+    X = P.MLP._rows(np.zeros((7, 5), dtype=np.float64), 5)
+    assert X.dtype == np.float32 and X.flags.c_contiguous and X.shape == (7, 5)
+    assert P.MLP._rows(np.zeros((7, 3)), 3, 7).shape == (7, 3)
+    for bad, width, n in ((np.zeros((7, 4)), 5, None), (np.zeros(35), 5, None),
+                          (np.zeros((6, 3)), 3, 7)):
+        with pytest.raises(ValueError):
+            P.MLP._rows(bad, width, n)
