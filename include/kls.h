@@ -443,6 +443,20 @@ int kls_get_precompute_ms(kls_ctx* ctx, float* ms2);
 /* Kernels launched by this context since creation (monotone counter).      */
 int64_t kls_launch_count(const kls_ctx* ctx);
 
+/* ---- bounds-checked build (no reference counterpart) ---------------------- *
+ * libkls_checked.so, built from the same sources with KLS_CHECKED, guards
+ * the global accesses of the FP64 determinant path (orbits, W_l, rows,
+ * weights, contraction, reduction, LU, the allocation-free LU): an index
+ * outside its buffer's extent is skipped and logged instead of read or
+ * written.  kls_bounds_report returns, for the current device, the number
+ * of skipped accesses since the last reset and the site code (KlsSite in
+ * csrc/kls_internal.cuh), element index and extent of the first one;
+ * reset != 0 clears the logs.  Outputs may be NULL.  The reference has no
+ * sanitizer; this is the stand-in for one.  In the default libkls.so it
+ * returns KLS_ERR_UNSUPPORTED (message in kls_create_error()).             */
+int kls_bounds_report(int64_t* violations, int32_t* first_site, int64_t* first_index,
+                      int64_t* first_extent, int reset);
+
 #ifdef __cplusplus
 }
 #endif

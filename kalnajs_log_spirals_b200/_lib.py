@@ -10,6 +10,8 @@ import ctypes as C
 import os
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkls.so")
+# the same sources built with KLS_CHECKED (guarded accesses, kls_bounds_report)
+CHECKED_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libkls_checked.so")
 
 KLS_OK = 0
 KLS_ERR_CONFIG = 1
@@ -170,6 +172,8 @@ SIGNATURES = {
     "kls_get_stage_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_get_precompute_ms": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "kls_launch_count": (C.c_int64, [_P]),
+    "kls_bounds_report": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int]),
 }
 
 _lib = None
@@ -180,6 +184,17 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
+    _lib = _bind(path)
+    return _lib
+
+
+def load_checked(path: str = CHECKED_LIB_PATH) -> C.CDLL:
+    """The bounds-checked build (a separate library object, not cached as
+    the default); raises KlsError if it is missing."""
+    return _bind(path)
+
+
+def _bind(path: str) -> C.CDLL:
     if not os.path.exists(path):
         raise KlsError(KLS_ERR_STATE, f"{path} is missing: build it with "
                                       "`python -m kalnajs_log_spirals_b200.build`")
@@ -188,7 +203,6 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    _lib = lib
     return lib
 
 

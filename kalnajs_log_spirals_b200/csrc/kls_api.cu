@@ -22,6 +22,18 @@
 
 static thread_local std::string g_create_err;
 
+#ifdef KLS_CHECKED
+// readers of the translation units' bounds logs (registered at load time)
+static std::vector<int (*)(KlsBoundsLog*, bool)>& bounds_readers() {
+  static std::vector<int (*)(KlsBoundsLog*, bool)> r;
+  return r;
+}
+int kls_bounds_register(int (*reader)(KlsBoundsLog* out, bool reset)) {
+  bounds_readers().push_back(reader);
+  return (int)bounds_readers().size();
+}
+#endif
+
 int kls_fail(kls_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
   else g_create_err = msg;
@@ -1120,5 +1132,34 @@ int kls_get_stage_ms(kls_ctx* c, float* ms4) {
 }
 
 int64_t kls_launch_count(const kls_ctx* c) { return c ? c->launches : 0; }
+
+int kls_bounds_report(int64_t* violations, int32_t* first_site, int64_t* first_index,
+                      int64_t* first_extent, int reset) {
+#ifdef KLS_CHECKED
+  int64_t n = 0, idx = 0, ext = 0;
+  int32_t site = 0;
+  for (auto rd : bounds_readers()) {
+    KlsBoundsLog l{};
+    if (rd(&l, reset != 0))
+      return kls_fail(nullptr, KLS_ERR_CUDA, "kls_bounds_report: a device log could not be read");
+    if (l.count && !n) {
+      site = l.site;
+      idx = l.index;
+      ext = l.extent;
+    }
+    n += (int64_t)l.count;
+  }
+  if (violations) *violations = n;
+  if (first_site) *first_site = site;
+  if (first_index) *first_index = idx;
+  if (first_extent) *first_extent = ext;
+  return KLS_OK;
+#else
+  (void)violations; (void)first_site; (void)first_index; (void)first_extent; (void)reset;
+  return kls_fail(nullptr, KLS_ERR_UNSUPPORTED,
+                  "kls_bounds_report: this library is the default build; the bounds-checked "
+                  "build is libkls_checked.so");
+#endif
+}
 
 }  // extern "C"

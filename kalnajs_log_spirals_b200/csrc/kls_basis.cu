@@ -43,6 +43,10 @@ struct WlParams {
   double astep;          // alpha grid step
 };
 
+// orbit p's sample k, guarded in the bounds-checked build (plain t[k] otherwise)
+#define WL_SMP(t, k) \
+  KLS_LD(KLS_IB((int64_t)p * nwa + (k), (int64_t)NPh * nwa, KS_WL_SAMPLES), t[k], 0.0)
+
 __global__ void __launch_bounds__(WL_THREADS)
 wl_kernel(WlParams P, const double* __restrict__ of, const int* __restrict__ valid,
           const double* __restrict__ w1g, const double* __restrict__ rag,
@@ -62,8 +66,9 @@ wl_kernel(WlParams P, const double* __restrict__ of, const int* __restrict__ val
   const double* w1 = w1g + (size_t)p * nwa;
   const double* ra = rag + (size_t)p * nwa;
   const double* pha = phag + (size_t)p * nwa;
-  const bool ok = valid[p] != 0;
-  const double ratio = of[(size_t)OF_OM2 * NPh + p] / of[(size_t)OF_OM1 * NPh + p];
+  const bool ok = KLS_LD(KLS_IB(p, NPh, KS_WL_SAMPLES), valid[p] != 0, false);
+  const double ratio = KLS_LD(KLS_IB(p, NPh, KS_WL_SAMPLES),
+                              of[(size_t)OF_OM2 * NPh + p] / of[(size_t)OF_OM1 * NPh + p], 0.0);
 
   // accumulators: warp covers all 32 harmonics (4 m-tiles) x 16 alphas (2 n-tiles)
   double accR[4][2][2], accI[4][2][2];
@@ -85,14 +90,14 @@ wl_kernel(WlParams P, const double* __restrict__ of, const int* __restrict__ val
       // ---- generate C and E for samples k0..k0+15
       const int k = k0 + gk;
       if (k < nwa) {
-        double wk = w1[k], rk = ra[k];
-        double wm = k > 0 ? w1[k - 1] : 0.0, wp = k < nwa - 1 ? w1[k + 1] : 0.0;
+        double wk = WL_SMP(w1, k), rk = WL_SMP(ra, k);
+        double wm = k > 0 ? WL_SMP(w1, k - 1) : 0.0, wp = k < nwa - 1 ? WL_SMP(w1, k + 1) : 0.0;
         double sw;
         if (nwa < 2) sw = 0.0;
         else if (k == 0) sw = (wp - wk) / 2;
         else if (k == nwa - 1) sw = (wk - wm) / 2;
         else sw = (wp - wm) / 2;
-        double phi = ratio * wk - pha[k];
+        double phi = ratio * wk - WL_SMP(pha, k);
         // C: cos(l w1 + m phi), anchor at l_first, rotate by w1
         double th = (double)(P.l_min + l_first) * wk + (double)P.m * phi;
         double s, c, ss, cs;
@@ -110,7 +115,8 @@ wl_kernel(WlParams P, const double* __restrict__ of, const int* __restrict__ val
         // E: r^{-1/2} e^{-i alpha ln r}, anchor at a_first, rotate by -astep ln r
         double lr = log(rk);
         double isq = 1.0 / sqrt(rk);
-        double ta = -alpha[min(a_first, P.Na - 1)] * lr;
+        double ta = -KLS_LD(KLS_IB(min(a_first, P.Na - 1), P.Na, KS_WL_SAMPLES),
+                            alpha[min(a_first, P.Na - 1)], 0.0) * lr;
         sincos(ta, &s, &c);
         sincos(-P.astep * lr, &ss, &cs);
 #pragma unroll
@@ -170,6 +176,8 @@ wl_kernel(WlParams P, const double* __restrict__ of, const int* __restrict__ val
       double i0 = accI[i][j][0] / KLS_PI, i1 = accI[i][j][1] / KLS_PI;
       if (a0 >= P.Na) { r0 = 0.0; i0 = 0.0; }
       if (a0 + 1 >= P.Na) { r1 = 0.0; i1 = 0.0; }
+      KLS_UNLESS(KLS_IB((int64_t)row + a0 + 1, (int64_t)P.n_l * NPh * P.Na_pad, KS_WL_OUT),
+                 continue)
       *reinterpret_cast<double2*>(Wre + row + a0) = make_double2(r0, r1);
       *reinterpret_cast<double2*>(Wim + row + a0) = make_double2(i0, i1);
     }
@@ -212,6 +220,7 @@ __global__ void n_kernel(int Na, int m, const double* __restrict__ alpha,
                          const double* __restrict__ dalpha, double* __restrict__ Nk) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= Na) return;
+  KLS_UNLESS(KLS_IB(i, Na, KS_NKERNEL), return)
   double a = alpha[i];
   double l1 = ln_abs_gamma((m + 0.5) / 2, a / 2);
   double l3 = ln_abs_gamma((m + 1.5) / 2, a / 2);
@@ -223,8 +232,10 @@ __global__ void rows_kernel(int NPh, int n_l, int l_min, int m, int64_t K, int64
                             double* __restrict__ Ok, double* __restrict__ F0l) {
   int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K_pad) return;
+  KLS_UNLESS(KLS_IB(k, K_pad, KS_ROWS), return)
   if (k >= K) { Gk[k] = 0.0; Ok[k] = 0.0; F0l[k] = 0.0; return; }
   int il = (int)(k / NPh), p = (int)(k % NPh);
+  KLS_UNLESS(KLS_IB((int64_t)OF_DJ * NPh + p, (int64_t)OF_COUNT * NPh, KS_ROWS), return)
   double l = (double)(l_min + il);
   double om1 = of[(size_t)OF_OM1 * NPh + p], om2 = of[(size_t)OF_OM2 * NPh + p];
   double FE = of[(size_t)OF_FE * NPh + p], FL = of[(size_t)OF_FL * NPh + p];

@@ -70,7 +70,7 @@ __device__ __forceinline__ void weights_body(int64_t K_pad, double wr, double wi
                                              double2* __restrict__ out) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K_pad;
        k += (int64_t)gridDim.x * blockDim.x)
-    out[k] = weight_at(Gk[k], Ok[k], wr, wi);
+    KLS_IF(KLS_IB(k, K_pad, KS_WEIGHTS)) out[k] = weight_at(Gk[k], Ok[k], wr, wi);
 }
 
 // anchored: w_k(omega) - w_k(omega_a), each with the denominator clamp; the
@@ -89,11 +89,12 @@ __global__ void weights_kernel(int64_t K_pad, const double* __restrict__ omega,
   if (wr == ar && wi == ai) {                // at the anchor dM is exactly zero
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K_pad;
          k += (int64_t)gridDim.x * blockDim.x)
-      out[k] = make_double2(0.0, 0.0);
+      KLS_IF(KLS_IB(k, K_pad, KS_WEIGHTS)) out[k] = make_double2(0.0, 0.0);
     return;
   }
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < K_pad;
        k += (int64_t)gridDim.x * blockDim.x) {
+    KLS_UNLESS(KLS_IB(k, K_pad, KS_WEIGHTS), continue)
     const double2 a = weight_at(Gk[k], Ok[k], wr, wi), b = weight_at(Gk[k], Ok[k], ar, ai);
     out[k] = make_double2(a.x - b.x, a.y - b.y);
   }
@@ -152,10 +153,14 @@ __device__ __forceinline__ void contract_tile(const ContractParams& P,
       int row = rem >> 5, col = (rem & 31) * 2;
       const double* src = (plane & 1) ? Wim : Wre;
       int c0 = (plane < 2) ? b0 : a0;
+      // (bounds-checked build: the copy's last element inside [K_pad][Na_pad])
+      KLS_IF(KLS_IB((k0 + row) * (int64_t)ld + c0 + col + 1, P.K_pad * (int64_t)ld,
+                    KS_CONTRACT_SRC))
       cp_async16(st + plane * CT_PLANE + row * CT_S + col,
                  src + (size_t)(k0 + row) * ld + c0 + col);
     }
-    if (tid < CT_BK) cp_async16(st + 4 * CT_PLANE + 2 * tid, wz + k0 + tid);
+    if (tid < CT_BK) KLS_IF(KLS_IB(k0 + tid, P.K_pad, KS_CONTRACT_SRC))
+      cp_async16(st + 4 * CT_PLANE + 2 * tid, wz + k0 + tid);
   };
 
   double cr[4][4][2], ci[4][4][2];
@@ -233,6 +238,7 @@ __device__ __forceinline__ void contract_tile(const ContractParams& P,
     for (int j = 0; j < 4; ++j) {
       int a = a0 + wn * 32 + j * 8 + 2 * (lane & 3);
       double2* o = out + (size_t)b * ld + a;
+      KLS_UNLESS(KLS_IB((int64_t)b * ld + a + 1, (int64_t)ld * ld, KS_CONTRACT_OUT), continue)
       o[0] = make_double2(cr[i][j][0], ci[i][j][0]);
       o[1] = make_double2(cr[i][j][1], ci[i][j][1]);
     }
@@ -287,10 +293,14 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
       int row = rem >> 5, col = (rem & 31) * 2;
       const double* src = (plane & 1) ? Wim : Wre;
       int c0 = (plane < 2) ? b0 : a0;
+      // (bounds-checked build: the copy's last element inside [K_pad][Na_pad])
+      KLS_IF(KLS_IB((k0 + row) * (int64_t)ld + c0 + col + 1, P.K_pad * (int64_t)ld,
+                    KS_CONTRACT_SRC))
       cp_async16(st + plane * CT_PLANE + row * CT_S + col,
                  src + (size_t)(k0 + row) * ld + c0 + col);
     }
-    if (tid < CT_BK) cp_async16(st + 4 * CT_PLANE + 2 * tid, wz + k0 + tid);
+    if (tid < CT_BK) KLS_IF(KLS_IB(k0 + tid, P.K_pad, KS_CONTRACT_SRC))
+      cp_async16(st + 4 * CT_PLANE + 2 * tid, wz + k0 + tid);
   };
 
   double p1[4][4][2], p2[4][4][2], p3[4][4][2];
@@ -357,6 +367,7 @@ __device__ __forceinline__ void contract_tile_3m(const ContractParams& P,
     for (int j = 0; j < 4; ++j) {
       int a = a0 + wn * 32 + j * 8 + 2 * (lane & 3);
       double2* o = out + (size_t)b * ld + a;
+      KLS_UNLESS(KLS_IB((int64_t)b * ld + a + 1, (int64_t)ld * ld, KS_CONTRACT_OUT), continue)
 #pragma unroll
       for (int h = 0; h < 2; ++h)
         o[h] = make_double2(__dsub_rn(p1[i][j][h], p2[i][j][h]),
@@ -438,6 +449,8 @@ __device__ __forceinline__ void reduce_body(int Na, int Na_pad, int splits, doub
     const double2* src = part + (size_t)b * Na_pad + a;
     double sr = 0.0, si = 0.0;
     for (int s = 0; s < splits; ++s) {
+      KLS_UNLESS(KLS_IB((int64_t)s * plane + (int64_t)b * Na_pad + a,
+                        (int64_t)splits * plane, KS_REDUCE), continue)
       double2 v = src[(size_t)s * plane];
       sr += v.x;
       si += v.y;
@@ -445,6 +458,7 @@ __device__ __forceinline__ void reduce_body(int Na, int Na_pad, int splits, doub
     double n = Nk[a];
     // unfused products: 1 - mr must not become an FMA in one kernel only
     double mr = __dmul_rn(__dmul_rn(sr, G), n), mi = __dmul_rn(__dmul_rn(si, G), n);
+    KLS_UNLESS(KLS_IB(e, (int64_t)Na * Na, KS_REDUCE), continue)
     A[e] = make_double2((a == b ? 1.0 : 0.0) - mr, -mi);
     if (Mout) Mout[e] = make_double2(mr, mi);
   }

@@ -247,3 +247,71 @@ struct KlsRange {
   KlsRange(const KlsRange&) = delete;
   KlsRange& operator=(const KlsRange&) = delete;
 };
+
+// ---- bounds-checked build (KLS_CHECKED) ------------------------------------
+// libkls_checked.so is the same sources compiled with -DKLS_CHECKED: every
+// guarded global access of the FP64 determinant path (orbit, W_l, row,
+// weight, contraction, reduction and LU kernels) first tests its element
+// index against the extent of the buffer it touches, as the launch's own
+// parameters size it.  An access outside is skipped (a load reads 0) and
+// counted in this translation unit's device log, with the site code, index
+// and extent of the first one; kls_bounds_report collects the logs of every
+// unit.  The guards are written with the statement macros below, which
+// expand to nothing (KLS_IF, KLS_UNLESS) or to the unguarded expression
+// (KLS_LD) in the default build, so its preprocessed source is the
+// unguarded one token for token.
+enum KlsSite {
+  KS_ORBIT_TABLE = 1,   // cos / sin of the w grid, Rc and S_RC tables
+  KS_ORBIT_SAMPLES,     // w1 / r / theta samples written per orbit
+  KS_ORBIT_FIELDS,      // per-orbit scalar fields and the validity flag
+  KS_WL_SAMPLES,        // orbit samples and fields read by the W_l kernel
+  KS_WL_OUT,            // W table rows written
+  KS_ROWS,              // G_k / Omega_res / F0l rows and the fields they read
+  KS_NKERNEL,           // alpha grid and N_m(alpha)
+  KS_WEIGHTS,           // omega and the weight rows
+  KS_CONTRACT_SRC,      // table tiles and weights staged by the contraction
+  KS_CONTRACT_OUT,      // contraction partials written
+  KS_REDUCE,            // partials summed, I - M and M written
+  KS_LU,                // LU matrices, determinants
+  KS_LU_STATIC,         // allocation-free LU: input, scratch, determinants
+};
+#ifdef KLS_CHECKED
+struct KlsBoundsLog {
+  unsigned long long count;
+  long long index, extent;
+  int site, pad;
+};
+namespace {
+__device__ KlsBoundsLog g_kls_bounds;   // one per translation unit
+}
+__device__ __forceinline__ bool kls_in_bounds(long long i, long long n, int site) {
+  if (i >= 0 && i < n) return true;
+  if (atomicAdd(&g_kls_bounds.count, 1ull) == 0ull) {
+    g_kls_bounds.index = i;
+    g_kls_bounds.extent = n;
+    g_kls_bounds.site = site;
+  }
+  return false;
+}
+#define KLS_IB(i, n, site) kls_in_bounds((long long)(i), (long long)(n), (site))
+#define KLS_IF(cond) if (cond)
+#define KLS_UNLESS(cond, action) if (!(cond)) action;
+#define KLS_LD(cond, expr, fallback) ((cond) ? (expr) : (fallback))
+// host: every unit registers the reader of its log at load time
+int kls_bounds_register(int (*reader)(KlsBoundsLog* out, bool reset));
+namespace {
+int kls_bounds_read(KlsBoundsLog* out, bool reset) {
+  if (cudaMemcpyFromSymbol(out, g_kls_bounds, sizeof(KlsBoundsLog)) != cudaSuccess) return -1;
+  if (reset) {
+    KlsBoundsLog z{};
+    if (cudaMemcpyToSymbol(g_kls_bounds, &z, sizeof z) != cudaSuccess) return -1;
+  }
+  return 0;
+}
+const int kls_bounds_registered = kls_bounds_register(&kls_bounds_read);
+}
+#else
+#define KLS_IF(cond)
+#define KLS_UNLESS(cond, action)
+#define KLS_LD(cond, expr, fallback) expr
+#endif

@@ -32,6 +32,10 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
                       __fma_rn(a.x, b.y, __dmul_rn(a.y, b.x)));
 }
 
+// element (i, c) of the n x n matrix A, guarded in the bounds-checked build
+#define LU_IN(i, c) KLS_IB((int64_t)(i) * n + (c), (int64_t)n * n, KS_LU)
+#define LU_A(i, c) KLS_LD(LU_IN(i, c), A[(size_t)i * n + c], make_double2(0.0, 0.0))
+
 // LU of one n x n row-major matrix A by the whole CTA; writes *det_out and,
 // if given, *logabs_out.  sh holds 2 n complex values.
 __device__ __forceinline__ void lu_det_body(int n, double2* __restrict__ A, double2* sh,
@@ -55,7 +59,7 @@ __device__ __forceinline__ void lu_det_body(int n, double2* __restrict__ A, doub
     double bv = -1.0;
     int bi = n;
     for (int i = j + tid; i < n; i += blockDim.x) {
-      double2 v = A[(size_t)i * n + j];
+      double2 v = LU_A(i, j);
       double m = fabs(v.x) + fabs(v.y);
       if (m > bv) { bv = m; bi = i; }
     }
@@ -81,6 +85,7 @@ __device__ __forceinline__ void lu_det_body(int n, double2* __restrict__ A, doub
     // ---- row interchange (columns j..n-1; L columns are not needed for det)
     if (piv != j) {
       for (int c = j + tid; c < n; c += blockDim.x) {
+        KLS_UNLESS(LU_IN(j, c) && LU_IN(piv, c), continue)
         double2 t = A[(size_t)j * n + c];
         A[(size_t)j * n + c] = A[(size_t)piv * n + c];
         A[(size_t)piv * n + c] = t;
@@ -88,11 +93,11 @@ __device__ __forceinline__ void lu_det_body(int n, double2* __restrict__ A, doub
     }
     __syncthreads();
     // ---- pivot row and scaled column to shared memory
-    double2 u = A[(size_t)j * n + j];
+    double2 u = LU_A(j, j);
     const bool nz = (u.x != 0.0 || u.y != 0.0);
     double2 ru = nz ? cinv(u.x, u.y) : make_double2(0.0, 0.0);
-    for (int c = j + 1 + tid; c < n; c += blockDim.x) prow[c] = A[(size_t)j * n + c];
-    for (int i = j + 1 + tid; i < n; i += blockDim.x) lcol[i] = cmul(A[(size_t)i * n + j], ru);
+    for (int c = j + 1 + tid; c < n; c += blockDim.x) prow[c] = LU_A(j, c);
+    for (int i = j + 1 + tid; i < n; i += blockDim.x) lcol[i] = cmul(LU_A(i, j), ru);
     if (tid == 0) s_u = u;
     __syncthreads();
     // ---- rank-1 update of the trailing matrix
@@ -100,6 +105,7 @@ __device__ __forceinline__ void lu_det_body(int n, double2* __restrict__ A, doub
       double2 l = lcol[i];
       double2* row = A + (size_t)i * n;
       for (int c = j + 1 + lane; c < n; c += 32) {
+        KLS_UNLESS(LU_IN(i, c), continue)
         double2 p = prow[c];
         double2 a = row[c];
         a.x = __dsub_rn(a.x, __fma_rn(l.x, p.x, -__dmul_rn(l.y, p.y)));
@@ -198,6 +204,7 @@ lu_cluster_kernel(int n, const double2* __restrict__ Aall, double2* __restrict__
   const double2* A = Aall + (size_t)mat * n * n;
   for (int e = tid; e < my_nc * n; e += T) {
     const int lc = e / n, i = e % n;
+    KLS_UNLESS(KLS_IB((int64_t)i * n + rank + C * lc, (int64_t)n * n, KS_LU), continue)
     col[(size_t)lc * n + i] = A[(size_t)i * n + rank + C * lc];
   }
   double2* rec_u0 = cl.map_shared_rank(rec_u, 0);

@@ -128,6 +128,9 @@ __device__ T block_exclusive_scan(T val, T* sh, T* total) {
   return incl - val;  // exclusive
 }
 
+// table read, guarded in the bounds-checked build (plain t[i] otherwise)
+#define ORB_TAB(t, i) KLS_LD(KLS_IB((i), P.nw, KS_ORBIT_TABLE), t[i], 0.0)
+
 __global__ void __launch_bounds__(ORB_THREADS)
 orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __restrict__ sinw,
              const double* __restrict__ rc_tab, const double* __restrict__ SRC,
@@ -141,7 +144,7 @@ orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __res
   const int tid = threadIdx.x;
 
   // ---- grid scalars (OrbitIntegration.jl:102-170), computed redundantly
-  const double Rc = rc_tab[iR];
+  const double Rc = KLS_LD(KLS_IB(iR, P.NR, KS_ORBIT_TABLE), rc_tab[iR], 0.0);
   double v = kls_lin(P.v_min, 1.0, P.Ne, ie);
   if (fabs(v) < 1e-14) v = 1e-12;
   const double sg = (v > 0) ? 1.0 : ((v < 0) ? -1.0 : 0.0);
@@ -180,9 +183,10 @@ orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __res
         r = Rc;
         ph = wa * Om2 / Om1;
       } else {
-        r = Rc - a_j * cosw[i];
-        ph = wa * Om2 / Om1 + 2 * Om / kap * a_j / Rc * sinw[i] * sg;
+        r = Rc - a_j * ORB_TAB(cosw, i);
+        ph = wa * Om2 / Om1 + 2 * Om / kap * a_j / Rc * ORB_TAB(sinw, i) * sg;
       }
+      KLS_UNLESS(KLS_IB((int64_t)p * nwa + j, (int64_t)NPh * nwa, KS_ORBIT_SAMPLES), continue)
       w1p[j] = wa; rap[j] = r; php[j] = ph;
       fin = fin && isfinite(wa) && isfinite(r) && isfinite(ph);
     }
@@ -194,12 +198,12 @@ orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __res
     const double dtc = drs * P.dw;
     // svr / svr_phi with the reference's endpoint extrapolation
     auto vals_at = [&](int i, double& x, double& svr, double& svp) {
-      PointVals a = point_vals(rs, drs, E, L2, nonradial, cosw[i], sinw[i]);
+      PointVals a = point_vals(rs, drs, E, L2, nonradial, ORB_TAB(cosw, i), ORB_TAB(sinw, i));
       x = a.x; svr = a.svr; svp = a.svp;
       if (i == 0 || i == nw - 1) {
         int i1 = (i == 0) ? 1 : nw - 2, i2 = (i == 0) ? 2 : nw - 3;
-        PointVals b = point_vals(rs, drs, E, L2, nonradial, cosw[i1], sinw[i1]);
-        PointVals c = point_vals(rs, drs, E, L2, nonradial, cosw[i2], sinw[i2]);
+        PointVals b = point_vals(rs, drs, E, L2, nonradial, ORB_TAB(cosw, i1), ORB_TAB(sinw, i1));
+        PointVals c = point_vals(rs, drs, E, L2, nonradial, ORB_TAB(cosw, i2), ORB_TAB(sinw, i2));
         if (i == nw - 1 || nonradial) svr = 2.0 * b.svr - c.svr;
         svp = 2.0 * b.svp - c.svp;
       }
@@ -248,6 +252,7 @@ orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __res
           if (phase_int) ph = L * rp;
           else ph = (j == 0) ? 0.0 : (KLS_PI / 2) * 1.0 * sg;
           double wv = rt * Om1;
+          KLS_UNLESS(KLS_IB((int64_t)p * nwa + j, (int64_t)NPh * nwa, KS_ORBIT_SAMPLES), continue)
           w1p[j] = wv; rap[j] = x; php[j] = ph;
           fin = fin && isfinite(wv) && isfinite(x) && isfinite(ph);
           if (i == P.Ia_last) sh_misc[0] = ph;
@@ -284,13 +289,15 @@ orbit_kernel(OrbitParams P, const double* __restrict__ cosw, const double* __res
     if (!isfinite(FE)) FE = 0.0;
     if (!isfinite(FL)) FL = 0.0;
     // S_e quadrature weight (OrbitIntegration.jl:119-123); S_RC from the host
-    double src = SRC[iR];
+    double src = KLS_LD(KLS_IB(iR, P.NR, KS_ORBIT_TABLE), SRC[iR], 0.0);
     double se = v_weight(P, ie);
     double vals[OF_COUNT] = {Rc, ecc, v, R1, R2, E, L, L2, sg, se,
                              Om1, Om2, jac, F0, FE, FL, src * se * jac};
-    for (int f = 0; f < OF_COUNT; ++f) of[(size_t)f * NPh + p] = vals[f];
+    for (int f = 0; f < OF_COUNT; ++f)
+      KLS_IF(KLS_IB((int64_t)f * NPh + p, (int64_t)OF_COUNT * NPh, KS_ORBIT_FIELDS))
+      of[(size_t)f * NPh + p] = vals[f];
     double ratio = Om2 / Om1;
-    valid[p] = (all_fin && isfinite(ratio)) ? 1 : 0;
+    KLS_IF(KLS_IB(p, NPh, KS_ORBIT_FIELDS)) valid[p] = (all_fin && isfinite(ratio)) ? 1 : 0;
   }
 }
 

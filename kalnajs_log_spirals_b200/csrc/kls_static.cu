@@ -66,7 +66,8 @@ lu_det_static_kernel(int n, const double2* __restrict__ in, double2* __restrict_
   double2* A = scratch + (size_t)blockIdx.x * nn;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
-  for (size_t e = tid; e < nn; e += blockDim.x) A[e] = src[e];
+  for (size_t e = tid; e < nn; e += blockDim.x)
+    KLS_IF(KLS_IB((int64_t)blockIdx.x * nn + e, KLS_STATIC_LU_MAX, KS_LU_STATIC)) A[e] = src[e];
   __syncthreads();
 
   double2 mant = make_double2(1.0, 0.0);

@@ -138,3 +138,33 @@ def test_dptr_accepts_only_contiguous_doubles():
                 np.zeros((4, 4))[:, 1]):
         with pytest.raises(TypeError):
             _lib.dptr(bad)
+
+
+def test_bounds_checked_build_loads_and_reports(lib_path):
+    """libkls_checked.so (the same sources with KLS_CHECKED: guarded global
+    accesses, a device log per translation unit) is built beside libkls.so,
+    exports the same symbols, and answers kls_bounds_report; the default
+    library answers KLS_ERR_UNSUPPORTED and names the checked one."""
+    import torch
+    lib = _lib.load(lib_path)
+    v = C.c_int64(-1)
+    assert lib.kls_bounds_report(C.byref(v), None, None, None, 0) == _lib.KLS_ERR_UNSUPPORTED
+    assert b"libkls_checked.so" in lib.kls_create_error()
+    assert v.value == -1
+    checked = _lib.load_checked()
+    for s in header_symbols():
+        assert hasattr(checked, s), s
+    out = subprocess_ldd(_lib.CHECKED_LIB_PATH)
+    assert "torch" not in out and "libcudart.so" not in out
+    site, idx, ext = C.c_int32(-1), C.c_int64(-1), C.c_int64(-1)
+    code = checked.kls_bounds_report(C.byref(v), C.byref(site), C.byref(idx), C.byref(ext), 1)
+    if torch.cuda.is_available():
+        assert code == _lib.KLS_OK and v.value == 0
+    else:
+        # no device: the logs cannot be read, and the call says so
+        assert code == _lib.KLS_ERR_CUDA and b"device log" in checked.kls_create_error()
+
+
+def subprocess_ldd(path):
+    import subprocess
+    return subprocess.run(["ldd", path], capture_output=True, text=True).stdout
