@@ -1,5 +1,6 @@
 """CPU checks of the proposer's oracle and feature encoding."""
 import numpy as np
+import pytest
 
 from oracle import np_mlp as O
 from kalnajs_log_spirals_b200 import proposer as P
@@ -126,3 +127,24 @@ def test_propose_includes_the_lowest_gamma_row():
     Op, g, used = P.propose(net, spec, det_fn, k=12)
     assert (Op, g) == (float(np.linspace(0.2, 0.6, 41)[32]), 0.01)
     assert calls[0] == 12 + 41 - len(set(range(0, 41 * 20, 20)) & set(P.shortlist(net, spec, k=12)[2]))
+
+
+def test_propose_ties_go_to_the_first_point_in_column_major_order():
+    """|det| constant on the grid: find_minimum (GridScan.jl:234-246) takes
+    grid index 0, and so does the proposal."""
+    spec = P.ModelSpec(4, 7.0, 2)
+    net = _StubNet(0.4, 0.1)
+    Op, g, _ = P.propose(net, spec, lambda om: np.ones(len(om)), k=12)
+    assert (Op, g) == (0.2, 0.01)
+
+
+def test_network_inputs_are_shape_checked_before_the_library_reads_them():
+    """The library reads n x 5 features and n x 3 targets: other shapes raise
+    on the host instead of being read out of bounds."""
+    X = P.MLP._rows(np.zeros((7, 5), dtype=np.float64), 5)
+    assert X.dtype == np.float32 and X.flags.c_contiguous and X.shape == (7, 5)
+    assert P.MLP._rows(np.zeros((7, 3)), 3, 7).shape == (7, 3)
+    for bad, width, n in ((np.zeros((7, 4)), 5, None), (np.zeros(35), 5, None),
+                          (np.zeros((6, 3)), 3, 7)):
+        with pytest.raises(ValueError):
+            P.MLP._rows(bad, width, n)
