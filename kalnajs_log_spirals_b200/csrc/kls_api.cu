@@ -72,7 +72,11 @@ int validate(const kls_config* k, std::string& msg) {
     return KLS_ERR_CONFIG;
   }
   double np = (double)k->NR * k->Ne;
+  if (np > (double)INT_MAX) return bad("NR * Ne must be below 2^31 (orbit index range)");
   if (np * (k->l_max - k->l_min + 1) > 4.0e9) return bad("NPh * n_l too large");
+  // the determinant's LU keeps two rows of N_alpha complex values in the
+  // shared memory of one CTA (227 KB on sm_100)
+  if (k->N_alpha > 7168) return bad("N_alpha must be <= 7168 (LU rows in shared memory)");
   if (!std::isfinite(k->G) || !std::isfinite(k->L0) || !std::isfinite(k->v_min))
     return bad("non-finite G, L0 or v_min");
   for (int q : {k->quad_alpha, k->quad_rc, k->quad_v})

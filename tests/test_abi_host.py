@@ -61,6 +61,13 @@ def test_invalid_config_rejected_before_device(lib_path):
     cfg.nw, cfg.nwa = 101, 11
     cfg.l_max = -5
     assert lib.kls_create(C.byref(cfg), 0, C.byref(h)) == _lib.KLS_ERR_CONFIG
+    cfg.l_max = 1
+    cfg.NR, cfg.Ne = 50000, 50000          # 2.5e9 orbits: past the int32 orbit index
+    assert lib.kls_create(C.byref(cfg), 0, C.byref(h)) == _lib.KLS_ERR_CONFIG
+    assert b"2^31" in lib.kls_create_error()
+    cfg.NR, cfg.Ne, cfg.N_alpha = 4, 3, 8000   # LU rows beyond one CTA's shared memory
+    assert lib.kls_create(C.byref(cfg), 0, C.byref(h)) == _lib.KLS_ERR_CONFIG
+    assert b"N_alpha" in lib.kls_create_error()
 
 
 def test_null_context_calls_fail_cleanly(lib_path):
