@@ -136,7 +136,12 @@ typedef struct kls_scan_cfg {
 typedef struct kls_ctx kls_ctx;
 
 /* ---- lifecycle ---------------------------------------------------------- */
-/* Replaces create_toomre_zang_model + the device selection of to_device. */
+/* Replaces create_toomre_zang_model + the device selection of to_device.
+ * The configuration is checked before the device is touched
+ * (KLS_ERR_CONFIG): the reference's own (nw, nwa) DimensionMismatch, and the
+ * sizes this library supports: NR * Ne < 2^31, NPh * n_l <= 4e9 and
+ * N_alpha <= 7168 (the LU keeps two rows of N_alpha complex values in one
+ * CTA's shared memory). */
 int kls_create(const kls_config* cfg, int device, kls_ctx** out);
 int kls_destroy(kls_ctx* ctx);
 /* Message of the last failing call on this context (never NULL). */
